@@ -1,0 +1,392 @@
+"""Benchmark of the displacement-field generator (gradient method).
+
+Workload (the headline configuration): a 256^3 volume, target J = clip(exp(
+sum of 16 Gaussian blobs), 0.7, 1.4), mask = |log J| > 0.01 dilated by 3,
+zero initial field, the reference's default parameters; FP32 field and
+stencils with FP64 reductions.  One step = one solve from the zero field
+capped at --it-max iterations.  Metric: voxel-iterations/s = voxels x
+iterations completed / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank solves its own volume (independent volumes: weak
+scaling, no collective on the data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "gradient-descent voxel-iters/s at 256³, FP32-mixed vs FP64 plain; % HBM peak"
+UNIT = "voxel-iters/s"
+# Algorithmic bytes per voxel of one launch (FP32 field): the trial reads the
+# field, the gradient, the target map and the mask and writes the candidate;
+# the gradient pass reads the field, the target map and the mask and writes
+# the gradient.
+BYTES_PER_VOXEL = {"trial": 12 + 12 + 4 + 1 + 12, "gradient": 12 + 4 + 1 + 12}
+BYTES_PER_VOXEL_FP64 = {"trial": 24 + 24 + 8 + 1 + 24, "gradient": 24 + 8 + 1 + 24}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--size", type=int, default=256)
+    p.add_argument("--it-max", type=int, default=100)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(world, v: float) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def iterations_done(st) -> int:
+    # the loop counter exceeds it_max by one when the budget ran out
+    return int(st["iterations"] - 1 if st["reason"] == "it_max" else st["iterations"])
+
+
+def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6):
+    """The reference C library (FP64, OpenMP, all host cores) on the same
+    volume: per-iteration rate from two solves (it_max it_lo and it_hi), so
+    set-up work cancels out."""
+    from oracle.oracle import Oracle, Reference
+    if Reference.available("ref64"):
+        impl, kind = Reference("ref64"), "reference"
+    else:
+        impl, kind = Oracle(4), "port"
+    times = {}
+    for it in (it_lo, it_hi):
+        t0 = time.perf_counter()
+        impl.solve("gradient", Jt, mask, it_max=it)
+        times[it] = time.perf_counter() - t0
+    n = Jt.size
+    rate = n * (it_hi - it_lo) / max(times[it_hi] - times[it_lo], 1e-9)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return rate, kind, cores, times
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    from disptools_b200.synthetic import blob_problem
+    n = args.size
+    Jt, mask = blob_problem((n, n, n), blobs=16, seed=0)
+    rates = []
+    samples = []
+    for s in range(args.warmup + args.steps):
+        rate, kind, cores, times = reference_cpu_rate(Jt, mask)
+        if s >= args.warmup:
+            rates.append(rate)
+            samples.append(times)
+    value = statistics.mean(rates)
+    sample = (f"per step: reference C library (FLOAT_SIZE=64, ORDER_PD=4, OpenMP) solving the "
+              f"{n}^3 volume with it_max=1 and it_max=6; rate = voxels x 5 / time difference")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * statistics.mean(t[6] + t[1] for t in samples),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"config 2: gradient method on {n}^3, 16 Gaussian blobs",
+                   "size": [n, n, n]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+
+    import disptools_b200 as dt
+    from disptools_b200 import _native as N
+    from disptools_b200 import torch_ops
+    from disptools_b200.synthetic import blob_problem
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.size
+    Jt_np, mask_np = blob_problem((n, n, n), blobs=16, seed=rank)
+    nvox = Jt_np.size
+    IT = args.it_max
+
+    Jt = torch.from_numpy(Jt_np).float().to(dev)
+    mask = torch.from_numpy(mask_np).to(dev)
+    field = torch.zeros((3, n, n, n), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        field.zero_()
+        return torch_ops.solve(Jt, mask, field, it_max=IT)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs
+    dt.set_profiling(True)
+    launches0 = dt.kernel_launch_count()
+    iters = trials = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            st = step()
+            iters += iterations_done(st)
+            trials += st["trials"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    launches = dt.kernel_launch_count() - launches0
+    prof = dt.kernel_profile()
+    dt.set_profiling(False)
+    ms_max = max_over_ranks(world, ms)
+    total_vi = sum_over_ranks(world, float(nvox) * iters)
+    value = total_vi / (ms_max / 1000.0)
+    tbar = trials / max(iters, 1)
+
+    # ---- roofline of the dominant kernel (device time of the launches that did work)
+    hbm, peak_kind = peaks()
+    dom = max(prof, key=lambda k: prof[k][1]) if prof else "trial"
+    nl, tot_ms = prof.get(dom, (0, 0.0))
+    avg_ms = tot_ms / max(nl, 1)
+    bytes_launch = BYTES_PER_VOXEL[dom] * nvox
+    achieved = bytes_launch / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            t = json.load(open(tpath))
+            traffic = t.get(dom, {}).get("bytes_per_launch_256")
+        except Exception:
+            traffic = None
+    kernels = {k: {"launches": v[0], "avg_ms": v[1] / max(v[0], 1),
+                   "achieved_gbs": BYTES_PER_VOXEL[k] * nvox / (v[1] / max(v[0], 1) / 1000.0) / 1e9
+                   if v[0] else None,
+                   "share": v[1] / max(sum(x[1] for x in prof.values()), 1e-12)}
+               for k, v in prof.items()}
+    path_achieved = (29 + 41 * tbar) * value / 1e9 / world
+
+    # ---- plain FP64 path (same workload, fewer steps)
+    fp64 = None
+    if not args.no_fp64:
+        Jt64 = torch.from_numpy(Jt_np).to(dev)
+        f64 = torch.zeros((3, n, n, n), dtype=torch.float64, device=dev)
+        f64.zero_()
+        torch_ops.solve(Jt64, mask, f64, it_max=IT)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it64 = 0
+        k64 = max(1, min(args.steps, 2))
+        for _ in range(k64):
+            f64.zero_()
+            s64 = torch_ops.solve(Jt64, mask, f64, it_max=IT)
+            it64 += iterations_done(s64)
+        torch.cuda.synchronize()
+        t64 = time.perf_counter() - t0
+        v64 = nvox * it64 / t64
+        fp64 = {"value": v64, "unit": UNIT, "ratio_mixed_over_fp64": (value / world) / v64,
+                "steps": k64}
+        del Jt64, f64
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        from disptools_b200.api import make_params
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        Jh = pin(np.ascontiguousarray(Jt_np))
+        mh = pin(np.ascontiguousarray(mask_np))
+        fh = pin(np.zeros((3, n, n, n)))
+        p = make_params(it_max=IT)
+        stt = N.SolveStats()
+
+        def e2e_step():
+            fh[...] = 0.0
+            rc = N.lib.dtb_generate_displacement(0, 0, n, n, n, 1.0, 1.0, 1.0, Jh.ctypes.data,
+                                                 mh.ctypes.data, C.byref(p), fh.ctypes.data,
+                                                 C.byref(stt))
+            N.check(rc)
+            return stt.as_dict()
+
+        e2e_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        ie = 0
+        ke = max(1, min(args.steps, 3))
+        for _ in range(ke):
+            ie += iterations_done(e2e_step())
+        te = max_over_ranks(world, time.perf_counter() - t0)
+        e2e = {"value": sum_over_ranks(world, float(nvox) * ie) / te, "unit": UNIT,
+               "h2d_bytes_per_step": int(Jh.nbytes + mh.nbytes + fh.nbytes),
+               "d2h_bytes_per_step": int(fh.nbytes), "steps": ke,
+               "path": "dtb_generate_displacement (C ABI, host float64 arrays in pinned memory)"}
+
+    # ---- CPU baseline (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, times = reference_cpu_rate(Jt_np, mask_np)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"{n}^3 volume, reference C library FP64 OpenMP: solves with it_max=1 "
+                         f"({times[1]:.2f} s) and it_max=6 ({times[6]:.2f} s); "
+                         f"rate = voxels x 5 / time difference"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"config 2: gradient method on {n}^3 (16 Gaussian blobs), "
+                                   f"FP32 field, FP64 reductions, zero initial field, "
+                                   f"it_max={IT} per step",
+                       "size": [n, n, n], "it_max_per_step": IT,
+                       "l2": "inputs larger than L2 (FP32 field 201 MB + gradient 201 MB)",
+                       "iterations_per_step": iters / args.steps,
+                       "trials_per_iteration": tbar, "parallelism": f"{world} independent volumes"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "bytes_per_launch": bytes_launch, "avg_launch_ms": avg_ms,
+                         "kernels": kernels,
+                         "path_achieved_gbs": path_achieved,
+                         "path_frac": path_achieved / hbm},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "fp64_plain": fp64,
+        }
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,861 @@
+// Host side of disptools_b200: the C ABI, the error state, the device
+// workspace and the device-resident solve loop.
+//
+// A solve runs as a sequence of "steps"; each step is one gradient launch
+// (a no-op for volumes that do not need a new gradient) followed by one trial
+// launch whose last block runs the step control of every volume on the
+// device.  Steps are captured once into a CUDA graph of K steps and the graph
+// is relaunched until every volume reports done; the host reads the small
+// state array once per graph launch, never per trial.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+#include <vector>
+
+#include "dt_internal.h"
+
+using namespace dtb;
+
+// ---------------------------------------------------------------------------
+// Error state: same record and semantics as src/disptools.c:8-43.
+// ---------------------------------------------------------------------------
+static disptools_error_state g_error = {false, -1, "", "", "", ""};
+
+static void set_error(int line, const char *function, const char *message) {
+    g_error.error = true;
+    g_error.line = line;
+    std::snprintf(g_error.file, sizeof g_error.file, "%s", __FILE__);
+    std::snprintf(g_error.function, sizeof g_error.function, "%s", function);
+    std::snprintf(g_error.message, sizeof g_error.message, "%s", message);
+    g_error.trace[0] = '\0';
+}
+
+#define DTB_FAIL(code, msg)                         \
+    do {                                            \
+        set_error(__LINE__, __func__, (msg));       \
+        return (code);                              \
+    } while (0)
+
+#define DTB_CUDA(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            char m_[1024];                                                                     \
+            std::snprintf(m_, sizeof m_, "CUDA error %d (%s) in %s", (int) e_,                 \
+                          cudaGetErrorString(e_), #call);                                      \
+            set_error(__LINE__, __func__, m_);                                                 \
+            return DTB_ERR_CUDA;                                                               \
+        }                                                                                      \
+    } while (0)
+
+extern "C" disptools_error_state *disptools_get_error(void) { return &g_error; }
+extern "C" bool disptools_has_error(void) { return g_error.error; }
+extern "C" void disptools_clear_error(void) {
+    g_error.error = false;
+    g_error.line = -1;
+    g_error.file[0] = g_error.function[0] = g_error.message[0] = g_error.trace[0] = '\0';
+}
+extern "C" int get_float_type_size(void) { return 64; }
+
+static std::atomic<unsigned long long> g_launches{0};
+static thread_local bool t_capturing = false;
+void dtb::set_capturing(bool on) { t_capturing = on; }
+void dtb::count_launch(unsigned n) {
+    if (!t_capturing) g_launches += n;
+}
+extern "C" unsigned long long dtb_kernel_launch_count(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------------------
+// Kernel profiling: per-kernel launch counts and device time of the launches
+// that did work, measured with CUDA events recorded between the kernels of
+// the captured step graph.
+// ---------------------------------------------------------------------------
+namespace {
+enum { PROF_TRIAL = 0, PROF_GRADIENT = 1, PROF_KINDS = 2 };
+const char *const kProfNames[PROF_KINDS] = {"trial", "gradient"};
+struct Profile {
+    bool on = false;
+    long long launches[PROF_KINDS] = {0, 0};
+    double ms[PROF_KINDS] = {0.0, 0.0};
+};
+std::mutex g_prof_mutex;
+Profile g_prof;
+}  // namespace
+
+extern "C" int dtb_set_profiling(int on) {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    g_prof = Profile();
+    g_prof.on = on != 0;
+    return DTB_OK;
+}
+
+extern "C" int dtb_get_profile(dtb_kernel_profile *out, int max) {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    int n = 0;
+    for (int k = 0; k < PROF_KINDS && n < max; ++k, ++n) {
+        std::snprintf(out[n].name, sizeof out[n].name, "%s", kProfNames[k]);
+        out[n].launches = g_prof.launches[k];
+        out[n].total_ms = g_prof.ms[k];
+    }
+    return n;
+}
+
+static int default_precision_init() {
+    const char *p = std::getenv("DISPTOOLS_B200_PRECISION");
+    if (p && (!std::strcmp(p, "fp64") || !std::strcmp(p, "FP64") || !std::strcmp(p, "double")))
+        return DTB_PRECISION_FP64;
+    return DTB_PRECISION_MIXED;
+}
+static int g_default_precision = default_precision_init();
+
+extern "C" int dtb_set_default_precision(int precision) {
+    if (precision != DTB_PRECISION_MIXED && precision != DTB_PRECISION_FP64) {
+        set_error(__LINE__, __func__, "invalid precision");
+        return DTB_ERR_ARGUMENT;
+    }
+    g_default_precision = precision;
+    return DTB_OK;
+}
+extern "C" int dtb_get_default_precision(void) { return g_default_precision; }
+
+// cuda/device.cu:4-15
+extern "C" bool set_device(const int id) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        set_error(__LINE__, __func__, "cannot query the CUDA device count");
+        return false;
+    }
+    if (id < 0 || id >= n) return false;
+    if (cudaSetDevice(id) != cudaSuccess) {
+        cudaGetLastError();
+        set_error(__LINE__, __func__, "cudaSetDevice failed");
+        return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Device workspace: one growing allocation reused across calls.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Workspace {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+};
+std::mutex g_ws_mutex;
+Workspace g_ws;
+
+// Returns a device buffer of at least `bytes` on the current device.
+int workspace(size_t bytes, char **out) {
+    int dev = 0;
+    DTB_CUDA(cudaGetDevice(&dev));
+    if (g_ws.ptr && (g_ws.bytes < bytes || g_ws.device != dev)) {
+        if (g_ws.device == dev) cudaFree(g_ws.ptr);
+        g_ws.ptr = nullptr;
+        g_ws.bytes = 0;
+    }
+    if (!g_ws.ptr) {
+        const size_t want = bytes + bytes / 8;
+        if (cudaMalloc(&g_ws.ptr, want) != cudaSuccess) {
+            cudaGetLastError();
+            g_ws.ptr = nullptr;
+            DTB_FAIL(DTB_ERR_ALLOC, "cannot allocate the device workspace");
+        }
+        g_ws.bytes = want;
+        g_ws.device = dev;
+    }
+    *out = static_cast<char *>(g_ws.ptr);
+    return DTB_OK;
+}
+
+// Bump allocator over a workspace region (256-byte alignment).
+struct Carve {
+    char *base;
+    size_t off = 0;
+    template <typename U>
+    U *take(size_t count) {
+        off = (off + 255) & ~size_t(255);
+        U *p = reinterpret_cast<U *>(base + off);
+        off += count * sizeof(U);
+        return p;
+    }
+};
+
+bool valid_dims(size_t nx, size_t ny, size_t nz) {
+    // The one-sided boundary stencils read two voxels inward (src/headers/
+    // jacobian_macros.h:7-99), so every axis needs at least three voxels.
+    return nx >= 3 && ny >= 3 && nz >= 3 && nx < (1u << 30) && ny < (1u << 30) && nz < (1u << 30);
+}
+
+Geom make_geom(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz, int order = 4) {
+    Geom g;
+    g.nx = (int) nx;
+    g.ny = (int) ny;
+    g.nz = (int) nz;
+    g.order = order;
+    g.ys = (long long) nx;
+    g.zs = (long long) nx * ny;
+    g.cs = (long long) nx * ny * nz;
+    g.ih[0] = 1.0 / dx;  // src/jacobian.c:73-75
+    g.ih[1] = 1.0 / dy;
+    g.ih[2] = 1.0 / dz;
+    g.sp[0] = dx;
+    g.sp[1] = dy;
+    g.sp[2] = dz;
+    return g;
+}
+
+int pick_bz(int nz) {
+    const char *e = std::getenv("DISPTOOLS_B200_BZ");
+    if (e) {
+        const int v = std::atoi(e);
+        if (v > 0) return v;
+    }
+    return nz < 32 ? nz : 32;
+}
+
+int steps_per_graph() {
+    const char *e = std::getenv("DISPTOOLS_B200_STEPS_PER_GRAPH");
+    if (e) {
+        const int v = std::atoi(e);
+        if (v > 0) return v;
+    }
+    return 16;
+}
+
+// Device view of one volume for the solver (device pointers of type T).
+template <typename T>
+struct DevVol {
+    Geom g;
+    const T *Jt;
+    const uint8_t *mask;
+    T *field;  // in: initial guess, out: result
+};
+
+// Device-resident solve of `vols` (all inputs already on the device).
+template <typename T>
+int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                    dtb_solve_stats *stats, int precision, cudaStream_t stream);
+
+// Runs the solve on a private non-blocking stream (graph capture is not
+// allowed on the legacy default stream), ordered after the caller's stream
+// and before anything the caller enqueues next.
+template <typename T>
+int solve_device(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                 dtb_solve_stats *stats, int precision, cudaStream_t user) {
+    cudaStream_t work;
+    DTB_CUDA(cudaStreamCreateWithFlags(&work, cudaStreamNonBlocking));
+    cudaEvent_t ev;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        cudaStreamDestroy(work);
+        DTB_CUDA(cudaGetLastError());
+    }
+    int rc = DTB_OK;
+    if (cudaEventRecord(ev, user) != cudaSuccess || cudaStreamWaitEvent(work, ev, 0) != cudaSuccess) {
+        rc = DTB_ERR_CUDA;
+        set_error(__LINE__, __func__, "cannot order the solve after the caller's stream");
+    } else {
+        rc = solve_device_on<T>(algorithm, vols, p, stats, precision, work);
+        if (cudaEventRecord(ev, work) == cudaSuccess) cudaStreamWaitEvent(user, ev, 0);
+    }
+    cudaStreamSynchronize(work);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(work);
+    return rc;
+}
+
+template <typename T>
+int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                    dtb_solve_stats *stats, int precision, cudaStream_t stream) {
+    const int count = (int) vols.size();
+    // ---- workspace layout
+    std::vector<int> tiles(count), tbegin(count);
+    int total_tiles = 0;
+    size_t need = 0;
+    auto align = [](size_t b) { return (b + 255) & ~size_t(255); };
+    for (int i = 0; i < count; ++i) {
+        const Geom &g = vols[i].g;
+        const int bz = pick_bz(g.nz);
+        const int t = ((g.nx + BX - 1) / BX) * ((g.ny + BY - 1) / BY) * ((g.nz + bz - 1) / bz);
+        tiles[i] = t;
+        tbegin[i] = total_tiles;
+        total_tiles += t;
+        const size_t N = (size_t) g.cs;
+        need += align(3 * N * sizeof(T));                                   // field[1]
+        need += align(3 * N * sizeof(T));                                   // gradient
+        if (algorithm == DTB_ALGORITHM_GREEDY) need += 2 * align(N * sizeof(T));  // error maps
+        need += align(t * sizeof(double2)) + align(t * sizeof(double));
+        need += align(sizeof(SolverState));
+    }
+    need += align(count * sizeof(VolumeDesc<T>)) + align(total_tiles * sizeof(int));
+
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    char *base = nullptr;
+    int rc = workspace(need, &base);
+    if (rc != DTB_OK) return rc;
+    Carve cv{base};
+
+    std::vector<VolumeDesc<T>> desc(count);
+    std::vector<SolverState> hst(count);
+    std::vector<int> tile_vol(total_tiles);
+    for (int i = 0; i < count; ++i) {
+        const Geom &g = vols[i].g;
+        const size_t N = (size_t) g.cs;
+        VolumeDesc<T> &d = desc[i];
+        std::memset(&d, 0, sizeof d);
+        d.g = g;
+        d.field[0] = vols[i].field;
+        d.field[1] = cv.take<T>(3 * N);
+        d.grad = cv.take<T>(3 * N);
+        d.Jt = vols[i].Jt;
+        d.mask = vols[i].mask;
+        if (algorithm == DTB_ALGORITHM_GREEDY) {
+            d.v[0] = cv.take<T>(N);
+            d.v[1] = cv.take<T>(N);
+        } else {
+            d.v[0] = d.v[1] = nullptr;
+        }
+        d.jout = nullptr;
+        d.part_t = cv.take<double2>(tiles[i]);
+        d.part_g = cv.take<double>(tiles[i]);
+        d.st = cv.take<SolverState>(1);
+        const int bz = pick_bz(g.nz);
+        d.tiles_x = (g.nx + BX - 1) / BX;
+        d.tiles_y = (g.ny + BY - 1) / BY;
+        d.tiles_z = (g.nz + bz - 1) / bz;
+        d.tile_begin = tbegin[i];
+        d.ntiles = tiles[i];
+        d.bz = bz;
+        for (int t = 0; t < tiles[i]; ++t) tile_vol[tbegin[i] + t] = i;
+
+        SolverState &s = hst[i];
+        std::memset(&s, 0, sizeof s);
+        s.epsilon = p.epsilon;
+        s.tolerance = p.tolerance;
+        s.eta_max = p.eta_max;
+        s.alpha = p.alpha;
+        s.beta = p.beta;
+        s.gamma = p.gamma;
+        s.delta = p.delta;
+        s.zeta = p.zeta;
+        s.theta = p.theta;
+        s.iota = p.iota;
+        s.it_max = p.it_max;
+        s.strict = p.strict;
+        s.algorithm = algorithm;
+        s.eta = p.eta;
+        s.E_last = DBL_MAX;
+        s.M_last = DBL_MAX;
+        s.phase = PH_EVAL0;
+
+        // The second field buffer starts at zero: the greedy update never
+        // writes boundary voxels, so they keep the buffer's content
+        // (src/displacement_field_greedy.c:43-65 with calloc'd buffers).
+        DTB_CUDA(cudaMemsetAsync(d.field[1], 0, 3 * N * sizeof(T), stream));
+        DTB_CUDA(cudaMemsetAsync(d.grad, 0, 3 * N * sizeof(T), stream));
+        if (d.v[0]) {
+            DTB_CUDA(cudaMemsetAsync(d.v[0], 0, N * sizeof(T), stream));
+            DTB_CUDA(cudaMemsetAsync(d.v[1], 0, N * sizeof(T), stream));
+        }
+    }
+    VolumeDesc<T> *d_desc = cv.take<VolumeDesc<T>>(count);
+    int *d_tile_vol = cv.take<int>(total_tiles);
+    // States are contiguous per volume but carved separately; gather them.
+    std::vector<SolverState *> d_states(count);
+    for (int i = 0; i < count; ++i) {
+        d_states[i] = desc[i].st;
+        DTB_CUDA(cudaMemcpyAsync(desc[i].st, &hst[i], sizeof(SolverState), cudaMemcpyHostToDevice, stream));
+    }
+    DTB_CUDA(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(VolumeDesc<T>), cudaMemcpyHostToDevice, stream));
+    DTB_CUDA(cudaMemcpyAsync(d_tile_vol, tile_vol.data(), total_tiles * sizeof(int), cudaMemcpyHostToDevice,
+                             stream));
+
+    const int mode = algorithm == DTB_ALGORITHM_GREEDY ? MODE_GREEDY : MODE_GRAD;
+    const int grid = total_tiles;
+
+    cudaEvent_t ev0, ev1;
+    DTB_CUDA(cudaEventCreate(&ev0));
+    DTB_CUDA(cudaEventCreate(&ev1));
+    DTB_CUDA(cudaEventRecord(ev0, stream));
+
+    // Evaluate the initial fields (launched once, outside the graph; this is
+    // also the first launch of each kernel, which sets its attributes).
+    DTB_CUDA(launch_trial<T>(mode, d_desc, d_tile_vol, total_tiles, grid, stream));
+    if (algorithm == DTB_ALGORITHM_GRADIENT)
+        DTB_CUDA(launch_gradient<T>(d_desc, d_tile_vol, total_tiles, grid, stream));
+
+    // Capture K steps into a graph.  With profiling on, event records are
+    // captured between the kernels and every kernel gets a flag that it sets
+    // when it did work.
+    const int K = steps_per_graph();
+    const bool prof = g_prof.on;
+    const int kernels_per_step = algorithm == DTB_ALGORITHM_GRADIENT ? 2 : 1;
+    const int nk = K * kernels_per_step;
+    std::vector<cudaEvent_t> evs(prof ? nk + 1 : 0);
+    unsigned char *d_flags = nullptr, *h_flags = nullptr;
+    if (prof) {
+        for (auto &e : evs) DTB_CUDA(cudaEventCreate(&e));
+        DTB_CUDA(cudaMalloc(&d_flags, nk));
+        DTB_CUDA(cudaMallocHost(&h_flags, nk));
+    }
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    set_capturing(true);
+    DTB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    if (prof) {
+        cudaMemsetAsync(d_flags, 0, nk, stream);
+        cudaEventRecord(evs[0], stream);
+    }
+    for (int k = 0, j = 0; k < K; ++k) {
+        if (algorithm == DTB_ALGORITHM_GRADIENT) {
+            launch_gradient<T>(d_desc, d_tile_vol, total_tiles, grid, stream, prof ? d_flags + j : nullptr);
+            if (prof) cudaEventRecord(evs[j + 1], stream);
+            ++j;
+        }
+        launch_trial<T>(mode, d_desc, d_tile_vol, total_tiles, grid, stream, prof ? d_flags + j : nullptr);
+        if (prof) cudaEventRecord(evs[j + 1], stream);
+        ++j;
+    }
+    cudaError_t cap = cudaStreamEndCapture(stream, &graph);
+    set_capturing(false);
+    if (cap != cudaSuccess) {
+        cudaGetLastError();
+        DTB_CUDA(cap);
+    }
+    DTB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+
+    // Host copy of the states, refreshed once per graph launch.
+    SolverState *h_states = nullptr;
+    DTB_CUDA(cudaMallocHost(&h_states, count * sizeof(SolverState)));
+    long long max_steps = 0;
+    for (int i = 0; i < count; ++i) max_steps = std::max(max_steps, 64 * (p.it_max + 2) + 4096);
+    long long steps = 0;
+    int status = DTB_OK;
+    for (;;) {
+        if (cudaGraphLaunch(exec, stream) != cudaSuccess) {
+            status = DTB_ERR_CUDA;
+            break;
+        }
+        count_launch(nk);
+        steps += K;
+        for (int i = 0; i < count; ++i)
+            cudaMemcpyAsync(&h_states[i], d_states[i], sizeof(SolverState), cudaMemcpyDeviceToHost, stream);
+        if (prof) cudaMemcpyAsync(h_flags, d_flags, nk, cudaMemcpyDeviceToHost, stream);
+        if (cudaStreamSynchronize(stream) != cudaSuccess) {
+            status = DTB_ERR_CUDA;
+            break;
+        }
+        if (prof) {
+            std::lock_guard<std::mutex> lock(g_prof_mutex);
+            for (int j = 0; j < nk; ++j) {
+                if (!h_flags[j]) continue;
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, evs[j], evs[j + 1]);
+                const int kind = (algorithm == DTB_ALGORITHM_GRADIENT && j % 2 == 0) ? PROF_GRADIENT : PROF_TRIAL;
+                g_prof.launches[kind]++;
+                g_prof.ms[kind] += ms;
+            }
+        }
+        bool all_done = true;
+        for (int i = 0; i < count; ++i) all_done &= h_states[i].done != 0;
+        if (all_done) break;
+        if (steps > max_steps) {
+            status = DTB_ERR_ARGUMENT;
+            break;
+        }
+    }
+    DTB_CUDA(cudaEventRecord(ev1, stream));
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (prof) {
+        for (auto &e : evs) cudaEventDestroy(e);
+        cudaFree(d_flags);
+        cudaFreeHost(h_flags);
+    }
+    if (status == DTB_ERR_CUDA) {
+        cudaError_t e = cudaGetLastError();
+        cudaFreeHost(h_states);
+        DTB_CUDA(e != cudaSuccess ? e : cudaErrorUnknown);
+    }
+    if (status != DTB_OK) {
+        cudaFreeHost(h_states);
+        DTB_FAIL(status, "the solver did not terminate within its step bound");
+    }
+
+    // Results: the accepted field is field[old_buf]; move it into the
+    // caller's buffer when it is the second one.
+    for (int i = 0; i < count; ++i) {
+        const SolverState &s = h_states[i];
+        if (s.old_buf == 1)
+            DTB_CUDA(cudaMemcpyAsync(desc[i].field[0], desc[i].field[1], 3 * (size_t) desc[i].g.cs * sizeof(T),
+                                     cudaMemcpyDeviceToDevice, stream));
+    }
+    DTB_CUDA(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    if (stats) {
+        for (int i = 0; i < count; ++i) {
+            const SolverState &s = h_states[i];
+            dtb_solve_stats &o = stats[i];
+            o.iterations = s.it;
+            o.trials = s.trials;
+            o.gradients = s.gradients;
+            o.reason = s.reason;
+            o.precision = precision;
+            o.error = s.ret_E;
+            o.max_error = s.ret_M;
+            o.cand_error = s.E;
+            o.cand_max_error = s.M;
+            o.eta = s.eta;
+            o.device_ms = ms;
+        }
+    }
+    cudaFreeHost(h_states);
+    return DTB_OK;
+}
+
+bool check_params(const dtb_params &p, const char **why) {
+    // ASSERT_PARAMETERS, src/headers/disptools.h:107-152, as errors.
+    if (!(p.alpha > 0.0)) return *why = "alpha must be positive", false;
+    if (!(p.beta > 0.0)) return *why = "beta must be positive", false;
+    if (!(p.gamma > 0.0)) return *why = "gamma must be positive", false;
+    if (!(p.delta > 0.0)) return *why = "delta must be positive", false;
+    if (!(p.zeta > 0.0)) return *why = "zeta must be positive", false;
+    if (!(p.eta > 0.0)) return *why = "eta must be positive", false;
+    if (!(p.eta_max > 0.0)) return *why = "eta_max must be positive", false;
+    if (!(p.theta >= 0.0)) return *why = "theta must be non-negative", false;
+    if (!(p.iota >= 0.0)) return *why = "iota must be non-negative", false;
+    if (!(p.tolerance >= 0.0)) return *why = "tolerance must be non-negative", false;
+    if (!(p.epsilon > 0.0)) return *why = "epsilon must be positive", false;
+    if (p.it_max < 0) return *why = "it_max must be non-negative", false;
+    return true;
+}
+
+// Host-array solve: upload (converting to T), solve on the device, download.
+template <typename T>
+int solve_host(int algorithm, int count, const dtb_volume *vols, const dtb_params &p, dtb_solve_stats *stats,
+               int precision) {
+    cudaStream_t stream;
+    DTB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    struct Own {
+        std::vector<void *> ptrs;
+        cudaStream_t s;
+        ~Own() {
+            for (void *q : ptrs) cudaFree(q);
+            cudaStreamDestroy(s);
+        }
+    } own{{}, stream};
+    std::vector<DevVol<T>> dv(count);
+    size_t stage_elems = 0;
+    for (int i = 0; i < count; ++i) stage_elems = std::max(stage_elems, 3 * vols[i].nx * vols[i].ny * vols[i].nz);
+    double *stage = nullptr;
+    if (!std::is_same<T, double>::value) {
+        if (cudaMalloc(&stage, stage_elems * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            DTB_FAIL(DTB_ERR_ALLOC, "cannot allocate the staging buffer");
+        }
+        own.ptrs.push_back(stage);
+    }
+    for (int i = 0; i < count; ++i) {
+        const dtb_volume &v = vols[i];
+        const size_t N = v.nx * v.ny * v.nz;
+        T *field = nullptr, *Jt = nullptr;
+        uint8_t *mask = nullptr;
+        if (cudaMalloc(&field, 3 * N * sizeof(T)) != cudaSuccess || (own.ptrs.push_back(field), false) ||
+            cudaMalloc(&Jt, N * sizeof(T)) != cudaSuccess || (own.ptrs.push_back(Jt), false) ||
+            cudaMalloc(&mask, N) != cudaSuccess || (own.ptrs.push_back(mask), false)) {
+            cudaGetLastError();
+            DTB_FAIL(DTB_ERR_ALLOC, "cannot allocate device buffers for the volume");
+        }
+        if (std::is_same<T, double>::value) {
+            DTB_CUDA(cudaMemcpyAsync(field, v.field, 3 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+            DTB_CUDA(cudaMemcpyAsync(Jt, v.J, N * sizeof(double), cudaMemcpyHostToDevice, stream));
+        } else {
+            DTB_CUDA(cudaMemcpyAsync(stage, v.field, 3 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
+            DTB_CUDA(launch_convert<T>(stage, 1, field, 3 * (long long) N, stream));
+            DTB_CUDA(cudaMemcpyAsync(stage, v.J, N * sizeof(double), cudaMemcpyHostToDevice, stream));
+            DTB_CUDA(launch_convert<T>(stage, 1, Jt, (long long) N, stream));
+        }
+        static_assert(sizeof(bool) == 1, "bool must be one byte");
+        DTB_CUDA(cudaMemcpyAsync(mask, v.mask, N, cudaMemcpyHostToDevice, stream));
+        dv[i] = DevVol<T>{make_geom(v.nx, v.ny, v.nz, v.dx, v.dy, v.dz), Jt, mask, field};
+    }
+    int rc = solve_device<T>(algorithm, dv, p, stats, precision, stream);
+    if (rc != DTB_OK) return rc;
+    for (int i = 0; i < count; ++i) {
+        const dtb_volume &v = vols[i];
+        const size_t N = v.nx * v.ny * v.nz;
+        if (std::is_same<T, double>::value) {
+            DTB_CUDA(cudaMemcpyAsync(v.field, dv[i].field, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        } else {
+            DTB_CUDA(launch_to_double<T>(dv[i].field, stage, 3 * (long long) N, stream));
+            DTB_CUDA(cudaMemcpyAsync(v.field, stage, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        }
+        DTB_CUDA(cudaStreamSynchronize(stream));
+    }
+    return DTB_OK;
+}
+
+int check_volumes(int count, const dtb_volume *vols) {
+    if (count < 1 || !vols) DTB_FAIL(DTB_ERR_ARGUMENT, "no volumes");
+    for (int i = 0; i < count; ++i) {
+        const dtb_volume &v = vols[i];
+        if (!valid_dims(v.nx, v.ny, v.nz)) DTB_FAIL(DTB_ERR_ARGUMENT, "every axis needs at least 3 voxels");
+        if (!v.J || !v.mask || !v.field) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+        if (!(v.dx > 0.0 && v.dy > 0.0 && v.dz > 0.0)) DTB_FAIL(DTB_ERR_ARGUMENT, "spacing must be positive");
+    }
+    return DTB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Explicit entry points.
+// ---------------------------------------------------------------------------
+extern "C" int dtb_generate_displacement_batched(int algorithm, int precision, int count,
+                                                 const dtb_volume *volumes, const dtb_params *params,
+                                                 dtb_solve_stats *stats) {
+    disptools_clear_error();
+    if (algorithm != DTB_ALGORITHM_GRADIENT && algorithm != DTB_ALGORITHM_GREEDY)
+        DTB_FAIL(DTB_ERR_ARGUMENT, "invalid algorithm");
+    if (precision != DTB_PRECISION_MIXED && precision != DTB_PRECISION_FP64)
+        DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+    if (!params) DTB_FAIL(DTB_ERR_ARGUMENT, "null parameters");
+    const char *why = nullptr;
+    if (!check_params(*params, &why)) DTB_FAIL(DTB_ERR_ARGUMENT, why);
+    int rc = check_volumes(count, volumes);
+    if (rc != DTB_OK) return rc;
+    if (precision == DTB_PRECISION_FP64) return solve_host<double>(algorithm, count, volumes, *params, stats, precision);
+    return solve_host<float>(algorithm, count, volumes, *params, stats, precision);
+}
+
+extern "C" int dtb_generate_displacement(int algorithm, int precision, size_t nx, size_t ny, size_t nz, double dx,
+                                         double dy, double dz, const double *J, const bool *mask,
+                                         const dtb_params *params, double *field, dtb_solve_stats *stats) {
+    const dtb_volume v = {nx, ny, nz, dx, dy, dz, J, mask, field};
+    return dtb_generate_displacement_batched(algorithm, precision, 1, &v, params, stats);
+}
+
+extern "C" int dtb_generate_displacement_batched_device(int algorithm, int precision, int count,
+                                                        const dtb_device_volume *volumes,
+                                                        const dtb_params *params, dtb_solve_stats *stats,
+                                                        void *stream) {
+    disptools_clear_error();
+    if (algorithm != DTB_ALGORITHM_GRADIENT && algorithm != DTB_ALGORITHM_GREEDY)
+        DTB_FAIL(DTB_ERR_ARGUMENT, "invalid algorithm");
+    if (precision != DTB_PRECISION_MIXED && precision != DTB_PRECISION_FP64)
+        DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+    if (!params || count < 1 || !volumes) DTB_FAIL(DTB_ERR_ARGUMENT, "null argument");
+    const char *why = nullptr;
+    if (!check_params(*params, &why)) DTB_FAIL(DTB_ERR_ARGUMENT, why);
+    for (int i = 0; i < count; ++i) {
+        const dtb_device_volume &v = volumes[i];
+        if (!valid_dims(v.nx, v.ny, v.nz)) DTB_FAIL(DTB_ERR_ARGUMENT, "every axis needs at least 3 voxels");
+        if (!v.J || !v.mask || !v.field) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+        if (!(v.dx > 0.0 && v.dy > 0.0 && v.dz > 0.0)) DTB_FAIL(DTB_ERR_ARGUMENT, "spacing must be positive");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == DTB_PRECISION_FP64) {
+        std::vector<DevVol<double>> dv(count);
+        for (int i = 0; i < count; ++i) {
+            const dtb_device_volume &v = volumes[i];
+            dv[i] = DevVol<double>{make_geom(v.nx, v.ny, v.nz, v.dx, v.dy, v.dz), static_cast<const double *>(v.J),
+                                   static_cast<const uint8_t *>(v.mask), static_cast<double *>(v.field)};
+        }
+        return solve_device<double>(algorithm, dv, *params, stats, precision, s);
+    }
+    std::vector<DevVol<float>> dv(count);
+    for (int i = 0; i < count; ++i) {
+        const dtb_device_volume &v = volumes[i];
+        dv[i] = DevVol<float>{make_geom(v.nx, v.ny, v.nz, v.dx, v.dy, v.dz), static_cast<const float *>(v.J),
+                              static_cast<const uint8_t *>(v.mask), static_cast<float *>(v.field)};
+    }
+    return solve_device<float>(algorithm, dv, *params, stats, precision, s);
+}
+
+// ---------------------------------------------------------------------------
+// Reference-named solver entry points (FLOATING = double).
+// ---------------------------------------------------------------------------
+static void reference_solve(int algorithm, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+                            const double *J, const bool *mask, double epsilon, double tolerance, double eta,
+                            double eta_max, double alpha, double beta, double gamma, double delta, double zeta,
+                            double theta, double iota, bool strict, size_t it_max, double *field) {
+    dtb_params p;
+    p.epsilon = epsilon;
+    p.tolerance = tolerance;
+    p.eta = eta;
+    p.eta_max = eta_max;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.gamma = gamma;
+    p.delta = delta;
+    p.zeta = zeta;
+    p.theta = theta;
+    p.iota = iota;
+    p.strict = strict ? 1 : 0;
+    p.it_max = (long long) it_max;
+    dtb_generate_displacement(algorithm, g_default_precision, nx, ny, nz, dx, dy, dz, J, mask, &p, field, nullptr);
+}
+
+extern "C" void generate_displacement_gradient_cuda(
+    const size_t nx, const size_t ny, const size_t nz, const double dx, const double dy, const double dz,
+    const double *J, const bool *mask, const double epsilon, const double tolerance, double eta,
+    const double eta_max, const double alpha, const double beta, const double gamma, const double delta,
+    const double zeta, const double theta, const double iota, const bool strict, const size_t it_max,
+    double *field) {
+    reference_solve(DTB_ALGORITHM_GRADIENT, nx, ny, nz, dx, dy, dz, J, mask, epsilon, tolerance, eta, eta_max, alpha,
+                    beta, gamma, delta, zeta, theta, iota, strict, it_max, field);
+}
+
+extern "C" void generate_displacement_greedy_cuda(
+    const size_t nx, const size_t ny, const size_t nz, const double dx, const double dy, const double dz,
+    const double *J, const bool *mask, const double epsilon, const double tolerance, double eta,
+    const double eta_max, const double alpha, const double beta, const double gamma, const double delta,
+    const double zeta, const double theta, const double iota, const bool strict, const size_t it_max,
+    double *field) {
+    reference_solve(DTB_ALGORITHM_GREEDY, nx, ny, nz, dx, dy, dz, J, mask, epsilon, tolerance, eta, eta_max, alpha,
+                    beta, gamma, delta, zeta, theta, iota, strict, it_max, field);
+}
+
+// ---------------------------------------------------------------------------
+// Jacobian (device pointers) and its adjoint.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    const int bz = pick_bz(g.nz);
+    const int ntiles = ((g.nx + BX - 1) / BX) * ((g.ny + BY - 1) / BY) * ((g.nz + bz - 1) / bz);
+    char *base = nullptr;
+    int rc = workspace(1024 + sizeof(VolumeDesc<T>) + (size_t) ntiles * sizeof(int), &base);
+    if (rc != DTB_OK) return rc;
+    Carve cv{base};
+    VolumeDesc<T> *d_desc = cv.take<VolumeDesc<T>>(1);
+    int *d_tv = cv.take<int>(ntiles);
+    VolumeDesc<T> d;
+    std::memset(&d, 0, sizeof d);
+    d.g = g;
+    d.field[0] = const_cast<T *>(field);
+    d.jout = J;
+    d.tiles_x = (g.nx + BX - 1) / BX;
+    d.tiles_y = (g.ny + BY - 1) / BY;
+    d.tiles_z = (g.nz + bz - 1) / bz;
+    d.tile_begin = 0;
+    d.ntiles = ntiles;
+    d.bz = bz;
+    DTB_CUDA(cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s));
+    DTB_CUDA(cudaMemsetAsync(d_tv, 0, (size_t) ntiles * sizeof(int), s));
+    DTB_CUDA(launch_trial<T>(MODE_JAC, d_desc, d_tv, ntiles, ntiles, s));
+    // The descriptor lives in the shared workspace: finish before releasing it.
+    DTB_CUDA(cudaStreamSynchronize(s));
+    return DTB_OK;
+}
+
+template <typename T>
+int adjoint_device_impl(const Geom &g, const T *field, const T *gJ, T *gout, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    char *base = nullptr;
+    int rc = workspace(9 * (size_t) g.cs * sizeof(T) + 256, &base);
+    if (rc != DTB_OK) return rc;
+    T *W = reinterpret_cast<T *>(base);
+    DTB_CUDA(launch_adjoint<T>(g, field, gJ, W, gout, s));
+    DTB_CUDA(cudaStreamSynchronize(s));
+    return DTB_OK;
+}
+
+}  // namespace
+
+extern "C" int dtb_jacobian_device(int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy,
+                                   double dz, const void *field, void *J, void *stream) {
+    disptools_clear_error();
+    if (!valid_dims(nx, ny, nz)) DTB_FAIL(DTB_ERR_ARGUMENT, "every axis needs at least 3 voxels");
+    if (!field || !J) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+    if (order != 4 && order != 2) DTB_FAIL(DTB_ERR_ARGUMENT, "order must be 4 or 2");
+    const Geom g = make_geom(nx, ny, nz, dx, dy, dz, order);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == DTB_PRECISION_FP64)
+        return jacobian_device_impl<double>(g, static_cast<const double *>(field), static_cast<double *>(J), s);
+    if (precision == DTB_PRECISION_MIXED)
+        return jacobian_device_impl<float>(g, static_cast<const float *>(field), static_cast<float *>(J), s);
+    DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
+extern "C" int dtb_jacobian_adjoint_device(int precision, int order, size_t nx, size_t ny, size_t nz, double dx,
+                                           double dy, double dz, const void *field, const void *grad_J,
+                                           void *grad_field, void *stream) {
+    disptools_clear_error();
+    if (!valid_dims(nx, ny, nz)) DTB_FAIL(DTB_ERR_ARGUMENT, "every axis needs at least 3 voxels");
+    if (!field || !grad_J || !grad_field) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+    if (order != 4 && order != 2) DTB_FAIL(DTB_ERR_ARGUMENT, "order must be 4 or 2");
+    const Geom g = make_geom(nx, ny, nz, dx, dy, dz, order);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == DTB_PRECISION_FP64)
+        return adjoint_device_impl<double>(g, static_cast<const double *>(field), static_cast<const double *>(grad_J),
+                                           static_cast<double *>(grad_field), s);
+    if (precision == DTB_PRECISION_MIXED)
+        return adjoint_device_impl<float>(g, static_cast<const float *>(field), static_cast<const float *>(grad_J),
+                                          static_cast<float *>(grad_field), s);
+    DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
+// src/jacobian.c:7-21, on the device in FP64.
+extern "C" void jacobian_dynamic(const size_t nx, const size_t ny, const size_t nz, const double dx, const double dy,
+                                 const double dz, const double *f, double *J) {
+    disptools_clear_error();
+    if (!valid_dims(nx, ny, nz)) {
+        set_error(__LINE__, __func__, "every axis needs at least 3 voxels");
+        return;
+    }
+    const size_t N = nx * ny * nz;
+    double *df = nullptr, *dJ = nullptr;
+    if (cudaMalloc(&df, 3 * N * sizeof(double)) != cudaSuccess || cudaMalloc(&dJ, N * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(df);
+        set_error(__LINE__, __func__, "cannot allocate device buffers");
+        return;
+    }
+    cudaError_t e = cudaMemcpy(df, f, 3 * N * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && dtb_jacobian_device(DTB_PRECISION_FP64, 4, nx, ny, nz, dx, dy, dz, df, dJ, nullptr) == DTB_OK)
+        e = cudaMemcpy(J, dJ, N * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(__LINE__, __func__, cudaGetErrorString(e));
+    }
+    cudaFree(df);
+    cudaFree(dJ);
+}
+
+// src/jacobian.c:29-55, on the device.
+extern "C" void regularise(const size_t nx, const size_t ny, const size_t nz, double *J, double epsilon) {
+    disptools_clear_error();
+    const size_t N = nx * ny * nz;
+    if (N == 0) return;
+    double *dJ = nullptr;
+    if (cudaMalloc(&dJ, N * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error(__LINE__, __func__, "cannot allocate device buffers");
+        return;
+    }
+    cudaError_t e = cudaMemcpy(dJ, J, N * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_regularise<double>(dJ, (long long) N, epsilon, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(J, dJ, N * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(__LINE__, __func__, cudaGetErrorString(e));
+    }
+    cudaFree(dJ);
+}

@@ -1,0 +1,113 @@
+// Internal declarations shared by the host driver and the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "disptools_b200.h"
+
+namespace dtb {
+
+// Thread-block shape of every stencil kernel: BX threads along x (one warp,
+// coalesced rows), BY along y; each block marches a z-range of one tile.
+constexpr int BX = 32;
+constexpr int BY = 8;
+constexpr int NT = BX * BY;
+
+// Phases of the per-volume step-control state machine.
+enum Phase {
+    PH_EVAL0 = 0,   // evaluate the initial field
+    PH_SEARCH = 1,  // initial step-length search (gradient method)
+    PH_MAIN = 2,    // backtracking line search (gradient method)
+    PH_GREEDY = 3,  // greedy iterations
+};
+
+// Per-volume solver state, resident in device memory.  The last block of each
+// trial launch runs the step control on it (one thread, FP64), so no host
+// round trip is needed between trials.
+struct SolverState {
+    // parameters (reference signature order)
+    double epsilon, tolerance, eta_max, alpha, beta, gamma, delta, zeta, theta, iota;
+    long long it_max;
+    int strict;
+    int algorithm;
+    // control
+    double eta;
+    double E_last, M_last;   // error of the last accepted field; M_last for `strict`
+    double E0, M0;           // error of the initial field
+    double gn2;              // squared norm of the current gradient
+    double E, M;             // last evaluated candidate
+    double ret_E, ret_M;     // error of the field that would be returned
+    long long it, trials, gradients;
+    int phase;
+    int done;
+    int reason;
+    int old_buf;             // which field buffer holds the accepted field
+    int need_gradient;
+    int v_cur;               // greedy: which error map is the current one
+    unsigned int ticket_t;   // block counters of the trial / gradient launches
+    unsigned int ticket_g;
+};
+
+// Geometry of one volume on the device.
+struct Geom {
+    int nx, ny, nz;
+    int order;               // interior finite-difference order: 4 or 2
+    long long ys, zs, cs;    // element strides of y, z and the component
+    double ih[3];            // inverse spacing
+    double sp[3];            // spacing
+};
+
+// One volume of a launch (single solves use one).
+template <typename T>
+struct VolumeDesc {
+    Geom g;
+    T *field[2];             // ping-pong fields [3][nz][ny][nx]
+    T *grad;                 // gradient [3][nz][ny][nx], zero on the boundary
+    const T *Jt;             // target Jacobian
+    const uint8_t *mask;     // body mask
+    T *v[2];                 // greedy: error maps
+    T *jout;                 // jacobian-only launches: output map
+    SolverState *st;
+    double2 *part_t;         // per-tile partials of the trial launch (sum, max)
+    double *part_g;          // per-tile partials of the gradient launch
+    int tiles_x, tiles_y, tiles_z;
+    int tile_begin;          // first global tile index of this volume
+    int ntiles;
+    int bz;                  // planes per tile
+};
+
+enum Mode { MODE_JAC = 0, MODE_GRAD = 1, MODE_GREEDY = 2 };
+
+// Dynamic shared memory of the kernels (bytes).
+template <typename T> constexpr int trial_smem_bytes() {
+    return 5 * 3 * (BY + 4) * (BX + 4) * (int) sizeof(T);
+}
+template <typename T> constexpr int gradient_smem_bytes() {
+    return 5 * 3 * (BY + 6) * (BX + 6) * (int) sizeof(T) + 3 * 9 * (BY + 2) * (BX + 2) * (int) sizeof(T);
+}
+
+// Launch wrappers, instantiated for float and double in dt_kernels_*.cu.
+// `work_flag` (may be null) is set to 1 by a launch that did work for at
+// least one volume (profiling separates real launches from no-op ones).
+template <typename T>
+cudaError_t launch_trial(int mode, const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
+                         int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
+template <typename T>
+cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
+                            int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
+template <typename T>
+cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s);
+template <typename T>
+cudaError_t launch_convert(const void *src, int src_is_double, T *dst, long long n, cudaStream_t s);
+template <typename T>
+cudaError_t launch_to_double(const T *src, double *dst, long long n, cudaStream_t s);
+template <typename T>
+cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s);
+
+// Kernel-launch counter (host side).  Launches issued while a stream is being
+// captured are not counted; each replay of a graph counts its kernels.
+void count_launch(unsigned n = 1);
+void set_capturing(bool on);
+
+}  // namespace dtb

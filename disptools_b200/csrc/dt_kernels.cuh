@@ -1,0 +1,807 @@
+// Stencil kernels of the displacement-field generator (sm_100a).
+//
+// Included by dt_kernels_f32.cu (FP32 field and stencils; FMA contraction
+// allowed) and dt_kernels_f64.cu (FP64; compiled with -fmad=false so the
+// per-voxel arithmetic rounds exactly like the reference C library).
+//
+// Every kernel is a 2.5-D stencil: a block of BX x BY threads owns one x-y
+// tile and marches a range of z planes, keeping a ring of planes (with an
+// x-y halo) in shared memory.  Reductions are FP64 whatever the element type:
+// each tile writes one partial, and the last tile of a volume to finish (an
+// atomic ticket, no spinning) folds the partials in a fixed order and runs
+// that volume's step control.  The result is deterministic run to run.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include "dt_internal.h"
+
+namespace dtb {
+
+enum { S_FWD = 0, S_BWD = 1, S_C2 = 2, S_C4 = 3 };
+
+// Coefficients of src/headers/jacobian_macros.h:4-5.
+template <typename T> struct FD;
+template <> struct FD<double> {
+    static constexpr double two_thirds = 0.666666666666666666666666666;
+    static constexpr double one_twelfth = 0.083333333333333333333333333;
+};
+template <> struct FD<float> {
+    static constexpr float two_thirds = 0.666666666666666666666666666f;
+    static constexpr float one_twelfth = 0.083333333333333333333333333f;
+};
+
+// One-sided and central differences with the operation order of
+// src/headers/jacobian_macros.h:7-148 (values at offsets m2 m1 0 p1 p2).
+template <typename T>
+__device__ __forceinline__ T fd_fwd(T a0, T p1, T p2, T ih) {
+    return (T(-1.5) * a0 + T(2.0) * p1 - T(0.5) * p2) * ih;
+}
+template <typename T>
+__device__ __forceinline__ T fd_bwd(T a0, T m1, T m2, T ih) {
+    return (T(1.5) * a0 - T(2.0) * m1 + T(0.5) * m2) * ih;
+}
+template <typename T>
+__device__ __forceinline__ T fd_c2(T p1, T m1, T ih) {
+    return (p1 - m1) * ih * T(.5);
+}
+template <typename T>
+__device__ __forceinline__ T fd_c4(T p1, T m1, T p2, T m2, T ih) {
+    return ((p1 - m1) * FD<T>::two_thirds - (p2 - m2) * FD<T>::one_twelfth) * ih;
+}
+
+// det(I + a), first-row expansion as det3/det3j (src/headers/disptools.h:185-199).
+template <typename T>
+__device__ __forceinline__ T det_i_plus(const T a[3][3]) {
+    const T a11 = a[0][0] + T(1.0), a12 = a[0][1], a13 = a[0][2];
+    const T a21 = a[1][0], a22 = a[1][1] + T(1.0), a23 = a[1][2];
+    const T a31 = a[2][0], a32 = a[2][1], a33 = a[2][2] + T(1.0);
+    return a11 * (a22 * a33 - a23 * a32) - a12 * (a21 * a33 - a23 * a31) +
+           a13 * (a21 * a32 - a22 * a31);
+}
+
+// Scheme along each axis at voxel (x, y, z): the case analysis of
+// src/jacobian.c:70-242 stated per voxel.  Outer layer: one-sided along the
+// axes where the voxel is at 0 / n-1, central second order along the others.
+// Otherwise central second order on the penultimate layer (or everywhere
+// when order == 2), central fourth order inside.
+__device__ __forceinline__ void schemes_at(int x, int y, int z, const Geom &g, int k[3]) {
+    const int p[3] = {x, y, z};
+    const int n[3] = {g.nx, g.ny, g.nz};
+    bool outer = false, pen = false;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        outer |= (p[a] == 0) | (p[a] == n[a] - 1);
+        pen |= (p[a] == 1) | (p[a] == n[a] - 2);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (outer)
+            k[a] = p[a] == 0 ? S_FWD : (p[a] == n[a] - 1 ? S_BWD : S_C2);
+        else
+            k[a] = (g.order == 2 || pen) ? S_C2 : S_C4;
+    }
+}
+
+__device__ __forceinline__ int ring_slot(int z, int ns) {
+    int s = z % ns;
+    return s < 0 ? s + ns : s;
+}
+
+// Shared-memory ring of z planes: [NS][3][PY][PX].
+template <typename T, int PX, int PY>
+struct Ring {
+    T *base;
+    __device__ __forceinline__ T &at(int slot, int c, int ly, int lx) const {
+        return base[((slot * 3 + c) * PY + ly) * PX + lx];
+    }
+};
+
+// Derivative of component c along axis `a` with scheme k at ring cell
+// (lx, ly) of plane z (slots of z-2..z+2 in s[0..4]).
+template <typename T, int PX, int PY>
+__device__ __forceinline__ T ring_deriv(const Ring<T, PX, PY> &r, const int s[5], int c, int lx,
+                                        int ly, int a, int k, T ih) {
+    auto val = [&](int o) -> T {
+        if (a == 0) return r.at(s[2], c, ly, lx + o);
+        if (a == 1) return r.at(s[2], c, ly + o, lx);
+        return r.at(s[2 + o], c, ly, lx);
+    };
+    switch (k) {
+    case S_FWD: return fd_fwd<T>(val(0), val(1), val(2), ih);
+    case S_BWD: return fd_bwd<T>(val(0), val(-1), val(-2), ih);
+    case S_C2: return fd_c2<T>(val(1), val(-1), ih);
+    default: return fd_c4<T>(val(1), val(-1), val(2), val(-2), ih);
+    }
+}
+
+template <typename T, int PX, int PY>
+__device__ __forceinline__ void ring_matrix(const Ring<T, PX, PY> &r, const int s[5], int lx, int ly,
+                                            const int k[3], const T ih[3], T a[3][3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) a[c][ax] = ring_deriv<T, PX, PY>(r, s, c, lx, ly, ax, k[ax], ih[ax]);
+}
+
+// Per-voxel error of src/headers/error.h:128-142.
+template <typename T>
+__device__ __forceinline__ T voxel_error(T J, T Jt, bool in_mask, T tol) {
+    const T e = J - Jt;
+    if (in_mask) return e;
+    const T ae = fabs(e);
+    return ae < tol ? T(0.0) : copysign(ae - tol, e);
+}
+
+__device__ __forceinline__ bool is_normal(double x) {
+    const double a = fabs(x);
+    return a >= DBL_MIN && a <= DBL_MAX;
+}
+
+// ------------------------------------------------------------------------
+// Step control (one thread, FP64), the decision logic of
+// src/displacement_field_gradient.c:289-416 and
+// src/displacement_field_greedy.c:161-233.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void finish(SolverState *st, int reason) {
+    st->done = 1;
+    st->reason = reason;
+}
+
+__device__ inline void control_after_trial(SolverState *st, double E, double M) {
+    st->E = E;
+    st->M = M;
+    switch (st->phase) {
+    case PH_EVAL0:
+        st->E0 = E;
+        st->M0 = M;
+        st->E_last = E;
+        st->ret_E = E;
+        st->ret_M = M;
+        st->it = 1;
+        if (st->algorithm == DTB_ALGORITHM_GRADIENT) {
+            st->phase = PH_SEARCH;
+            st->need_gradient = 1;
+            st->eta *= st->alpha;  // :291
+        } else {
+            st->phase = PH_GREEDY;
+            if (st->it_max < 1) finish(st, DTB_STOP_IT_MAX);
+        }
+        break;
+    case PH_SEARCH:
+        st->trials++;
+        if (st->eta < st->eta_max && E - st->E_last > -st->gamma * st->eta * st->gn2) {  // :313
+            st->eta *= st->alpha;
+        } else {
+            st->eta /= st->alpha * st->alpha;  // :317
+            st->E_last = st->E0;               // :320-326
+            st->M_last = DBL_MAX;
+            st->phase = PH_MAIN;
+            st->it = 1;
+            if (st->it_max < 1) {
+                finish(st, DTB_STOP_IT_MAX);
+            } else {
+                // Iteration 1 recomputes the gradient of the same field with
+                // the same error map (:332-339); the stored one is identical.
+                st->eta *= st->alpha;  // :342-343
+                st->eta = st->eta > st->eta_max ? st->eta_max : st->eta;
+            }
+        }
+        break;
+    case PH_MAIN: {
+        st->trials++;
+        const bool eta_good = st->eta >= st->iota;  // :366-374
+        const bool ag = E - st->E_last > -st->gamma * st->eta * st->gn2;
+        const bool sc = st->strict && M > st->M_last;
+        if (eta_good && (ag || sc)) {
+            st->eta *= st->beta;
+            break;
+        }
+        if (!is_normal(E)) finish(st, DTB_STOP_ERROR_EXPLODED);  // :387-410
+        else if (st->eta < st->iota) finish(st, DTB_STOP_ETA);
+        else if (1.0 - E / st->E_last < st->theta) finish(st, DTB_STOP_THETA);
+        else if (!is_normal(M)) finish(st, DTB_STOP_MAX_EXPLODED);
+        else if (M < st->epsilon) finish(st, DTB_STOP_EPSILON);
+        else {
+            st->E_last = E;  // :413-415
+            st->M_last = M;
+            st->ret_E = E;
+            st->ret_M = M;
+            st->old_buf ^= 1;
+            st->it++;
+            if (st->it > st->it_max) {
+                finish(st, DTB_STOP_IT_MAX);
+            } else {
+                st->need_gradient = 1;
+                st->eta *= st->alpha;
+                st->eta = st->eta > st->eta_max ? st->eta_max : st->eta;
+            }
+        }
+        break;
+    }
+    case PH_GREEDY:
+        st->trials++;
+        st->v_cur ^= 1;  // the error map just written is the current one, accepted or not
+        if (!is_normal(E)) finish(st, DTB_STOP_ERROR_EXPLODED);  // :193-196
+        else if (E >= st->E_last) {                               // :198-213
+            st->eta *= st->beta;
+            if (st->eta < st->iota) finish(st, DTB_STOP_ETA);
+        } else if (1.0 - E / st->E_last < st->theta) finish(st, DTB_STOP_THETA);
+        else if (!is_normal(M)) finish(st, DTB_STOP_MAX_EXPLODED);
+        else if (M < st->epsilon) finish(st, DTB_STOP_EPSILON);
+        else {
+            st->E_last = E;
+            st->ret_E = E;
+            st->ret_M = M;
+            st->old_buf ^= 1;
+            st->it++;
+            if (st->it > st->it_max) finish(st, DTB_STOP_IT_MAX);
+        }
+        break;
+    }
+}
+
+// ------------------------------------------------------------------------
+// Block reductions (deterministic: shuffles and a fixed tree).
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Returns (sum, max) of the block in thread 0.
+__device__ __forceinline__ double2 block_reduce(double s, double m, double *red) {
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    s = warp_sum(s);
+    m = warp_max(m);
+    if ((tid & 31) == 0) {
+        red[tid >> 5] = s;
+        red[NT / 32 + (tid >> 5)] = m;
+    }
+    __syncthreads();
+    double2 r = make_double2(0.0, 0.0);
+    if (tid < 32) {
+        s = tid < NT / 32 ? red[tid] : 0.0;
+        m = tid < NT / 32 ? red[NT / 32 + tid] : 0.0;
+        s = warp_sum(s);
+        m = warp_max(m);
+        r = make_double2(s, m);
+    }
+    __syncthreads();
+    return r;
+}
+
+// Publishes a tile partial and returns true in every thread of the block
+// that finished the volume's last tile.  Thread 0 holds `mine`.
+__device__ __forceinline__ bool publish_partial(unsigned int *ticket, int ntiles, int *s_flag) {
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    if (tid == 0) {
+        __threadfence();
+        const unsigned int t = atomicAdd(ticket, 1u);
+        *s_flag = (t == (unsigned int) (ntiles - 1));
+    }
+    __syncthreads();
+    const bool last = *s_flag;
+    if (last) __threadfence();
+    return last;
+}
+
+template <typename T>
+__device__ __forceinline__ T ldcg(const T *p) {
+    return __ldcg(p);
+}
+__device__ __forceinline__ int ldcg_int(const int *p) { return __ldcg(p); }
+
+// ------------------------------------------------------------------------
+// Trial / evaluation / Jacobian kernel.
+//
+// MODE_JAC:    J = det(I + grad f) of field[0] into jout.
+// MODE_GRAD:   phase EVAL0 evaluates field[old]; otherwise the candidate
+//              field[old] - eta * grad is formed on the fly, written to
+//              field[1-old] and evaluated (the move_field + jacobian +
+//              compute_error passes of the reference, fused).
+// MODE_GREEDY: phase EVAL0 evaluates field[old] and stores its error map;
+//              otherwise the candidate field[old] + (eta d / 2) (v(x+e) -
+//              v(x-e)) on interior voxels (src/displacement_field_greedy.c:23-67;
+//              the boundary keeps the stale content of the new buffer) is
+//              written, evaluated and its error map stored.
+// ------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(NT) k_trial(const VolumeDesc<T> *__restrict__ vols,
+                                              const int *__restrict__ tile_vol, int total_tiles,
+                                              unsigned char *__restrict__ work_flag) {
+    constexpr int H = 2, PX = BX + 2 * H, PY = BY + 2 * H, NS = 5;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Ring<T, PX, PY> ring{reinterpret_cast<T *>(smem_raw)};
+    __shared__ double red[2 * (NT / 32)];
+    __shared__ int s_flag;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const VolumeDesc<T> &V = vols[tile_vol[tile]];
+        const Geom g = V.g;
+        SolverState *st = V.st;
+        int phase = PH_EVAL0, old_b = 0, v_cur = 0;
+        double eta = 0.0;
+        if (MODE != MODE_JAC) {
+            if (ldcg_int(&st->done)) continue;
+            phase = ldcg_int(&st->phase);
+            old_b = ldcg_int(&st->old_buf);
+            v_cur = ldcg_int(&st->v_cur);
+            eta = __ldcg(&st->eta);
+        }
+        const bool trial = MODE != MODE_JAC && phase != PH_EVAL0;
+        const int lt = tile - V.tile_begin;
+        const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
+        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
+        const int z1 = min(z0 + V.bz, g.nz);
+
+        const T *src = MODE == MODE_JAC ? V.field[0] : V.field[old_b];
+        T *dst = V.field[old_b ^ 1];
+        const T *gp = V.grad;
+        const T *vlast = V.v[v_cur];
+        T *vout = MODE == MODE_GREEDY ? V.v[trial ? v_cur ^ 1 : v_cur] : nullptr;
+        const T eta_t = (T) eta;
+        // src/displacement_field_greedy.c:36-38
+        const T dd0 = (T) (eta * g.sp[0] * .5), dd1 = (T) (eta * g.sp[1] * .5), dd2 = (T) (eta * g.sp[2] * .5);
+        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+        const T tol = (T) (MODE == MODE_JAC ? 0.0 : st->tolerance);
+
+        // Fill ring slot of plane zq (tile + halo 2), forming the candidate.
+        auto load_plane = [&](int zq) {
+            const int slot = ring_slot(zq, NS);
+            const bool zin = zq >= 0 && zq < g.nz;
+            const bool zcore = zq >= z0 && zq < z1;
+            for (int i = tid; i < 3 * PY * PX; i += NT) {
+                const int c = i / (PY * PX);
+                const int r = i - c * (PY * PX);
+                const int ly = r / PX, lx = r - ly * PX;
+                const int gx = x0 - H + lx, gy = y0 - H + ly;
+                T val = T(0);
+                if (zin && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny) {
+                    const long long so = (long long) zq * g.zs + (long long) gy * g.ys + gx;
+                    const long long off = c * g.cs + so;
+                    const bool core = zcore && lx >= H && lx < H + BX && ly >= H && ly < H + BY;
+                    if (!trial) {
+                        val = src[off];
+                    } else if (MODE == MODE_GRAD) {
+                        val = src[off] - eta_t * gp[off];  // src/displacement_field_gradient.c:169-171
+                        if (core) dst[off] = val;
+                    } else {
+                        const bool interior = gx >= 1 && gx < g.nx - 1 && gy >= 1 && gy < g.ny - 1 &&
+                                              zq >= 1 && zq < g.nz - 1;
+                        if (interior) {
+                            const long long stc = c == 0 ? 1 : (c == 1 ? g.ys : g.zs);
+                            const T ddc = c == 0 ? dd0 : (c == 1 ? dd1 : dd2);
+                            val = src[off] + ddc * (vlast[so + stc] - vlast[so - stc]);
+                            if (core) dst[off] = val;
+                        } else {
+                            val = dst[off];
+                        }
+                    }
+                }
+                ring.at(slot, c, ly, lx) = val;
+            }
+        };
+
+        for (int zq = z0 - 2; zq < z0 + 2; ++zq) load_plane(zq);
+
+        const int x = x0 + tx, y = y0 + ty;
+        const bool in_xy = x < g.nx && y < g.ny;
+        double acc_s = 0.0, acc_m = 0.0;
+        for (int z = z0; z < z1; ++z) {
+            load_plane(z + 2);
+            __syncthreads();
+            if (in_xy) {
+                int k[3];
+                schemes_at(x, y, z, g, k);
+                const int s[5] = {ring_slot(z - 2, NS), ring_slot(z - 1, NS), ring_slot(z, NS),
+                                  ring_slot(z + 1, NS), ring_slot(z + 2, NS)};
+                T a[3][3];
+                ring_matrix<T, PX, PY>(ring, s, tx + H, ty + H, k, ih, a);
+                const T J = det_i_plus<T>(a);
+                const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
+                if (MODE == MODE_JAC) {
+                    V.jout[so] = J;
+                } else {
+                    const bool m = V.mask[so] != 0;
+                    const T vv = voxel_error<T>(J, V.Jt[so], m, tol);
+                    acc_s += (double) vv * (double) vv;
+                    const double av = fabs((double) vv);
+                    if (m && av > acc_m) acc_m = av;
+                    if (MODE == MODE_GREEDY) vout[so] = vv;
+                }
+            }
+            __syncthreads();
+        }
+
+        if (MODE != MODE_JAC) {
+            const double2 r = block_reduce(acc_s, acc_m, red);
+            if (tid == 0) V.part_t[lt] = r;
+            if (publish_partial(&st->ticket_t, V.ntiles, &s_flag)) {
+                double s = 0.0, m = 0.0;
+                for (int i = tid; i < V.ntiles; i += NT) {
+                    const double2 p = __ldcg(&V.part_t[i]);
+                    s += p.x;
+                    m = fmax(m, p.y);
+                }
+                const double2 tot = block_reduce(s, m, red);
+                if (tid == 0) {
+                    st->ticket_t = 0;
+                    control_after_trial(st, tot.x, tot.y);
+                    if (work_flag) *work_flag = 1;
+                    __threadfence();
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------
+// Gradient kernel (src/displacement_field_gradient.c:26-145).
+//
+// J and the error map of the accepted field are recomputed in the tile
+// (halo 3) instead of being read back, so the launch streams only the field,
+// the target map and the mask and writes the gradient.  For each plane the
+// kernel forms P[i][k](q) = e'(q) * minor_ik(M(q)) on the tile plus a halo
+// of one (e' the regularised error, M = I + grad u by second-order central
+// differences), keeps three planes of P, and takes
+//   g_i(p) = sum_k (-1)^(i+k) ih_k (P[i][k](p - e_k) - P[i][k](p + e_k)).
+// Boundary voxels of the gradient are never written (they stay zero).
+// ------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) k_gradient(const VolumeDesc<T> *__restrict__ vols,
+                                                 const int *__restrict__ tile_vol, int total_tiles,
+                                                 unsigned char *__restrict__ work_flag) {
+    constexpr int HU = 3, PXU = BX + 2 * HU, PYU = BY + 2 * HU, NSU = 5;
+    constexpr int PXP = BX + 2, PYP = BY + 2, NSP = 3;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Ring<T, PXU, PYU> ur{reinterpret_cast<T *>(smem_raw)};
+    T *pr = reinterpret_cast<T *>(smem_raw) + NSU * 3 * PYU * PXU;  // [NSP][9][PYP][PXP]
+    __shared__ double red[2 * (NT / 32)];
+    __shared__ int s_flag;
+    auto P = [&](int slot, int ik, int ly, int lx) -> T & {
+        return pr[((slot * 9 + ik) * PYP + ly) * PXP + lx];
+    };
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const VolumeDesc<T> &V = vols[tile_vol[tile]];
+        const Geom g = V.g;
+        SolverState *st = V.st;
+        if (ldcg_int(&st->done) || !ldcg_int(&st->need_gradient)) continue;
+        const int old_b = ldcg_int(&st->old_buf);
+        const int lt = tile - V.tile_begin;
+        const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
+        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
+        const int z1 = min(z0 + V.bz, g.nz);
+        const T *u = V.field[old_b];
+        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+        const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
+
+        auto load_plane = [&](int zq) {
+            const int slot = ring_slot(zq, NSU);
+            const bool zin = zq >= 0 && zq < g.nz;
+            for (int i = tid; i < 3 * PYU * PXU; i += NT) {
+                const int c = i / (PYU * PXU);
+                const int r = i - c * (PYU * PXU);
+                const int ly = r / PXU, lx = r - ly * PXU;
+                const int gx = x0 - HU + lx, gy = y0 - HU + ly;
+                T val = T(0);
+                if (zin && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
+                    val = u[c * g.cs + (long long) zq * g.zs + (long long) gy * g.ys + gx];
+                ur.at(slot, c, ly, lx) = val;
+            }
+        };
+
+        // P on plane zp over the tile plus a halo of one.
+        auto compute_p = [&](int zp) {
+            const int ps = ring_slot(zp, NSP);
+            const int s[5] = {ring_slot(zp - 2, NSU), ring_slot(zp - 1, NSU), ring_slot(zp, NSU),
+                              ring_slot(zp + 1, NSU), ring_slot(zp + 2, NSU)};
+            for (int i = tid; i < PYP * PXP; i += NT) {
+                const int ly = i / PXP, lx = i - ly * PXP;
+                const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
+                if (zp >= 0 && zp < g.nz && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny) {
+                    const int lxu = lx + 2, lyu = ly + 2;
+                    int k[3];
+                    schemes_at(gx, gy, zp, g, k);
+                    T a[3][3];
+                    ring_matrix<T, PXU, PYU>(ur, s, lxu, lyu, k, ih, a);
+                    const T J = det_i_plus<T>(a);
+                    const long long so = (long long) zp * g.zs + (long long) gy * g.ys + gx;
+                    const T v = voxel_error<T>(J, V.Jt[so], V.mask[so] != 0, tol);
+                    T ep = v;
+                    if (J < delta) ep += zeta * (J - delta);  // :71-88
+                    // M = I + grad u, second-order central (:13-21)
+                    T m[3][3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        m[c][0] = fd_c2<T>(ur.at(s[2], c, lyu, lxu + 1), ur.at(s[2], c, lyu, lxu - 1), ih[0]);
+                        m[c][1] = fd_c2<T>(ur.at(s[2], c, lyu + 1, lxu), ur.at(s[2], c, lyu - 1, lxu), ih[1]);
+                        m[c][2] = fd_c2<T>(ur.at(s[3], c, lyu, lxu), ur.at(s[1], c, lyu, lxu), ih[2]);
+                        m[c][c] += T(1.0);
+                    }
+#pragma unroll
+                    for (int ii = 0; ii < 3; ++ii) {
+                        const int r0 = ii == 0 ? 1 : 0, r1 = ii == 2 ? 1 : 2;
+#pragma unroll
+                        for (int kk = 0; kk < 3; ++kk) {
+                            const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
+                            P(ps, ii * 3 + kk, ly, lx) = ep * (m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int ik = 0; ik < 9; ++ik) P(ps, ik, ly, lx) = T(0);
+                }
+            }
+        };
+
+        for (int zq = z0 - 3; zq < z0 + 2; ++zq) load_plane(zq);
+        __syncthreads();
+        compute_p(z0 - 1);
+        __syncthreads();
+        load_plane(z0 + 2);
+        __syncthreads();
+        compute_p(z0);
+        __syncthreads();  // the first load of the loop reuses the slot of z0 - 2
+
+        const int x = x0 + tx, y = y0 + ty;
+        const bool interior_xy = x >= 1 && x < g.nx - 1 && y >= 1 && y < g.ny - 1;
+        double acc = 0.0;
+        for (int z = z0; z < z1; ++z) {
+            load_plane(z + 3);
+            __syncthreads();
+            compute_p(z + 1);
+            __syncthreads();
+            if (interior_xy && z >= 1 && z < g.nz - 1) {
+                const int lx = tx + 1, ly = ty + 1;
+                const int sm = ring_slot(z - 1, NSP), s0 = ring_slot(z, NSP), sp = ring_slot(z + 1, NSP);
+                T t[3][3];
+#pragma unroll
+                for (int ii = 0; ii < 3; ++ii) {
+                    t[ii][0] = ih[0] * (P(s0, ii * 3 + 0, ly, lx - 1) - P(s0, ii * 3 + 0, ly, lx + 1));
+                    t[ii][1] = ih[1] * (P(s0, ii * 3 + 1, ly - 1, lx) - P(s0, ii * 3 + 1, ly + 1, lx));
+                    t[ii][2] = ih[2] * (P(sm, ii * 3 + 2, ly, lx) - P(sp, ii * 3 + 2, ly, lx));
+                }
+                const T gx = t[0][0] - t[0][1] + t[0][2];
+                const T gy = -t[1][0] + t[1][1] - t[1][2];
+                const T gz = t[2][0] - t[2][1] + t[2][2];
+                const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
+                V.grad[so] = gx;
+                V.grad[g.cs + so] = gy;
+                V.grad[2 * g.cs + so] = gz;
+                acc += (double) (gx * gx + gy * gy + gz * gz);
+            }
+        }
+
+        const double2 r = block_reduce(acc, 0.0, red);
+        if (tid == 0) V.part_g[lt] = r.x;
+        if (publish_partial(&st->ticket_g, V.ntiles, &s_flag)) {
+            double s = 0.0;
+            for (int i = tid; i < V.ntiles; i += NT) s += __ldcg(&V.part_g[i]);
+            const double2 tot = block_reduce(s, 0.0, red);
+            if (tid == 0) {
+                st->ticket_g = 0;
+                st->gn2 = tot.x;
+                st->need_gradient = 0;
+                st->gradients++;
+                if (work_flag) *work_flag = 1;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------
+// Exact adjoint of the Jacobian stencil (for autograd).
+// Pass 1: W[c][a](p) = w(p) * cof_ca(I + A(p)) * ih_a, A the stencil matrix.
+// Pass 2: grad_c(q) = sum_a sum_t W[c][a](q - t e_a) * kappa(k_a(q - t e_a), t).
+// ------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T gload_deriv(const T *f, long long o, long long s, int k, T ih) {
+    switch (k) {
+    case S_FWD: return fd_fwd<T>(f[o], f[o + s], f[o + 2 * s], ih);
+    case S_BWD: return fd_bwd<T>(f[o], f[o - s], f[o - 2 * s], ih);
+    case S_C2: return fd_c2<T>(f[o + s], f[o - s], ih);
+    default: return fd_c4<T>(f[o + s], f[o - s], f[o + 2 * s], f[o - 2 * s], ih);
+    }
+}
+
+template <typename T>
+__global__ void k_adjoint_w(Geom g, const T *__restrict__ f, const T *__restrict__ gJ, T *__restrict__ W) {
+    const long long N = (long long) g.nx * g.ny * g.nz;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < N;
+         i += (long long) gridDim.x * blockDim.x) {
+        const int x = (int) (i % g.nx);
+        const int y = (int) ((i / g.nx) % g.ny);
+        const int z = (int) (i / ((long long) g.nx * g.ny));
+        int k[3];
+        schemes_at(x, y, z, g, k);
+        const long long o = (long long) z * g.zs + (long long) y * g.ys + x;
+        const long long st[3] = {1, g.ys, g.zs};
+        T m[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) m[c][a] = gload_deriv<T>(f + c * g.cs, o, st[a], k[a], (T) g.ih[a]) + (c == a ? T(1) : T(0));
+        const T w = gJ[o];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int c0 = a == 0 ? 1 : 0, c1 = a == 2 ? 1 : 2;
+                const T minor = m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
+                const T cof = ((c + a) & 1) ? -minor : minor;
+                W[(c * 3 + a) * N + i] = w * cof * (T) g.ih[a];
+            }
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T kappa(int k, int t) {
+    switch (k) {
+    case S_FWD: return t == 0 ? T(-1.5) : t == 1 ? T(2.0) : t == 2 ? T(-0.5) : T(0);
+    case S_BWD: return t == 0 ? T(1.5) : t == -1 ? T(-2.0) : t == -2 ? T(0.5) : T(0);
+    case S_C2: return t == 1 ? T(.5) : t == -1 ? T(-.5) : T(0);
+    default:
+        return t == 1 ? FD<T>::two_thirds : t == -1 ? -FD<T>::two_thirds
+             : t == 2 ? -FD<T>::one_twelfth : t == -2 ? FD<T>::one_twelfth : T(0);
+    }
+}
+
+template <typename T>
+__global__ void k_adjoint_gather(Geom g, const T *__restrict__ W, T *__restrict__ out) {
+    const long long N = (long long) g.nx * g.ny * g.nz;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < N;
+         i += (long long) gridDim.x * blockDim.x) {
+        const int q[3] = {(int) (i % g.nx), (int) ((i / g.nx) % g.ny), (int) (i / ((long long) g.nx * g.ny))};
+        const int n[3] = {g.nx, g.ny, g.nz};
+        const long long dstr[3] = {1, g.nx, (long long) g.nx * g.ny};  // W is dense
+        T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            for (int t = -2; t <= 2; ++t) {
+                int p[3] = {q[0], q[1], q[2]};
+                p[a] -= t;
+                if (p[a] < 0 || p[a] >= n[a]) continue;
+                int k[3];
+                schemes_at(p[0], p[1], p[2], g, k);
+                const T kp = kappa<T>(k[a], t);
+                if (kp == T(0)) continue;
+                const long long pi = i - t * dstr[a];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) acc[c] += W[(c * 3 + a) * N + pi] * kp;
+            }
+        }
+        const long long o = (long long) q[2] * g.zs + (long long) q[1] * g.ys + q[0];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) out[c * g.cs + o] = acc[c];
+    }
+}
+
+// ------------------------------------------------------------------------
+// Element-wise helpers.
+// ------------------------------------------------------------------------
+template <typename T>
+__global__ void k_convert(const void *__restrict__ src, int src_is_double, T *__restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x)
+        dst[i] = src_is_double ? (T) static_cast<const double *>(src)[i] : (T) static_cast<const float *>(src)[i];
+}
+
+template <typename T>
+__global__ void k_to_double(const T *__restrict__ src, double *__restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x)
+        dst[i] = (double) src[i];
+}
+
+// src/jacobian.c:29-55
+template <typename T>
+__global__ void k_regularise(T *__restrict__ J, long long n, T eps) {
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < n;
+         i += (long long) gridDim.x * blockDim.x)
+        if (J[i] < eps) J[i] = eps;
+}
+
+// ------------------------------------------------------------------------
+// Launch wrappers.
+// ------------------------------------------------------------------------
+inline int elementwise_grid(long long n) {
+    long long b = (n + 255) / 256;
+    return (int) (b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+template <typename T>
+cudaError_t launch_trial(int mode, const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                         cudaStream_t s, unsigned char *work_flag) {
+    constexpr int smem = trial_smem_bytes<T>();
+    const dim3 block(BX, BY);
+    // Opt in to the dynamic shared memory once per process (outside any
+    // stream capture: the first call of each kernel happens before capture).
+    static const cudaError_t attr = [] {
+        cudaError_t e = cudaFuncSetAttribute(k_trial<T, MODE_JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_trial<T, MODE_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_trial<T, MODE_GREEDY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        return e;
+    }();
+    if (attr != cudaSuccess) return attr;
+    switch (mode) {
+    case MODE_JAC: k_trial<T, MODE_JAC><<<grid, block, smem, s>>>(vols, tile_vol, total_tiles, work_flag); break;
+    case MODE_GRAD: k_trial<T, MODE_GRAD><<<grid, block, smem, s>>>(vols, tile_vol, total_tiles, work_flag); break;
+    default: k_trial<T, MODE_GREEDY><<<grid, block, smem, s>>>(vols, tile_vol, total_tiles, work_flag); break;
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                            cudaStream_t s, unsigned char *work_flag) {
+    constexpr int smem = gradient_smem_bytes<T>();
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_gradient<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr != cudaSuccess) return attr;
+    k_gradient<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles, work_flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s) {
+    const long long N = (long long) g.nx * g.ny * g.nz;
+    k_adjoint_w<T><<<elementwise_grid(N), 256, 0, s>>>(g, field, gJ, W);
+    k_adjoint_gather<T><<<elementwise_grid(N), 256, 0, s>>>(g, W, gout);
+    count_launch(2);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_convert(const void *src, int src_is_double, T *dst, long long n, cudaStream_t s) {
+    k_convert<T><<<elementwise_grid(n), 256, 0, s>>>(src, src_is_double, dst, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_to_double(const T *src, double *dst, long long n, cudaStream_t s) {
+    k_to_double<T><<<elementwise_grid(n), 256, 0, s>>>(src, dst, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s) {
+    k_regularise<T><<<elementwise_grid(n), 256, 0, s>>>(J, n, (T) eps);
+    count_launch();
+    return cudaGetLastError();
+}
+
+#define DTB_INSTANTIATE(T)                                                                                   \
+    template cudaError_t launch_trial<T>(int, const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
+                                         unsigned char *);                                                   \
+    template cudaError_t launch_gradient<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,      \
+                                            unsigned char *);                                                \
+    template cudaError_t launch_adjoint<T>(const Geom &, const T *, const T *, T *, T *, cudaStream_t);      \
+    template cudaError_t launch_convert<T>(const void *, int, T *, long long, cudaStream_t);                 \
+    template cudaError_t launch_to_double<T>(const T *, double *, long long, cudaStream_t);                  \
+    template cudaError_t launch_regularise<T>(T *, long long, double, cudaStream_t);
+
+}  // namespace dtb

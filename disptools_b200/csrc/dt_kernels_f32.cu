@@ -1,0 +1,7 @@
+// FP32 instantiation of the stencil kernels (mixed path: FP32 field and
+// stencil arithmetic, FP64 reductions and step control).
+#include "dt_kernels.cuh"
+
+namespace dtb {
+DTB_INSTANTIATE(float)
+}

@@ -1,0 +1,8 @@
+// FP64 instantiation of the stencil kernels.  This file is compiled with
+// -fmad=false: no multiply-add contraction, so every per-voxel expression
+// rounds exactly as the reference C library computes it.
+#include "dt_kernels.cuh"
+
+namespace dtb {
+DTB_INSTANTIATE(double)
+}

@@ -1,0 +1,84 @@
+"""Seeded synthetic target maps and fields (NumPy / SciPy).
+
+These stand in for data sets (the reference publishes no benchmark data):
+
+* :func:`blob_problem` — target J = clip(exp(sum of isotropic Gaussian
+  blobs), 0.7, 1.4), mask = voxels with |log J| > 0.01 dilated by 3;
+* :func:`ellipsoid_problem` — 1 to 4 ellipsoids of J in [0.80, 0.95],
+  J = 1 elsewhere, mask = ellipsoids dilated by 2;
+* :func:`smooth_field` — Gaussian-filtered white noise scaled to a maximum
+  displacement.
+
+Arrays are in the library layout: maps ``[nz, ny, nx]`` float64, masks bool,
+fields ``[3, nz, ny, nx]`` float64.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _dilate(mask: np.ndarray, radius: float) -> np.ndarray:
+    """Binary dilation by a Euclidean ball of `radius` voxels."""
+    from scipy.ndimage import distance_transform_edt
+    if not mask.any():
+        return mask.copy()
+    return distance_transform_edt(~mask) <= radius
+
+
+def blob_problem(shape=(256, 256, 256), blobs: int = 16, seed: int = 0,
+                 sigma=(8.0, 24.0), amplitude: float = 0.25):
+    """log J = sum_b A_b exp(-|x - c_b|^2 / (2 sigma_b^2)), centres uniform in
+    the grid, sigma_b ~ U(sigma), A_b ~ U(-amplitude, amplitude); J clipped to
+    [0.7, 1.4]; mask = |log J| > 0.01 dilated by 3."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    logj = np.zeros(shape)
+    z = np.arange(nz, dtype=np.float64)
+    y = np.arange(ny, dtype=np.float64)
+    x = np.arange(nx, dtype=np.float64)
+    for _ in range(blobs):
+        c = rng.uniform([0, 0, 0], [nz, ny, nx])
+        s = rng.uniform(*sigma)
+        a = rng.uniform(-amplitude, amplitude)
+        ez = np.exp(-(z - c[0]) ** 2 / (2 * s * s))
+        ey = np.exp(-(y - c[1]) ** 2 / (2 * s * s))
+        ex = np.exp(-(x - c[2]) ** 2 / (2 * s * s))
+        logj += a * ez[:, None, None] * (ey[:, None] * ex[None, :])[None]
+    J = np.clip(np.exp(logj), 0.7, 1.4)
+    mask = _dilate(np.abs(logj) > 0.01, 3.0)
+    return np.ascontiguousarray(J), np.ascontiguousarray(mask)
+
+
+def ellipsoid_problem(shape, seed: int = 0, count=None):
+    """1-4 random ellipsoids (semi-axes U(4, 20) voxels) of J ~ U(0.80, 0.95);
+    J = 1 elsewhere; mask = the ellipsoids dilated by 2."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    J = np.ones(shape)
+    inside = np.zeros(shape, bool)
+    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    for _ in range(int(count or rng.integers(1, 5))):
+        r = rng.uniform(4, 20, 3)
+        c = rng.uniform([0, 0, 0], [nz, ny, nx])
+        e = ((zz - c[0]) / r[0]) ** 2 + ((yy - c[1]) / r[1]) ** 2 + ((xx - c[2]) / r[2]) ** 2 <= 1
+        J[e] = rng.uniform(0.80, 0.95)
+        inside |= e
+    return np.ascontiguousarray(J), np.ascontiguousarray(_dilate(inside, 2.0))
+
+
+def batch_sizes(count: int = 64, low: int = 48, high: int = 192, seed: int = 0):
+    """Per-axis sizes drawn uniformly from [low, high]."""
+    rng = np.random.default_rng(seed)
+    return [tuple(int(v) for v in rng.integers(low, high + 1, 3)) for _ in range(count)]
+
+
+def smooth_field(shape, sigma: float = 6.0, max_disp: float = 3.0, seed: int = 0) -> np.ndarray:
+    """White noise N(0, 1) filtered by a Gaussian of `sigma` voxels and scaled
+    so that max |u| = max_disp; shape ``[3, *shape]``."""
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.default_rng(seed)
+    f = np.empty((3,) + tuple(shape))
+    for c in range(3):
+        f[c] = gaussian_filter(rng.standard_normal(shape), sigma, mode="wrap")
+    f *= max_disp / np.max(np.abs(f))
+    return np.ascontiguousarray(f)

@@ -1,0 +1,141 @@
+"""Device-tensor entry points and the differentiable Jacobian.
+
+PyTorch supplies device memory and the current stream; every computation is a
+kernel of ``libdisptools_b200.so`` called through the C ABI with raw device
+pointers.  Tensors must be CUDA, C-contiguous, float32 (mixed path) or
+float64 (FP64 path); fields are ``[3, nz, ny, nx]`` (or a leading batch
+dimension for :func:`jacobian`), scalar maps ``[nz, ny, nx]``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Sequence
+
+import torch
+
+from . import _native as N
+from .api import make_params
+
+
+def _precision(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return N.PRECISION_MIXED
+    if t.dtype == torch.float64:
+        return N.PRECISION_FP64
+    raise TypeError(f"expected float32 or float64, got {t.dtype}")
+
+
+def _check(t: torch.Tensor, name: str) -> None:
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def _stream(t: torch.Tensor) -> int:
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def jacobian_raw(field: torch.Tensor, spacing: Sequence[float] = (1.0, 1.0, 1.0),
+                 order: int = 4) -> torch.Tensor:
+    """Jacobian map of one ``[3, nz, ny, nx]`` device field (no autograd)."""
+    _check(field, "field")
+    if field.dim() != 4 or field.shape[0] != 3:
+        raise ValueError("field must have shape (3, nz, ny, nx)")
+    _, nz, ny, nx = field.shape
+    J = torch.empty((nz, ny, nx), dtype=field.dtype, device=field.device)
+    with torch.cuda.device(field.device):
+        N.check(N.lib.dtb_jacobian_device(_precision(field), order, nx, ny, nz,
+                                          *map(float, spacing), field.data_ptr(), J.data_ptr(),
+                                          _stream(field)))
+    return J
+
+
+def jacobian_adjoint_raw(field: torch.Tensor, grad_J: torch.Tensor,
+                         spacing: Sequence[float] = (1.0, 1.0, 1.0), order: int = 4) -> torch.Tensor:
+    """(dJ/dfield)^T grad_J for one device field."""
+    _check(field, "field")
+    grad_J = grad_J.contiguous()
+    _check(grad_J, "grad_J")
+    if grad_J.dtype != field.dtype or grad_J.shape != field.shape[1:]:
+        raise ValueError("grad_J must match the field's dtype and spatial shape")
+    _, nz, ny, nx = field.shape
+    out = torch.empty_like(field)
+    with torch.cuda.device(field.device):
+        N.check(N.lib.dtb_jacobian_adjoint_device(_precision(field), order, nx, ny, nz,
+                                                  *map(float, spacing), field.data_ptr(),
+                                                  grad_J.data_ptr(), out.data_ptr(),
+                                                  _stream(field)))
+    return out
+
+
+class JacobianFunction(torch.autograd.Function):
+    """J = det(I + grad u) with the reference stencil (src/jacobian.c:70-242);
+    the backward pass is the hand-written adjoint stencil kernel."""
+
+    @staticmethod
+    def forward(ctx, field, spacing, order):
+        ctx.save_for_backward(field)
+        ctx.spacing = tuple(float(s) for s in spacing)
+        ctx.order = order
+        if field.dim() == 5:
+            return torch.stack([jacobian_raw(f, spacing, order) for f in field])
+        return jacobian_raw(field, spacing, order)
+
+    @staticmethod
+    def backward(ctx, grad_J):
+        (field,) = ctx.saved_tensors
+        if field.dim() == 5:
+            g = torch.stack([jacobian_adjoint_raw(f, gj, ctx.spacing, ctx.order)
+                             for f, gj in zip(field, grad_J)])
+        else:
+            g = jacobian_adjoint_raw(field, grad_J, ctx.spacing, ctx.order)
+        return g, None, None
+
+
+def jacobian(field: torch.Tensor, spacing: Sequence[float] = (1.0, 1.0, 1.0),
+             order: int = 4) -> torch.Tensor:
+    """Differentiable Jacobian determinant of ``[3, nz, ny, nx]`` or
+    ``[B, 3, nz, ny, nx]`` device fields."""
+    field = field.contiguous()
+    return JacobianFunction.apply(field, tuple(spacing), order)
+
+
+def solve(J: torch.Tensor, mask: torch.Tensor, field: torch.Tensor,
+          spacing: Sequence[float] = (1.0, 1.0, 1.0), algorithm: str = "gradient", **params):
+    """Solve in place on device tensors (``field`` is the initial guess and
+    receives the result).  Returns the statistics dict."""
+    return solve_batched([(J, mask, field, spacing)], algorithm, **params)[0]
+
+
+def solve_batched(volumes, algorithm: str = "gradient", **params):
+    """Batched in-place solve of ``(J, mask, field[, spacing])`` device
+    tensors; all volumes share one dtype (float32 = mixed, float64 = FP64)."""
+    vols = list(volumes)
+    arr = (N.Volume * len(vols))()
+    prec = None
+    device = None
+    for i, v in enumerate(vols):
+        J, mask, field = v[0], v[1], v[2]
+        spacing = v[3] if len(v) > 3 else (1.0, 1.0, 1.0)
+        for t, n in ((J, "J"), (mask, "mask"), (field, "field")):
+            _check(t, n)
+        p = _precision(field)
+        if prec is not None and p != prec:
+            raise TypeError("all volumes must share one dtype")
+        prec = p
+        device = field.device
+        if J.dtype != field.dtype or mask.dtype not in (torch.bool, torch.uint8):
+            raise TypeError("J must match the field's dtype and mask must be bool")
+        nz, ny, nx = J.shape
+        if mask.shape != J.shape or field.shape != (3, nz, ny, nx):
+            raise ValueError("shapes of J, mask and field disagree")
+        arr[i] = N.Volume(nx, ny, nz, *map(float, spacing), J.data_ptr(), mask.data_ptr(),
+                          field.data_ptr())
+    p = make_params(**params)
+    stats = (N.SolveStats * len(vols))()
+    with torch.cuda.device(device):
+        N.check(N.lib.dtb_generate_displacement_batched_device(
+            N.algorithm_code(algorithm), prec, len(vols), arr, C.byref(p), stats,
+            torch.cuda.current_stream(device).cuda_stream))
+    return [s.as_dict() for s in stats]

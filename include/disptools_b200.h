@@ -1,0 +1,255 @@
+/*
+ * disptools_b200 — C ABI of the B200 (sm_100a) displacement-field generator.
+ *
+ * Drop-in for the CUDA entry points of disptools v0.4.1 and the C99 calls
+ * its `_disptools` NumPy extension binds, plus explicit-precision,
+ * statistics-returning and device-pointer entry points.
+ *
+ * All functions are `extern "C"` with plain pointers and sizes.  Arrays use
+ * the reference layout (src/headers/disptools.h:30-36 of the reference):
+ * vector fields are [3][nz][ny][nx] (component-major, x fastest), scalar maps
+ * [nz][ny][nx], masks `bool` (one byte per voxel).
+ *
+ * FLOATING at this ABI is `double` (the reference built with FLOAT_SIZE=64,
+ * which is the correctness oracle for this library).  The device arithmetic
+ * is selected separately (DTB_PRECISION_*): the default mixed path stores
+ * the field in FP32 and evaluates the stencils in FP32 while every cost
+ * reduction and every step-control decision is FP64.
+ *
+ * Errors follow the reference convention: the reference-named functions
+ * return void and set a process-wide error state that callers poll with
+ * disptools_has_error() (src/headers/disptools.h:202-264); the dtb_*
+ * functions also return 0 on success and a negative code on failure.
+ */
+#ifndef DISPTOOLS_B200_H
+#define DISPTOOLS_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Error state                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Same fields and sizes as the reference's disptools_error_state
+ * (src/headers/disptools.h:204-211). */
+typedef struct disptools_error_state {
+    bool error;
+    int line;
+    char file[512];
+    char function[512];
+    char message[1024];
+    char trace[4096];
+} disptools_error_state;
+
+/* Replaces disptools_get_error (src/headers/disptools.h:250, src/disptools.c:26-29). */
+disptools_error_state *disptools_get_error(void);
+/* Replaces disptools_has_error (src/headers/disptools.h:257, src/disptools.c:31-34). */
+bool disptools_has_error(void);
+/* Replaces disptools_clear_error (src/headers/disptools.h:264, src/disptools.c:36-43). */
+void disptools_clear_error(void);
+/* Replaces get_float_type_size (src/headers/disptools.h:289, src/disptools.c:45-48).
+ * Returns 64: FLOATING is double at this ABI. */
+int get_float_type_size(void);
+
+/* ------------------------------------------------------------------ */
+/* Reference-named entry points (FLOATING = double)                    */
+/* ------------------------------------------------------------------ */
+
+/* Replaces set_device (cuda/headers/generate_displacement.cuh:11,
+ * cuda/device.cu:4-15): false when `id` is not a valid device. */
+bool set_device(const int id);
+
+/* Replaces generate_displacement_gradient_cuda
+ * (cuda/headers/generate_displacement.cuh:39-62) with the semantics of the
+ * C library's generate_displacement_gradient
+ * (src/displacement_field_gradient.c:191-431): one-sided Jacobian at the
+ * boundary, mask-restricted maximum error, last accepted field returned.
+ * `field` is the initial guess on entry and the result on exit.  The device
+ * precision is the process default (dtb_set_default_precision). */
+void generate_displacement_gradient_cuda(
+    const size_t nx, const size_t ny, const size_t nz,
+    const double dx, const double dy, const double dz,
+    const double *J, const bool *mask,
+    const double epsilon, const double tolerance, double eta, const double eta_max,
+    const double alpha, const double beta, const double gamma, const double delta,
+    const double zeta, const double theta, const double iota,
+    const bool strict, const size_t it_max, double *field);
+
+/* Replaces generate_displacement_greedy_cuda
+ * (cuda/headers/generate_displacement.cuh:14-37) with the semantics of
+ * generate_displacement_greedy (src/displacement_field_greedy.c:85-247):
+ * the step length shrinks with eta on every rejection. */
+void generate_displacement_greedy_cuda(
+    const size_t nx, const size_t ny, const size_t nz,
+    const double dx, const double dy, const double dz,
+    const double *J, const bool *mask,
+    const double epsilon, const double tolerance, double eta, const double eta_max,
+    const double alpha, const double beta, const double gamma, const double delta,
+    const double zeta, const double theta, const double iota,
+    const bool strict, const size_t it_max, double *field);
+
+/* Replaces jacobian_dynamic (src/headers/jacobian.h:24-33,
+ * src/jacobian.c:7-21), computed on the current device in FP64. */
+void jacobian_dynamic(
+    const size_t nx, const size_t ny, const size_t nz,
+    const double dx, const double dy, const double dz,
+    const double *f, double *J);
+
+/* Replaces regularise (src/headers/jacobian.h:13-19, src/jacobian.c:29-55):
+ * J[i] = max(J[i], epsilon) in place, on the current device. */
+void regularise(const size_t nx, const size_t ny, const size_t nz,
+                double *J, double epsilon);
+
+/* ------------------------------------------------------------------ */
+/* Explicit entry points                                               */
+/* ------------------------------------------------------------------ */
+
+enum {
+    DTB_PRECISION_MIXED = 0, /* FP32 field and stencils, FP64 reductions/control */
+    DTB_PRECISION_FP64 = 1   /* FP64 everywhere */
+};
+
+enum {
+    DTB_ALGORITHM_GRADIENT = 0,
+    DTB_ALGORITHM_GREEDY = 1
+};
+
+enum {
+    DTB_OK = 0,
+    DTB_ERR_ARGUMENT = -1,
+    DTB_ERR_CUDA = -2,
+    DTB_ERR_ALLOC = -3,
+    DTB_ERR_DEVICE = -4
+};
+
+/* Why a solve stopped; the stopping conditions of
+ * src/displacement_field_gradient.c:387-410 and
+ * src/displacement_field_greedy.c:193-228. */
+enum {
+    DTB_STOP_IT_MAX = 0,
+    DTB_STOP_ERROR_EXPLODED = 1,
+    DTB_STOP_ETA = 2,
+    DTB_STOP_THETA = 3,
+    DTB_STOP_MAX_EXPLODED = 4,
+    DTB_STOP_EPSILON = 5
+};
+
+/* The 13 scalar solver parameters of the reference signature, in order
+ * (DisplacementFunction, python_c_extension/_disptools.c:62-85). */
+typedef struct dtb_params {
+    double epsilon, tolerance, eta, eta_max, alpha, beta, gamma, delta, zeta,
+        theta, iota;
+    int strict;
+    long long it_max;
+} dtb_params;
+
+/* Statistics of one solve (the reference prints these only when verbose). */
+typedef struct dtb_solve_stats {
+    long long iterations; /* loop counter when the loop ended */
+    long long trials;     /* candidate fields evaluated */
+    long long gradients;  /* gradient evaluations */
+    int reason;           /* DTB_STOP_* */
+    int precision;        /* DTB_PRECISION_* used */
+    double error;         /* total error of the returned field (FP64 sum) */
+    double max_error;     /* masked max |J - J_t| of the returned field */
+    double cand_error;    /* total error of the last evaluated candidate */
+    double cand_max_error;
+    double eta;           /* final step length */
+    double device_ms;     /* device time of the solve loop (CUDA events) */
+} dtb_solve_stats;
+
+/* Process-wide precision of the reference-named solver entry points.
+ * The initial value is DTB_PRECISION_MIXED, or DTB_PRECISION_FP64 when the
+ * environment variable DISPTOOLS_B200_PRECISION is "fp64" at load time. */
+int dtb_set_default_precision(int precision);
+int dtb_get_default_precision(void);
+
+/* One solve on the current device from host arrays, with statistics
+ * (`stats` may be NULL).  Returns DTB_OK or a DTB_ERR_* code; the error
+ * state is set as well. */
+int dtb_generate_displacement(
+    int algorithm, int precision,
+    size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+    const double *J, const bool *mask, const dtb_params *params,
+    double *field, dtb_solve_stats *stats);
+
+/* One volume of a batched solve (host arrays). */
+typedef struct dtb_volume {
+    size_t nx, ny, nz;
+    double dx, dy, dz;
+    const double *J;
+    const bool *mask;
+    double *field; /* in: initial guess, out: result */
+} dtb_volume;
+
+/* Solve `count` independent volumes of any sizes together: every device
+ * launch covers the tiles of all volumes still running, each volume keeps
+ * its own step-control state.  `stats` (may be NULL) has `count` entries. */
+int dtb_generate_displacement_batched(
+    int algorithm, int precision, int count, const dtb_volume *volumes,
+    const dtb_params *params, dtb_solve_stats *stats);
+
+/* One volume of a device-resident solve: `J` and `field` are device
+ * pointers of the element type of the precision (float for MIXED, double for
+ * FP64), `mask` a device array of one byte per voxel. */
+typedef struct dtb_device_volume {
+    size_t nx, ny, nz;
+    double dx, dy, dz;
+    const void *J;
+    const void *mask;
+    void *field; /* in: initial guess, out: result (device) */
+} dtb_device_volume;
+
+/* Batched solve of device-resident volumes on `stream` (a cudaStream_t or
+ * NULL).  Scratch memory comes from the library's device workspace. */
+int dtb_generate_displacement_batched_device(
+    int algorithm, int precision, int count, const dtb_device_volume *volumes,
+    const dtb_params *params, dtb_solve_stats *stats, void *stream);
+
+/* Jacobian determinant of a device-resident field (reference stencil and
+ * boundary rules, src/jacobian.c:70-242).  `field` is [3][nz][ny][nx] and
+ * `J` [nz][ny][nx], both device pointers of the element type of
+ * `precision` (float for MIXED, double for FP64); `order` is the interior
+ * finite-difference order, 4 (the reference default ORDER_PD) or 2;
+ * `stream` is a cudaStream_t or NULL. */
+int dtb_jacobian_device(
+    int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+    const void *field, void *J, void *stream);
+
+/* Adjoint of dtb_jacobian_device: grad_field = (dJ/dfield)^T grad_J, the
+ * exact transpose of the position-dependent stencil (fourth order inside,
+ * second order on the penultimate and outer layers).  Device pointers as
+ * above; grad_field is overwritten. */
+int dtb_jacobian_adjoint_device(
+    int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+    const void *field, const void *grad_J, void *grad_field, void *stream);
+
+/* Number of kernels this library has launched in the process (a counter
+ * kept by the host code, for benchmarks that report launch counts; each
+ * replay of a captured step graph counts the kernels it contains). */
+unsigned long long dtb_kernel_launch_count(void);
+
+/* Per-kernel profile of the solver: launches that did work and their summed
+ * device time, measured with CUDA events recorded between the kernels of the
+ * step graph while profiling is on. */
+typedef struct dtb_kernel_profile {
+    char name[32];        /* "trial" or "gradient" */
+    long long launches;
+    double total_ms;
+} dtb_kernel_profile;
+
+/* Turns profiling on or off and clears the counters. */
+int dtb_set_profiling(int on);
+/* Copies up to `max` entries into `out`; returns the number written. */
+int dtb_get_profile(dtb_kernel_profile *out, int max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DISPTOOLS_B200_H */

@@ -1,0 +1,133 @@
+"""Generate the golden fixtures of tests/golden/ from the reference C library.
+
+The reference library (disptools v0.4.1, src/*.c) is compiled from its own
+sources into oracle/_ref/ by oracle/Makefile (FLOAT_SIZE=64, ORDER_PD=4, and
+ORDER_PD=2 for the gradient check).  This script calls it through its C ABI
+(jacobian_dynamic, generate_displacement_gradient,
+generate_displacement_greedy) on seeded inputs and stores inputs and outputs
+as small .npz files.  Run it where the reference sources are available:
+
+    python tests/golden/make_golden.py
+
+Inputs are seeded synthetic data; the shapes mirror the reference's own tests
+(test/test_displacements.py:43-55 uses sin_vector_field(10);
+test/c/test_jacobian_macros.cpp:22-67 uses i*i data on a 5x6x7 grid with
+spacing (2, 3, 4)).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.oracle import Reference, build  # noqa: E402
+
+
+def sin_vector_field(n: int) -> np.ndarray:
+    """The field of disptools/drawing.py:368-390 in the library layout
+    [3, z, y, x] (all three components equal)."""
+    x = np.linspace(0, 0.5, n)
+    xx, yy, zz = np.meshgrid(x, x, x)
+    s = np.sin(xx ** 2 + yy ** 2 + zz ** 2)  # ITK array [z, y, x]
+    return np.ascontiguousarray(np.stack([s, s, s]))
+
+
+def i2_field() -> np.ndarray:
+    """data[i] = i*i over a 3 x 7 x 6 x 5 buffer (test_jacobian_macros.cpp:53-59)."""
+    nx, ny, nz = 5, 6, 7
+    i = np.arange(3 * nz * ny * nx, dtype=np.float64)
+    return (i * i).reshape(3, nz, ny, nx)
+
+
+def ball(n, c, r):
+    z, y, x = np.meshgrid(*[np.arange(n)] * 3, indexing="ij")
+    return (x - c) ** 2 + (y - c) ** 2 + (z - c) ** 2 <= r * r
+
+
+def small_problem(seed: int, shape):
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    Jt = np.ones(shape)
+    mask = np.zeros(shape, bool)
+    for _ in range(2):
+        c = rng.uniform([2, 2, 2], [nz - 3, ny - 3, nx - 3])
+        r = rng.uniform(1.5, 3.0)
+        inside = (z - c[0]) ** 2 + (y - c[1]) ** 2 + (x - c[2]) ** 2 <= r * r
+        Jt[inside] = rng.uniform(0.85, 1.15)
+        mask |= (z - c[0]) ** 2 + (y - c[1]) ** 2 + (x - c[2]) ** 2 <= (r + 1) ** 2
+    return np.ascontiguousarray(Jt), np.ascontiguousarray(mask)
+
+
+def main() -> None:
+    build(ref=True)
+    ref = Reference("ref64")
+    ref2 = Reference("ref64_pd2")
+
+    # Jacobian fixtures ---------------------------------------------------
+    rng = np.random.default_rng(0)
+    jac = {}
+    f = sin_vector_field(10)
+    jac["sin10_field"] = f
+    jac["sin10_J"] = ref.jacobian(f, (1.0, 1.0, 1.0))
+    f = i2_field()
+    jac["i2_field"] = f
+    jac["i2_J"] = ref.jacobian(f, (2.0, 3.0, 4.0))
+    for k, shape in enumerate([(3, 3, 3), (4, 5, 6), (7, 9, 11), (12, 5, 3)]):
+        f = rng.normal(scale=0.3, size=(3,) + shape)
+        sp = tuple(rng.uniform(0.5, 2.0, 3))
+        jac[f"rand{k}_field"] = f
+        jac[f"rand{k}_spacing"] = np.array(sp)
+        jac[f"rand{k}_J"] = ref.jacobian(f, sp)
+        jac[f"rand{k}_J_pd2"] = ref2.jacobian(f, sp)
+    np.savez_compressed(os.path.join(HERE, "jacobian.npz"), **jac)
+
+    # Solver fixtures (small volumes, full fields) ------------------------
+    sol = {}
+    cases = []
+    for k, (alg, shape, init, extra) in enumerate([
+        ("gradient", (12, 11, 10), False, {}),
+        ("gradient", (9, 13, 8), True, {"strict": True}),
+        ("gradient", (10, 10, 10), False, {"zeta": 100.0, "eta_max": 2.0}),
+        ("greedy", (12, 11, 10), False, {}),
+        ("greedy", (9, 13, 8), True, {}),
+    ]):
+        Jt, mask = small_problem(100 + k, shape)
+        field0 = (np.random.default_rng(200 + k).normal(scale=0.05, size=(3,) + shape)
+                  if init else np.zeros((3,) + shape))
+        params = dict(it_max=200, **extra)
+        out = ref.solve(alg, Jt, mask, field=field0, spacing=(1.0, 1.1, 0.9), **params)
+        sol[f"c{k}_Jt"] = Jt
+        sol[f"c{k}_mask"] = mask
+        sol[f"c{k}_field0"] = field0
+        sol[f"c{k}_out"] = out
+        cases.append({"name": f"c{k}", "algorithm": alg, "spacing": [1.0, 1.1, 0.9],
+                      "params": params})
+    np.savez_compressed(os.path.join(HERE, "solver.npz"), **sol)
+
+    # Config 1 (40^3 sphere): summary of the reference result -------------
+    n = 40
+    m = ball(n, 20, 10)
+    Jt = np.where(m, 1.1, 1.0)
+    out = ref.solve("gradient", Jt, m, it_max=1000)
+    Jout = ref.jacobian(out)
+    c1 = {
+        "masked_max": float(np.max(np.abs(Jout - Jt)[m])),
+        "total_error": float(np.sum(np.where(m, Jout - Jt, np.where(np.abs(Jout - Jt) < 0.2, 0.0,
+                                                                      np.sign(Jout - Jt) * (np.abs(Jout - Jt) - 0.2))) ** 2)),
+        "field_l2": float(np.sqrt(np.sum(out ** 2))),
+        "field_line": out[:, 20, 20, :].tolist(),
+    }
+    with open(os.path.join(HERE, "solver_cases.json"), "w") as fh:
+        json.dump({"cases": cases, "config1": c1}, fh, indent=1)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+"""Solver parity against the FP64 oracle (GPU)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import disptools_b200 as dt
+from tests.helpers import ball_problem, masked_max
+
+pytestmark = pytest.mark.gpu
+
+
+def _golden_case(golden, case):
+    k = case["name"]
+    s = golden["solver"]
+    return s[f"{k}_Jt"], s[f"{k}_mask"], s[f"{k}_field0"], s[f"{k}_out"]
+
+
+def test_golden_cases_fp64(golden):
+    for case in golden["cases"]["cases"]:
+        Jt, mask, f0, ref = _golden_case(golden, case)
+        out, st = dt.solve(Jt, mask, f0, spacing=tuple(case["spacing"]), algorithm=case["algorithm"],
+                           precision="fp64", **case["params"])
+        assert np.max(np.abs(out - ref)) <= 1e-10, (case, st)
+
+
+def test_golden_cases_mixed(golden, oracle):
+    for case in golden["cases"]["cases"]:
+        Jt, mask, f0, ref = _golden_case(golden, case)
+        sp = tuple(case["spacing"])
+        out, st = dt.solve(Jt, mask, f0, spacing=sp, algorithm=case["algorithm"], precision="mixed",
+                           **case["params"])
+        r_ref = masked_max(oracle.jacobian(ref, sp), Jt, mask)
+        r_out = masked_max(oracle.jacobian(out, sp), Jt, mask)
+        assert abs(r_out - r_ref) <= 1e-4, (case["name"], r_out, r_ref, st)
+
+
+def test_config1_drop_in(golden, oracle):
+    """Config 1 through the reference-named entry point and the extension."""
+    from disptools_b200 import _disptools
+    Jt, mask = ball_problem(40, 20, 10)
+    c1 = golden["cases"]["config1"]
+    args = [9.99e-4, 0.2, 0.1, 0.4, 1.2, 0.5, 0.1, 1e-3, 10.0, 1e-6, 1e-9, False, 1000]
+    dt.set_default_precision("fp64")
+    try:
+        f = np.zeros((3, 40, 40, 40))
+        _disptools.displacement((1.0, 1.0, 1.0), Jt, mask, *args, f, "gradient", 0)
+    finally:
+        dt.set_default_precision("mixed")
+    assert masked_max(oracle.jacobian(f), Jt, mask) == pytest.approx(c1["masked_max"], rel=1e-9)
+    np.testing.assert_allclose(f[:, 20, 20, :], np.array(c1["field_line"]), atol=1e-12)
+    f32 = np.zeros((3, 40, 40, 40))
+    _disptools.displacement((1.0, 1.0, 1.0), Jt, mask, *args, f32, "gradient", 0)
+    assert abs(masked_max(oracle.jacobian(f32), Jt, mask) - c1["masked_max"]) <= 1e-4
+
+
+def test_config1_stats_fp64_match_oracle(oracle):
+    Jt, mask = ball_problem(40, 20, 10)
+    ref, so = oracle.solve("gradient", Jt, mask, it_max=1000)
+    out, st = dt.solve(Jt, mask, precision="fp64", it_max=1000)
+    assert st["iterations"] == so.iterations == 123
+    assert st["trials"] == so.trials
+    assert st["reason"] == so.reason
+    assert st["max_error"] == pytest.approx(so.max_error, rel=1e-12)
+    assert st["error"] == pytest.approx(so.error, rel=1e-12)
+    assert np.max(np.abs(out - ref)) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("algorithm", ["gradient", "greedy"])
+def test_batched_equals_single(precision, algorithm):
+    rng = np.random.default_rng(11)
+    vols = []
+    for n in [(12, 17, 9), (20, 20, 20), (7, 33, 15)]:
+        Jt = 1.0 + 0.1 * rng.standard_normal(n)
+        mask = rng.random(n) < 0.3
+        vols.append((np.ascontiguousarray(Jt), np.ascontiguousarray(mask)))
+    single = [dt.solve(J, m, algorithm=algorithm, precision=precision, it_max=40) for J, m in vols]
+    batch = dt.solve_batched(vols, algorithm=algorithm, precision=precision, it_max=40)
+    for (a, sa), (b, sb) in zip(single, batch):
+        np.testing.assert_array_equal(a, b)
+        assert sa["iterations"] == sb["iterations"] and sa["trials"] == sb["trials"]
+
+
+EDGE_CASES = {
+    "minimal_3": dict(shape=(3, 3, 3)),
+    "thin_axis": dict(shape=(3, 17, 12)),
+    "empty_mask": dict(shape=(10, 11, 12), empty=True),
+    "it_max_0": dict(shape=(10, 10, 10), it_max=0),
+    "it_max_1": dict(shape=(10, 10, 10), it_max=1),
+    "strict": dict(shape=(14, 12, 10), strict=True),
+    "nan_target": dict(shape=(10, 10, 10), nan=True),
+    "anisotropic": dict(shape=(11, 13, 9), spacing=(0.5, 1.5, 2.5)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(EDGE_CASES))
+@pytest.mark.parametrize("algorithm", ["gradient", "greedy"])
+def test_edge_cases_fp64_vs_oracle(oracle, name, algorithm):
+    c = EDGE_CASES[name]
+    shape = c["shape"]
+    rng = np.random.default_rng(len(name))
+    Jt = np.ascontiguousarray(1.0 + 0.08 * rng.standard_normal(shape))
+    mask = np.zeros(shape, bool) if c.get("empty") else np.ascontiguousarray(rng.random(shape) < 0.5)
+    if c.get("nan"):
+        Jt[shape[0] // 2, shape[1] // 2, shape[2] // 2] = np.nan
+    f0 = rng.normal(scale=0.01, size=(3,) + shape)
+    sp = c.get("spacing", (1.0, 1.0, 1.0))
+    kw = dict(it_max=c.get("it_max", 60), strict=c.get("strict", False))
+    ref, so = oracle.solve(algorithm, Jt, mask, field=f0, spacing=sp, **kw)
+    out, st = dt.solve(Jt, mask, f0, spacing=sp, algorithm=algorithm, precision="fp64", **kw)
+    assert st["reason"] == so.reason and st["iterations"] == so.iterations, (st, so)
+    assert np.max(np.abs(out - ref)) <= 1e-10
+
+
+def test_device_tensor_solve_matches_host():
+    import torch
+    from disptools_b200 import torch_ops
+    Jt, mask = ball_problem(24, 12, 6, 0.9)
+    host, sh = dt.solve(Jt, mask, precision="mixed", it_max=100)
+    f = torch.zeros((3, 24, 24, 24), dtype=torch.float32, device="cuda")
+    st = torch_ops.solve(torch.from_numpy(Jt).float().cuda(), torch.from_numpy(mask).cuda(), f,
+                         it_max=100)
+    assert st["iterations"] == sh["iterations"]
+    np.testing.assert_allclose(f.cpu().numpy(), host, atol=1e-7)
+
+
+def test_full_size_256_fp64_first_iterations(oracle):
+    """Config-2 inputs at full size: a few FP64 iterations against the oracle."""
+    from disptools_b200.synthetic import blob_problem
+    Jt, mask = blob_problem((256, 256, 256), blobs=16, seed=0)
+    ref, so = oracle.solve("gradient", Jt, mask, it_max=3)
+    out, st = dt.solve(Jt, mask, precision="fp64", it_max=3)
+    assert st["trials"] == so.trials and st["reason"] == so.reason
+    assert st["error"] == pytest.approx(so.error, rel=1e-12)
+    assert np.max(np.abs(out - ref)) <= 1e-10
+
+
+def test_full_size_256_mixed_properties(oracle):
+    """Config-2 inputs at full size, mixed precision: the reported error of the
+    returned field matches an FP64 recomputation, and it decreased."""
+    from disptools_b200.synthetic import blob_problem
+    Jt, mask = blob_problem((256, 256, 256), blobs=16, seed=0)
+    out, st = dt.solve(Jt, mask, precision="mixed", it_max=25)
+    J = oracle.jacobian(out)
+    assert abs(masked_max(J, Jt, mask) - st["max_error"]) <= 1e-5
+    tot, mx, _ = oracle.compute_error(Jt, J, mask, 0.2)
+    assert tot == pytest.approx(st["error"], rel=1e-4)
+    _, s0 = dt.solve(Jt, mask, precision="mixed", it_max=0)
+    assert st["error"] < s0["error"]

@@ -1,0 +1,109 @@
+"""The differentiable Jacobian: adjoint kernel against FP64 central finite
+differences and against the reference's analytic gradient (GPU)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _affected(shape, q):
+    """Voxels whose Jacobian reads voxel q (the radius-2 cross)."""
+    out = []
+    for a in range(3):
+        for t in range(-2, 3):
+            p = list(q)
+            p[a] += t
+            if all(0 <= p[i] < shape[i] for i in range(3)) and (a == 0 or t != 0):
+                out.append(tuple(p))
+    return out
+
+
+def fd_check(field64, w, grad, probes, spacing=(1.0, 1.0, 1.0), h=1e-6, order=4):
+    """Central differences of L = sum w J(u) at `probes` (component, z, y, x),
+    differenced only over the voxels each probe affects."""
+    import torch
+    from disptools_b200 import torch_ops
+    fd = []
+    for c, z, y, x in probes:
+        f = field64.clone()
+        f[c, z, y, x] += h
+        Jp = torch_ops.jacobian_raw(f, spacing, order)
+        f[c, z, y, x] -= 2 * h
+        Jm = torch_ops.jacobian_raw(f, spacing, order)
+        idx = _affected(field64.shape[1:], (z, y, x))
+        zi, yi, xi = (torch.tensor(v, device=f.device) for v in zip(*idx))
+        fd.append(float(torch.sum(w[zi, yi, xi] * (Jp[zi, yi, xi] - Jm[zi, yi, xi]))) / (2 * h))
+    got = np.array([float(grad[c, z, y, x]) for c, z, y, x in probes])
+    return got, np.array(fd)
+
+
+def test_adjoint_fp64_vs_finite_differences():
+    import torch
+    from disptools_b200 import torch_ops
+    from disptools_b200.synthetic import smooth_field
+    f = torch.from_numpy(smooth_field((14, 12, 10), sigma=2.0, max_disp=0.8, seed=1)).cuda()
+    f.requires_grad_(True)
+    rng = np.random.default_rng(2)
+    w = torch.from_numpy(rng.standard_normal((14, 12, 10))).cuda()
+    sp = (0.9, 1.1, 1.3)
+    J = torch_ops.jacobian(f, sp)
+    (J * w).sum().backward()
+    probes = [(int(c), int(z), int(y), int(x)) for c, z, y, x in
+              zip(rng.integers(0, 3, 300), rng.integers(0, 14, 300), rng.integers(0, 12, 300),
+                  rng.integers(0, 10, 300))]
+    got, fd = fd_check(f.detach(), w, f.grad, probes, sp)
+    np.testing.assert_allclose(got, fd, rtol=1e-6, atol=1e-7)
+
+
+def test_adjoint_matches_reference_gradient(oracle_pd2):
+    """With second-order differences the cost gradient of the reference
+    (src/displacement_field_gradient.c:26-145) is the adjoint applied to
+    2 e' (e' the regularised error), on voxels away from the boundary."""
+    import torch
+    from disptools_b200 import torch_ops
+    from disptools_b200.synthetic import smooth_field
+    shape = (16, 15, 14)
+    f = smooth_field(shape, sigma=2.0, max_disp=1.5, seed=3)
+    rng = np.random.default_rng(4)
+    Jt = 1.0 + 0.1 * rng.standard_normal(shape)
+    mask = rng.random(shape) < 0.5
+    sp = (1.0, 1.2, 0.8)
+    delta, zeta = 0.9, 10.0  # a delta above some J values exercises the regulariser
+    J2 = oracle_pd2.jacobian(f, sp)
+    _, _, v = oracle_pd2.compute_error(Jt, J2, mask, 0.2)
+    g_ref, _ = oracle_pd2.gradient(f, J2, v, delta, zeta, sp)
+    ep = v + np.where(J2 < delta, zeta * (J2 - delta), 0.0)
+    g = torch_ops.jacobian_adjoint_raw(torch.from_numpy(f).cuda(), torch.from_numpy(2 * ep).cuda(),
+                                       sp, order=2).cpu().numpy()
+    inner = (slice(None),) + (slice(3, -3),) * 3
+    np.testing.assert_allclose(g[inner], g_ref[inner], rtol=1e-10, atol=1e-12)
+
+
+def test_batched_fp32_autograd_config3():
+    """4 fields of 192x224x192 (smooth noise, sigma 6, max |u| = 3): FP32
+    forward and backward; the backward checked on 1000 random voxels against
+    FP64 central differences (h = 1e-6)."""
+    import torch
+    from disptools_b200 import torch_ops
+    from disptools_b200.synthetic import smooth_field
+    shape = (192, 224, 192)
+    fields = np.stack([smooth_field(shape, 6.0, 3.0, seed=s) for s in range(4)])
+    f32 = torch.from_numpy(fields).float().cuda().requires_grad_(True)
+    rng = np.random.default_rng(9)
+    w = torch.from_numpy(rng.standard_normal((4,) + shape)).cuda()
+    J = torch_ops.jacobian(f32)
+    assert J.shape == (4,) + shape
+    (J * w.float()).sum().backward()
+    g = f32.grad
+    errs = []
+    for b in range(4):
+        f64 = torch.from_numpy(fields[b]).cuda()
+        probes = [(int(c), int(z), int(y), int(x)) for c, z, y, x in
+                  zip(rng.integers(0, 3, 250), rng.integers(0, shape[0], 250),
+                      rng.integers(0, shape[1], 250), rng.integers(0, shape[2], 250))]
+        got, fd = fd_check(f64, w[b], g[b], probes)
+        scale = np.maximum(np.abs(fd), 1.0)
+        errs.append(np.max(np.abs(got - fd) / scale))
+    assert max(errs) <= 1e-4, errs
