@@ -12,7 +12,7 @@ hand-written CUDA kernels in ``libdisptools_b200.so``; there is no CPU path.
   differentiable ``jacobian`` (torch is only needed there).
 """
 from ._native import DisptoolsError, lib  # noqa: F401  (loads the CUDA library)
-from .api import (jacobian, kernel_launch_count, regularise, set_default_precision, solve,  # noqa: F401
-                  solve_batched)
+from .api import (jacobian, kernel_launch_count, kernel_profile, regularise,  # noqa: F401
+                  set_default_precision, set_profiling, solve, solve_batched)
 
 __version__ = "0.1.0"

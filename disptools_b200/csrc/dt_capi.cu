@@ -272,6 +272,7 @@ int solve_device(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_pa
     cudaStreamSynchronize(work);
     cudaEventDestroy(ev);
     cudaStreamDestroy(work);
+    cudaGetLastError();
     return rc;
 }
 
@@ -413,18 +414,20 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     cudaGraphExec_t exec = nullptr;
     set_capturing(true);
     DTB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    // Inside a capture only cudaEventRecordExternal turns a record into an
+    // event-record node that fires on every replay.
     if (prof) {
         cudaMemsetAsync(d_flags, 0, nk, stream);
-        cudaEventRecord(evs[0], stream);
+        cudaEventRecordWithFlags(evs[0], stream, cudaEventRecordExternal);
     }
     for (int k = 0, j = 0; k < K; ++k) {
         if (algorithm == DTB_ALGORITHM_GRADIENT) {
             launch_gradient<T>(d_desc, d_tile_vol, total_tiles, grid, stream, prof ? d_flags + j : nullptr);
-            if (prof) cudaEventRecord(evs[j + 1], stream);
+            if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
             ++j;
         }
         launch_trial<T>(mode, d_desc, d_tile_vol, total_tiles, grid, stream, prof ? d_flags + j : nullptr);
-        if (prof) cudaEventRecord(evs[j + 1], stream);
+        if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
         ++j;
     }
     cudaError_t cap = cudaStreamEndCapture(stream, &graph);
@@ -442,8 +445,9 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     for (int i = 0; i < count; ++i) max_steps = std::max(max_steps, 64 * (p.it_max + 2) + 4096);
     long long steps = 0;
     int status = DTB_OK;
+    cudaError_t loop_err = cudaSuccess;
     for (;;) {
-        if (cudaGraphLaunch(exec, stream) != cudaSuccess) {
+        if ((loop_err = cudaGraphLaunch(exec, stream)) != cudaSuccess) {
             status = DTB_ERR_CUDA;
             break;
         }
@@ -452,7 +456,7 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         for (int i = 0; i < count; ++i)
             cudaMemcpyAsync(&h_states[i], d_states[i], sizeof(SolverState), cudaMemcpyDeviceToHost, stream);
         if (prof) cudaMemcpyAsync(h_flags, d_flags, nk, cudaMemcpyDeviceToHost, stream);
-        if (cudaStreamSynchronize(stream) != cudaSuccess) {
+        if ((loop_err = cudaStreamSynchronize(stream)) != cudaSuccess) {
             status = DTB_ERR_CUDA;
             break;
         }
@@ -461,7 +465,10 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
             for (int j = 0; j < nk; ++j) {
                 if (!h_flags[j]) continue;
                 float ms = 0.f;
-                cudaEventElapsedTime(&ms, evs[j], evs[j + 1]);
+                if (cudaEventElapsedTime(&ms, evs[j], evs[j + 1]) != cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
                 const int kind = (algorithm == DTB_ALGORITHM_GRADIENT && j % 2 == 0) ? PROF_GRADIENT : PROF_TRIAL;
                 g_prof.launches[kind]++;
                 g_prof.ms[kind] += ms;
@@ -475,7 +482,7 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
             break;
         }
     }
-    DTB_CUDA(cudaEventRecord(ev1, stream));
+    const cudaError_t rec_err = cudaEventRecord(ev1, stream);
     cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     if (prof) {
@@ -483,10 +490,14 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         cudaFree(d_flags);
         cudaFreeHost(h_flags);
     }
+    cudaGetLastError();  // nothing above may leave a stale error for the next call
+    if (status == DTB_OK && rec_err != cudaSuccess) {
+        status = DTB_ERR_CUDA;
+        loop_err = rec_err;
+    }
     if (status == DTB_ERR_CUDA) {
-        cudaError_t e = cudaGetLastError();
         cudaFreeHost(h_states);
-        DTB_CUDA(e != cudaSuccess ? e : cudaErrorUnknown);
+        DTB_CUDA(loop_err != cudaSuccess ? loop_err : cudaErrorUnknown);
     }
     if (status != DTB_OK) {
         cudaFreeHost(h_states);
@@ -503,9 +514,10 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     }
     DTB_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, ev0, ev1);
+    if (cudaEventElapsedTime(&ms, ev0, ev1) != cudaSuccess) ms = -1.f;
     cudaEventDestroy(ev0);
     cudaEventDestroy(ev1);
+    cudaGetLastError();
     if (stats) {
         for (int i = 0; i < count; ++i) {
             const SolverState &s = h_states[i];
