@@ -276,28 +276,95 @@ int solve_device(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_pa
     return rc;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = [] {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &ptr, 12000, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            ptr = nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(ptr);
+    }();
+    return fn;
+}
+
+// Tiled map over a pitched [comps][nz][ny][nx] array (comps = 1 gives rank 3).
+bool encode_map(CUtensorMap *out, CUtensorMapDataType type, size_t esize, const void *base, const Geom &g, int comps,
+                uint32_t box_x, uint32_t box_y) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const int rank = comps > 1 ? 4 : 3;
+    cuuint64_t dims[4] = {(cuuint64_t) g.nx, (cuuint64_t) g.ny, (cuuint64_t) g.nz, (cuuint64_t) comps};
+    cuuint64_t strides[3] = {(cuuint64_t) g.ys * esize, (cuuint64_t) g.zs * esize, (cuuint64_t) g.cs * esize};
+    cuuint32_t box[4] = {box_x, box_y, 1, (cuuint32_t) comps};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(out, type, rank, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Geometry of the solver's own buffers: rows padded to 16 elements so that
+// every row starts 16-byte aligned (a TMA requirement for all element types).
+Geom pitched(const Geom &g) {
+    Geom q = g;
+    q.ys = ((long long) g.nx + 15) / 16 * 16;
+    q.zs = q.ys * g.ny;
+    q.cs = q.zs * g.nz;
+    return q;
+}
+
+// Copies rows of a dense [rows][nx] array into/out of a pitched one.
+template <typename U>
+cudaError_t copy_rows(U *dst, size_t dpitch, const U *src, size_t spitch, size_t nx, size_t rows, cudaStream_t s) {
+    return cudaMemcpy2DAsync(dst, dpitch * sizeof(U), src, spitch * sizeof(U), nx * sizeof(U), rows,
+                             cudaMemcpyDeviceToDevice, s);
+}
+
+int num_sms() {
+    static int n = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
+    return n;
+}
+
 template <typename T>
 int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
                     dtb_solve_stats *stats, int precision, cudaStream_t stream) {
     const int count = (int) vols.size();
-    // ---- workspace layout
+    const bool gradient = algorithm == DTB_ALGORITHM_GRADIENT;
+    // ---- workspace layout: every buffer of the solve is the library's own,
+    // in the pitched layout.
     std::vector<int> tiles(count), tbegin(count);
+    std::vector<Geom> geo(count);
     int total_tiles = 0;
     size_t need = 0;
     auto align = [](size_t b) { return (b + 255) & ~size_t(255); };
     for (int i = 0; i < count; ++i) {
-        const Geom &g = vols[i].g;
+        const Geom g = pitched(vols[i].g);
+        geo[i] = g;
         const int bz = pick_bz(g.nz);
         const int t = ((g.nx + BX - 1) / BX) * ((g.ny + BY - 1) / BY) * ((g.nz + bz - 1) / bz);
         tiles[i] = t;
         tbegin[i] = total_tiles;
         total_tiles += t;
         const size_t N = (size_t) g.cs;
-        need += align(3 * N * sizeof(T));                                   // field[1]
-        need += align(3 * N * sizeof(T));                                   // gradient
-        if (algorithm == DTB_ALGORITHM_GREEDY) need += 2 * align(N * sizeof(T));  // error maps
+        need += 3 * align(3 * N * sizeof(T));       // field[0], field[1], gradient
+        need += align(N * sizeof(T)) + align(N);     // target map, mask
+        need += 2 * align(N * sizeof(T));            // e' (gradient) or error maps (greedy)
         need += align(t * sizeof(double2)) + align(t * sizeof(double));
-        need += align(sizeof(SolverState));
+        need += align(sizeof(SolverState)) + align(7 * sizeof(CUtensorMap));
     }
     need += align(count * sizeof(VolumeDesc<T>)) + align(total_tiles * sizeof(int));
 
@@ -310,27 +377,33 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     std::vector<VolumeDesc<T>> desc(count);
     std::vector<SolverState> hst(count);
     std::vector<int> tile_vol(total_tiles);
+    std::vector<CUtensorMap *> d_maps(count);
     for (int i = 0; i < count; ++i) {
-        const Geom &g = vols[i].g;
+        const Geom &g = geo[i];
+        const Geom &gu = vols[i].g;  // caller's dense layout
         const size_t N = (size_t) g.cs;
         VolumeDesc<T> &d = desc[i];
         std::memset(&d, 0, sizeof d);
         d.g = g;
-        d.field[0] = vols[i].field;
+        d.field[0] = cv.take<T>(3 * N);
         d.field[1] = cv.take<T>(3 * N);
         d.grad = cv.take<T>(3 * N);
-        d.Jt = vols[i].Jt;
-        d.mask = vols[i].mask;
-        if (algorithm == DTB_ALGORITHM_GREEDY) {
-            d.v[0] = cv.take<T>(N);
-            d.v[1] = cv.take<T>(N);
+        T *Jt = cv.take<T>(N);
+        uint8_t *mask = cv.take<uint8_t>(N);
+        d.Jt = Jt;
+        d.mask = mask;
+        T *aux0 = cv.take<T>(N), *aux1 = cv.take<T>(N);
+        if (gradient) {
+            d.ep[0] = aux0;
+            d.ep[1] = aux1;
         } else {
-            d.v[0] = d.v[1] = nullptr;
+            d.v[0] = aux0;
+            d.v[1] = aux1;
         }
-        d.jout = nullptr;
         d.part_t = cv.take<double2>(tiles[i]);
         d.part_g = cv.take<double>(tiles[i]);
         d.st = cv.take<SolverState>(1);
+        d_maps[i] = cv.take<CUtensorMap>(7);
         const int bz = pick_bz(g.nz);
         d.tiles_x = (g.nx + BX - 1) / BX;
         d.tiles_y = (g.ny + BY - 1) / BY;
@@ -360,19 +433,44 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         s.M_last = DBL_MAX;
         s.phase = PH_EVAL0;
 
+        // Inputs into the pitched layout.
+        const size_t rows = (size_t) gu.ny * gu.nz;
+        DTB_CUDA(copy_rows<T>(d.field[0], g.ys, vols[i].field, gu.ys, gu.nx, 3 * rows, stream));
+        DTB_CUDA(copy_rows<T>(Jt, g.ys, vols[i].Jt, gu.ys, gu.nx, rows, stream));
+        DTB_CUDA(copy_rows<uint8_t>(mask, g.ys, vols[i].mask, gu.ys, gu.nx, rows, stream));
         // The second field buffer starts at zero: the greedy update never
         // writes boundary voxels, so they keep the buffer's content
         // (src/displacement_field_greedy.c:43-65 with calloc'd buffers).
         DTB_CUDA(cudaMemsetAsync(d.field[1], 0, 3 * N * sizeof(T), stream));
         DTB_CUDA(cudaMemsetAsync(d.grad, 0, 3 * N * sizeof(T), stream));
-        if (d.v[0]) {
-            DTB_CUDA(cudaMemsetAsync(d.v[0], 0, N * sizeof(T), stream));
-            DTB_CUDA(cudaMemsetAsync(d.v[1], 0, N * sizeof(T), stream));
+        DTB_CUDA(cudaMemsetAsync(aux0, 0, N * sizeof(T), stream));
+        DTB_CUDA(cudaMemsetAsync(aux1, 0, N * sizeof(T), stream));
+
+        if (gradient) {
+            CUtensorMap h_maps[7];
+            const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+            bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, BX + 8, BY + 4) &&
+                      encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, BX + 8, BY + 4) &&
+                      encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, BX + 8, BY + 4) &&
+                      encode_map(&h_maps[3], ft, sizeof(T), d.ep[0], g, 1, BX + 8, BY + 4) &&
+                      encode_map(&h_maps[4], ft, sizeof(T), d.ep[1], g, 1, BX + 8, BY + 4) &&
+                      encode_map(&h_maps[5], ft, sizeof(T), Jt, g, 1, BX, BY) &&
+                      encode_map(&h_maps[6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, g, 1, BX, BY);
+            if (!ok) DTB_FAIL(DTB_ERR_CUDA, "cannot encode the TMA descriptors (cuTensorMapEncodeTiled)");
+            DTB_CUDA(cudaMemcpyAsync(d_maps[i], h_maps, sizeof h_maps, cudaMemcpyHostToDevice, stream));
+            d.tm_field[0] = d_maps[i] + 0;
+            d.tm_field[1] = d_maps[i] + 1;
+            d.tm_grad = d_maps[i] + 2;
+            d.tm_ep[0] = d_maps[i] + 3;
+            d.tm_ep[1] = d_maps[i] + 4;
+            d.tm_Jt = d_maps[i] + 5;
+            d.tm_mask = d_maps[i] + 6;
+            // The host copy of the maps must outlive the asynchronous copy.
+            DTB_CUDA(cudaStreamSynchronize(stream));
         }
     }
     VolumeDesc<T> *d_desc = cv.take<VolumeDesc<T>>(count);
     int *d_tile_vol = cv.take<int>(total_tiles);
-    // States are contiguous per volume but carved separately; gather them.
     std::vector<SolverState *> d_states(count);
     for (int i = 0; i < count; ++i) {
         d_states[i] = desc[i].st;
@@ -381,9 +479,20 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     DTB_CUDA(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(VolumeDesc<T>), cudaMemcpyHostToDevice, stream));
     DTB_CUDA(cudaMemcpyAsync(d_tile_vol, tile_vol.data(), total_tiles * sizeof(int), cudaMemcpyHostToDevice,
                              stream));
+    // Host vectors handed to async copies must stay alive until they ran.
+    DTB_CUDA(cudaStreamSynchronize(stream));
 
-    const int mode = algorithm == DTB_ALGORITHM_GREEDY ? MODE_GREEDY : MODE_GRAD;
-    const int grid = total_tiles;
+    // Persistent grids: as many blocks as fit on the device at once.
+    const int grid_t = gradient ? std::min(total_tiles, std::max(1, trial_tma_blocks_per_sm<T>()) * num_sms())
+                                : total_tiles;
+    const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>()) * num_sms());
+    auto launch_t = [&](unsigned char *flag) -> cudaError_t {
+        if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
+        return launch_trial<T>(MODE_GREEDY, d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
+    };
+    auto launch_g = [&](unsigned char *flag) -> cudaError_t {
+        return launch_gradient_tma<T>(d_desc, d_tile_vol, total_tiles, grid_g, stream, flag);
+    };
 
     cudaEvent_t ev0, ev1;
     DTB_CUDA(cudaEventCreate(&ev0));
@@ -392,16 +501,15 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
 
     // Evaluate the initial fields (launched once, outside the graph; this is
     // also the first launch of each kernel, which sets its attributes).
-    DTB_CUDA(launch_trial<T>(mode, d_desc, d_tile_vol, total_tiles, grid, stream));
-    if (algorithm == DTB_ALGORITHM_GRADIENT)
-        DTB_CUDA(launch_gradient<T>(d_desc, d_tile_vol, total_tiles, grid, stream));
+    DTB_CUDA(launch_t(nullptr));
+    if (gradient) DTB_CUDA(launch_g(nullptr));
 
     // Capture K steps into a graph.  With profiling on, event records are
     // captured between the kernels and every kernel gets a flag that it sets
     // when it did work.
     const int K = steps_per_graph();
     const bool prof = g_prof.on;
-    const int kernels_per_step = algorithm == DTB_ALGORITHM_GRADIENT ? 2 : 1;
+    const int kernels_per_step = gradient ? 2 : 1;
     const int nk = K * kernels_per_step;
     std::vector<cudaEvent_t> evs(prof ? nk + 1 : 0);
     unsigned char *d_flags = nullptr, *h_flags = nullptr;
@@ -421,12 +529,12 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         cudaEventRecordWithFlags(evs[0], stream, cudaEventRecordExternal);
     }
     for (int k = 0, j = 0; k < K; ++k) {
-        if (algorithm == DTB_ALGORITHM_GRADIENT) {
-            launch_gradient<T>(d_desc, d_tile_vol, total_tiles, grid, stream, prof ? d_flags + j : nullptr);
+        if (gradient) {
+            launch_g(prof ? d_flags + j : nullptr);
             if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
             ++j;
         }
-        launch_trial<T>(mode, d_desc, d_tile_vol, total_tiles, grid, stream, prof ? d_flags + j : nullptr);
+        launch_t(prof ? d_flags + j : nullptr);
         if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
         ++j;
     }
@@ -469,7 +577,7 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
                     cudaGetLastError();
                     continue;
                 }
-                const int kind = (algorithm == DTB_ALGORITHM_GRADIENT && j % 2 == 0) ? PROF_GRADIENT : PROF_TRIAL;
+                const int kind = (gradient && j % 2 == 0) ? PROF_GRADIENT : PROF_TRIAL;
                 g_prof.launches[kind]++;
                 g_prof.ms[kind] += ms;
             }
@@ -504,13 +612,17 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         DTB_FAIL(status, "the solver did not terminate within its step bound");
     }
 
-    // Results: the accepted field is field[old_buf]; move it into the
-    // caller's buffer when it is the second one.
+    // Results: the accepted field is field[old_buf]; copy it back into the
+    // caller's dense buffer.
     for (int i = 0; i < count; ++i) {
         const SolverState &s = h_states[i];
-        if (s.old_buf == 1)
-            DTB_CUDA(cudaMemcpyAsync(desc[i].field[0], desc[i].field[1], 3 * (size_t) desc[i].g.cs * sizeof(T),
-                                     cudaMemcpyDeviceToDevice, stream));
+        if (s.fault) {
+            cudaFreeHost(h_states);
+            DTB_FAIL(DTB_ERR_CUDA, "a TMA transfer did not complete within its bound");
+        }
+        const Geom &gu = vols[i].g;
+        DTB_CUDA(copy_rows<T>(vols[i].field, gu.ys, desc[i].field[s.old_buf], geo[i].ys, gu.nx,
+                              3 * (size_t) gu.ny * gu.nz, stream));
     }
     DTB_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.f;

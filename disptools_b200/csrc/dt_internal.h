@@ -1,6 +1,7 @@
 // Internal declarations shared by the host driver and the kernel files.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -47,6 +48,7 @@ struct SolverState {
     int v_cur;               // greedy: which error map is the current one
     unsigned int ticket_t;   // block counters of the trial / gradient launches
     unsigned int ticket_g;
+    int fault;               // a bounded wait gave up (reported as an error)
 };
 
 // Geometry of one volume on the device.
@@ -68,6 +70,13 @@ struct VolumeDesc {
     const uint8_t *mask;     // body mask
     T *v[2];                 // greedy: error maps
     T *jout;                 // jacobian-only launches: output map
+    T *ep[2];                // gradient method: regularised error e' of field[i]
+    // TMA descriptors (device memory) of field[0..1], grad, ep[0..1], Jt, mask
+    const CUtensorMap *tm_field[2];
+    const CUtensorMap *tm_grad;
+    const CUtensorMap *tm_ep[2];
+    const CUtensorMap *tm_Jt;
+    const CUtensorMap *tm_mask;
     SolverState *st;
     double2 *part_t;         // per-tile partials of the trial launch (sum, max)
     double *part_g;          // per-tile partials of the gradient launch
@@ -96,6 +105,16 @@ cudaError_t launch_trial(int mode, const VolumeDesc<T> *vols, const int *tile_vo
 template <typename T>
 cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
                             int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
+template <typename T>
+cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                             cudaStream_t s, unsigned char *work_flag = nullptr);
+template <typename T>
+cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                                cudaStream_t s, unsigned char *work_flag = nullptr);
+template <typename T>
+int trial_tma_blocks_per_sm();
+template <typename T>
+int gradient_tma_blocks_per_sm();
 template <typename T>
 cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s);
 template <typename T>

@@ -14,6 +14,7 @@
 
 #include <cfloat>
 #include <cstdint>
+#include <type_traits>
 
 #include "dt_internal.h"
 

@@ -1,0 +1,522 @@
+// TMA-pipelined kernels of the gradient method (sm_100a).
+//
+// Both kernels march a BX x BY tile through its z range.  One elected thread
+// streams one box per input per plane into a ring of shared-memory stages
+// with cp.async.bulk.tensor (completion on an mbarrier per stage); the other
+// threads never issue global loads for the stencil inputs.  Shared-memory
+// boxes start 4 voxels left of the tile so the innermost TMA coordinate stays
+// 16-byte aligned; planes outside the volume arrive zero-filled.
+//
+// k_trial_tma     candidate = field[old] - eta * grad (formed once per plane
+//                 in shared memory), written to field[1-old]; its Jacobian,
+//                 masked error and regularised error e' per voxel; FP64
+//                 partials and the on-device step control (last tile).
+// k_gradient_tma  g = sum_k +-ih_k (P_ik(p - e_k) - P_ik(p + e_k)) with
+//                 P_ik = e' * minor_ik(I + grad u) (second-order central
+//                 differences, src/displacement_field_gradient.c:26-145),
+//                 from field[old] and the stored e' of that field.
+#pragma once
+
+#include "dt_kernels.cuh"
+#include "dt_tma.cuh"
+
+namespace dtb {
+
+constexpr int TMA_HX = 4;               // x halo of the boxes (16-byte aligned start)
+constexpr int TMA_HY = 2;               // y halo
+constexpr int TMA_PX = BX + 2 * TMA_HX; // 40
+constexpr int TMA_PY = BY + 2 * TMA_HY; // 12
+constexpr int TMA_PLANE = TMA_PY * TMA_PX;  // elements of one component plane of a box
+
+template <typename T>
+struct TrialTmaLayout {
+    static constexpr int S = 3;  // pipeline stages
+    static constexpr int R = 6;  // candidate planes kept (z-2 .. z+2 plus the one being formed)
+    static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
+    static constexpr int JT_BYTES = BX * BY * (int) sizeof(T);
+    static constexpr int MASK_BYTES = BX * BY;
+    static constexpr int STAGE_BYTES = 2 * U_BYTES + JT_BYTES + MASK_BYTES;  // u, g, Jt, mask
+    static constexpr int RING_OFF = S * STAGE_BYTES;
+    static constexpr int BAR_OFF = RING_OFF + R * U_BYTES;
+    static constexpr int BYTES = BAR_OFF + S * 8;
+};
+
+template <typename T>
+struct GradTmaLayout {
+    static constexpr int S = 6;  // stages double as the plane ring (u, e')
+    static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
+    static constexpr int E_BYTES = TMA_PLANE * (int) sizeof(T);
+    static constexpr int STAGE_BYTES = U_BYTES + E_BYTES;
+    static constexpr int PXP = BX + 2, PYP = BY + 2;
+    static constexpr int P_OFF = S * STAGE_BYTES;  // P_x, P_y terms: [2][6][PYP][PXP]
+    static constexpr int P_BYTES = 2 * 6 * PYP * PXP * (int) sizeof(T);
+    static constexpr int BAR_OFF = P_OFF + P_BYTES;
+    static constexpr int BYTES = BAR_OFF + S * 8;
+};
+
+// TMA destinations must be 128-byte aligned in the shared window; the launch
+// asks for 128 spare bytes.
+__device__ __forceinline__ unsigned char *align_smem_128(unsigned char *p) {
+    const uint32_t a = smem_u32(p);
+    return p + ((128u - (a & 127u)) & 127u);
+}
+
+// Records a lost transfer: the volume stops with an error flag that the host
+// reports, and the calling thread waits (bounded) for the transfers of
+// iterations [from, to) that were issued but not consumed, so none lands in
+// shared memory after the block has left.
+template <int S>
+__device__ __forceinline__ void tma_fault(SolverState *st, uint64_t *bars, uint32_t kbase, int from, int to) {
+    atomicExch(&st->fault, 1);
+    atomicExch(&st->done, 1);
+    for (int j = from; j < to; ++j) {
+        const uint32_t k = kbase + j;
+        mbar_wait_bounded(&bars[k % S], (k / S) & 1u, 1u << 16);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restrict__ vols,
+                                                  const int *__restrict__ tile_vol, int total_tiles,
+                                                  unsigned char *__restrict__ work_flag) {
+    using L = TrialTmaLayout<T>;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem = align_smem_128(smem_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    T *ring = reinterpret_cast<T *>(smem + L::RING_OFF);
+    __shared__ double red[2 * (NT / 32)];
+    __shared__ int s_flag, s_ok;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+    if (tid == 0) {
+        for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const VolumeDesc<T> &V = vols[tile_vol[tile]];
+        SolverState *st = V.st;
+        if (ldcg_int(&st->done)) continue;
+        const Geom g = V.g;
+        const int phase = ldcg_int(&st->phase);
+        const int old_b = ldcg_int(&st->old_buf);
+        const double eta = __ldcg(&st->eta);
+        const bool trial = phase != PH_EVAL0;
+        const int lt = tile - V.tile_begin;
+        const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
+        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
+        const int z1 = min(z0 + V.bz, g.nz);
+        const int n_it = z1 - z0 + 4;  // candidate planes z0-2 .. z1+1
+        const CUtensorMap *tm_u = V.tm_field[old_b];
+        const CUtensorMap *tm_g = V.tm_grad;
+        T *dst = V.field[old_b ^ 1];
+        T *ep_out = V.ep[trial ? old_b ^ 1 : old_b];
+        const T eta_t = (T) eta;
+        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+        const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
+
+        int issued_n = 0;  // iterations whose loads were issued (thread 0)
+        // Issues the loads of iteration j (candidate plane z0-2+j) into its stage.
+        auto issue = [&](int j) {
+            issued_n = j + 1;
+            const uint32_t k = kbase + j;
+            const int s = k % L::S;
+            unsigned char *sb = smem + s * L::STAGE_BYTES;
+            const int q = z0 - 2 + j, ze = q - 2;
+            const bool with_target = ze >= z0 && ze < z1;
+            uint32_t bytes = L::U_BYTES + (trial ? L::U_BYTES : 0) + (with_target ? L::JT_BYTES + L::MASK_BYTES : 0);
+            mbar_arrive_expect_tx(&bars[s], bytes);
+            tma_load_4d(sb, tm_u, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
+            if (trial) tma_load_4d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
+            if (with_target) {
+                tma_load_3d(sb + 2 * L::U_BYTES, V.tm_Jt, &bars[s], x0, y0, ze);
+                tma_load_3d(sb + 2 * L::U_BYTES + L::JT_BYTES, V.tm_mask, &bars[s], x0, y0, ze);
+            }
+        };
+
+        if (tid == 0) {
+            tmap_acquire(tm_u);
+            tmap_acquire(tm_g);
+            tmap_acquire(V.tm_Jt);
+            tmap_acquire(V.tm_mask);
+            for (int j = 0; j < min(L::S, n_it); ++j) issue(j);
+        }
+
+        const int x = x0 + tx, y = y0 + ty;
+        const bool in_xy = x < g.nx && y < g.ny;
+        double acc_s = 0.0, acc_m = 0.0;
+        bool failed = false;
+        int fail_it = 0;
+        for (int it = 0; it < n_it; ++it) {
+            const uint32_t k = kbase + it;
+            const int s = k % L::S;
+            const uint32_t par = (k / L::S) & 1u;
+            if (tid == 0) s_ok = mbar_wait_bounded(&bars[s], par);
+            __syncthreads();
+            if (!s_ok) {
+                failed = true;
+                fail_it = it;
+                break;
+            }
+            mbar_try_wait(&bars[s], par);  // completed: acquire the data for this thread
+            const unsigned char *sb = smem + s * L::STAGE_BYTES;
+            const int q = z0 - 2 + it, ze = q - 2;
+            T *slot = ring + (size_t) ring_slot(q, L::R) * 3 * TMA_PLANE;
+            // Candidate plane q (tile + halo): u - eta g, vectorised.
+            {
+                const T *u = reinterpret_cast<const T *>(sb);
+                const T *gr = reinterpret_cast<const T *>(sb + L::U_BYTES);
+                constexpr int VEC = 16 / (int) sizeof(T);
+                using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+                const V4 *u4 = reinterpret_cast<const V4 *>(u);
+                const V4 *g4 = reinterpret_cast<const V4 *>(gr);
+                V4 *c4 = reinterpret_cast<V4 *>(slot);
+                for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NT) {
+                    V4 a = u4[i];
+                    if (trial) {
+                        const V4 b = g4[i];
+                        T *pa = reinterpret_cast<T *>(&a);
+                        const T *pb = reinterpret_cast<const T *>(&b);
+#pragma unroll
+                        for (int e = 0; e < VEC; ++e) pa[e] = pa[e] - eta_t * pb[e];
+                    }
+                    c4[i] = a;
+                }
+            }
+            T jt = T(0);
+            bool msk = false;
+            const bool eval = ze >= z0 && ze < z1;
+            if (eval) {
+                jt = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid];
+                msk = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid] != 0;
+            }
+            __syncthreads();
+            if (tid == 0 && it + L::S < n_it) issue(it + L::S);
+            // Store the candidate of core plane q.
+            if (trial && in_xy && q >= z0 && q < z1) {
+                const long long so = (long long) q * g.zs + (long long) y * g.ys + x;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    dst[c * g.cs + so] = slot[(c * TMA_PY + ty + TMA_HY) * TMA_PX + tx + TMA_HX];
+            }
+            if (eval && in_xy) {
+                const int sl[5] = {ring_slot(ze - 2, L::R), ring_slot(ze - 1, L::R), ring_slot(ze, L::R),
+                                   ring_slot(ze + 1, L::R), ring_slot(ze + 2, L::R)};
+                const int lx = tx + TMA_HX, ly = ty + TMA_HY;
+                T a[3][3];
+                const bool fast = x0 >= 2 && x0 + BX <= g.nx - 2 && y >= 2 && y <= g.ny - 3 && ze >= 2 &&
+                                  ze <= g.nz - 3 && g.order == 4;
+                if (fast) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const T *p = ring + ((size_t) sl[2] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
+                        const T *zm2 = ring + ((size_t) sl[0] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
+                        const T *zm1 = ring + ((size_t) sl[1] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
+                        const T *zp1 = ring + ((size_t) sl[3] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
+                        const T *zp2 = ring + ((size_t) sl[4] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
+                        a[c][0] = fd_c4<T>(p[1], p[-1], p[2], p[-2], ih[0]);
+                        a[c][1] = fd_c4<T>(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], ih[1]);
+                        a[c][2] = fd_c4<T>(*zp1, *zm1, *zp2, *zm2, ih[2]);
+                    }
+                } else {
+                    int kk[3];
+                    schemes_at(x, y, ze, g, kk);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int ax = 0; ax < 3; ++ax) {
+                            auto val = [&](int o) -> T {
+                                if (ax == 0) return ring[((size_t) sl[2] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx + o];
+                                if (ax == 1)
+                                    return ring[((size_t) sl[2] * 3 + c) * TMA_PLANE + (ly + o) * TMA_PX + lx];
+                                return ring[((size_t) sl[2 + o] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx];
+                            };
+                            T d;
+                            switch (kk[ax]) {
+                            case S_FWD: d = fd_fwd<T>(val(0), val(1), val(2), ih[ax]); break;
+                            case S_BWD: d = fd_bwd<T>(val(0), val(-1), val(-2), ih[ax]); break;
+                            case S_C2: d = fd_c2<T>(val(1), val(-1), ih[ax]); break;
+                            default: d = fd_c4<T>(val(1), val(-1), val(2), val(-2), ih[ax]); break;
+                            }
+                            a[c][ax] = d;
+                        }
+                }
+                const T J = det_i_plus<T>(a);
+                const T vv = voxel_error<T>(J, jt, msk, tol);
+                acc_s += (double) vv * (double) vv;
+                const double av = fabs((double) vv);
+                if (msk && av > acc_m) acc_m = av;
+                T ep = vv;
+                if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
+                ep_out[(long long) ze * g.zs + (long long) y * g.ys + x] = ep;
+            }
+        }
+        if (failed) {
+            if (tid == 0) tma_fault<L::S>(st, bars, kbase, fail_it + 1, issued_n);
+            __syncthreads();
+            return;
+        }
+        kbase += n_it;
+
+        const double2 r = block_reduce(acc_s, acc_m, red);
+        if (tid == 0) V.part_t[lt] = r;
+        if (publish_partial(&st->ticket_t, V.ntiles, &s_flag)) {
+            double ssum = 0.0, smax = 0.0;
+            for (int i = tid; i < V.ntiles; i += NT) {
+                const double2 p = __ldcg(&V.part_t[i]);
+                ssum += p.x;
+                smax = fmax(smax, p.y);
+            }
+            const double2 tot = block_reduce(ssum, smax, red);
+            if (tid == 0) {
+                st->ticket_t = 0;
+                control_after_trial(st, tot.x, tot.y);
+                if (work_flag) *work_flag = 1;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
+                                                     const int *__restrict__ tile_vol, int total_tiles,
+                                                     unsigned char *__restrict__ work_flag) {
+    using L = GradTmaLayout<T>;
+    constexpr int PXP = L::PXP, PYP = L::PYP;
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem = align_smem_128(smem_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    T *pxy = reinterpret_cast<T *>(smem + L::P_OFF);
+    __shared__ double red[2 * (NT / 32)];
+    __shared__ int s_flag, s_ok;
+    auto PX_ = [&](int slot, int t, int ly, int lx) -> T & {  // t: 0..2 P_ix, 3..5 P_iy
+        return pxy[((slot * 6 + t) * PYP + ly) * PXP + lx];
+    };
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+    if (tid == 0) {
+        for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t kbase = 0;
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const VolumeDesc<T> &V = vols[tile_vol[tile]];
+        SolverState *st = V.st;
+        if (ldcg_int(&st->done) || !ldcg_int(&st->need_gradient)) continue;
+        const Geom g = V.g;
+        const int old_b = ldcg_int(&st->old_buf);
+        const int lt = tile - V.tile_begin;
+        const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
+        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
+        const int z1 = min(z0 + V.bz, g.nz);
+        const int n_it = z1 - z0 + 4;  // u planes z0-2 .. z1+1
+        const CUtensorMap *tm_u = V.tm_field[old_b];
+        const CUtensorMap *tm_e = V.tm_ep[old_b];
+        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+
+        int issued_n = 0;
+        auto issue = [&](int j) {
+            issued_n = j + 1;
+            const uint32_t k = kbase + j;
+            const int s = k % L::S;
+            unsigned char *sb = smem + s * L::STAGE_BYTES;
+            const int q = z0 - 2 + j;
+            mbar_arrive_expect_tx(&bars[s], L::U_BYTES + L::E_BYTES);
+            tma_load_4d(sb, tm_u, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
+            tma_load_3d(sb + L::U_BYTES, tm_e, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q);
+        };
+        if (tid == 0) {
+            tmap_acquire(tm_u);
+            tmap_acquire(tm_e);
+            for (int j = 0; j < min(L::S, n_it); ++j) issue(j);
+        }
+        auto stage_u = [&](int j) -> const T * {
+            return reinterpret_cast<const T *>(smem + ((kbase + j) % L::S) * L::STAGE_BYTES);
+        };
+        auto stage_e = [&](int j) -> const T * {
+            return reinterpret_cast<const T *>(smem + ((kbase + j) % L::S) * L::STAGE_BYTES + L::U_BYTES);
+        };
+
+        const int x = x0 + tx, y = y0 + ty;
+        const bool interior_xy = x >= 1 && x < g.nx - 1 && y >= 1 && y < g.ny - 1;
+        T pz_m2[3] = {T(0), T(0), T(0)}, pz_m1[3] = {T(0), T(0), T(0)};
+        double acc = 0.0;
+        bool failed = false;
+        int fail_it = 0;
+        for (int it = 0; it < n_it; ++it) {
+            const uint32_t k = kbase + it;
+            const int s = k % L::S;
+            const uint32_t par = (k / L::S) & 1u;
+            if (tid == 0) s_ok = mbar_wait_bounded(&bars[s], par);
+            __syncthreads();
+            if (!s_ok) {
+                failed = true;
+                fail_it = it;
+                break;
+            }
+            mbar_try_wait(&bars[s], par);
+            const int q = z0 - 2 + it;
+            const int p = q - 1;  // plane of P computed now (needs u(q-2..q), e'(q-1))
+            T pz_new[3] = {T(0), T(0), T(0)};
+            if (it >= 2) {
+                const T *um = stage_u(it - 2), *u0 = stage_u(it - 1), *up = stage_u(it);
+                const T *e0 = stage_e(it - 1);
+                const int ps = p & 1;
+                // M = I + grad u at box cell (lx, ly) of plane p, second order central.
+                auto mat = [&](int lx, int ly, T m[3][3]) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int o = (c * TMA_PY + ly) * TMA_PX + lx;
+                        m[c][0] = fd_c2<T>(u0[o + 1], u0[o - 1], ih[0]);
+                        m[c][1] = fd_c2<T>(u0[o + TMA_PX], u0[o - TMA_PX], ih[1]);
+                        m[c][2] = fd_c2<T>(up[o], um[o], ih[2]);
+                        m[c][c] += T(1.0);
+                    }
+                };
+                auto minor = [](const T m[3][3], int i, int kk) -> T {
+                    const int r0 = i == 0 ? 1 : 0, r1 = i == 2 ? 1 : 2;
+                    const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
+                    return m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
+                };
+                {   // own cell: all nine terms (P_z kept in registers)
+                    const int lx = tx + TMA_HX, ly = ty + TMA_HY;
+                    T m[3][3];
+                    mat(lx, ly, m);
+                    const T ep = e0[ly * TMA_PX + lx];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        PX_(ps, i, ty + 1, tx + 1) = ep * minor(m, i, 0);
+                        PX_(ps, 3 + i, ty + 1, tx + 1) = ep * minor(m, i, 1);
+                        pz_new[i] = ep * minor(m, i, 2);
+                    }
+                }
+                // halo cells: P_x on the two side columns, P_y on the two end rows
+                if (tid < 2 * BY) {
+                    const int side = tid / BY, row = tid % BY;
+                    const int lx1 = side ? BX + 1 : 0;  // P index
+                    const int lx = lx1 - 1 + TMA_HX, ly = row + TMA_HY;
+                    T m[3][3];
+                    mat(lx, ly, m);
+                    const T ep = e0[ly * TMA_PX + lx];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) PX_(ps, i, row + 1, lx1) = ep * minor(m, i, 0);
+                } else if (tid < 2 * BY + 2 * BX) {
+                    const int t2 = tid - 2 * BY;
+                    const int side = t2 / BX, col = t2 % BX;
+                    const int ly1 = side ? BY + 1 : 0;
+                    const int lx = col + TMA_HX, ly = ly1 - 1 + TMA_HY;
+                    T m[3][3];
+                    mat(lx, ly, m);
+                    const T ep = e0[ly * TMA_PX + lx];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) PX_(ps, 3 + i, ly1, col + 1) = ep * minor(m, i, 1);
+                }
+            }
+            __syncthreads();
+            if (tid == 0 && it >= 2 && it - 2 + L::S < n_it) issue(it - 2 + L::S);
+            const int z = q - 2;  // gradient plane: P(z-1), P(z), P(z+1) ready
+            if (it >= 3 && z >= z0 && z < z1 && interior_xy && z >= 1 && z < g.nz - 1) {
+                const int ps = z & 1;
+                const int lx = tx + 1, ly = ty + 1;
+                T t[3][3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    t[i][0] = ih[0] * (PX_(ps, i, ly, lx - 1) - PX_(ps, i, ly, lx + 1));
+                    t[i][1] = ih[1] * (PX_(ps, 3 + i, ly - 1, lx) - PX_(ps, 3 + i, ly + 1, lx));
+                    t[i][2] = ih[2] * (pz_m2[i] - pz_new[i]);
+                }
+                const T gx = t[0][0] - t[0][1] + t[0][2];
+                const T gy = -t[1][0] + t[1][1] - t[1][2];
+                const T gz = t[2][0] - t[2][1] + t[2][2];
+                const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
+                V.grad[so] = gx;
+                V.grad[g.cs + so] = gy;
+                V.grad[2 * g.cs + so] = gz;
+                acc += (double) (gx * gx + gy * gy + gz * gz);
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                pz_m2[i] = pz_m1[i];
+                pz_m1[i] = pz_new[i];
+            }
+        }
+        if (failed) {
+            if (tid == 0) tma_fault<L::S>(st, bars, kbase, fail_it + 1, issued_n);
+            __syncthreads();
+            return;
+        }
+        kbase += n_it;
+
+        const double2 r = block_reduce(acc, 0.0, red);
+        if (tid == 0) V.part_g[lt] = r.x;
+        if (publish_partial(&st->ticket_g, V.ntiles, &s_flag)) {
+            double ssum = 0.0;
+            for (int i = tid; i < V.ntiles; i += NT) ssum += __ldcg(&V.part_g[i]);
+            const double2 tot = block_reduce(ssum, 0.0, red);
+            if (tid == 0) {
+                st->ticket_g = 0;
+                st->gn2 = tot.x;
+                st->need_gradient = 0;
+                st->gradients++;
+                if (work_flag) *work_flag = 1;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                             cudaStream_t s, unsigned char *work_flag) {
+    constexpr int smem = TrialTmaLayout<T>::BYTES + 128;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_trial_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr != cudaSuccess) return attr;
+    k_trial_tma<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles, work_flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                                cudaStream_t s, unsigned char *work_flag) {
+    constexpr int smem = GradTmaLayout<T>::BYTES + 128;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_gradient_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr != cudaSuccess) return attr;
+    k_gradient_tma<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles, work_flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+int trial_tma_blocks_per_sm() {
+    int n = 0;
+    cudaFuncSetAttribute(k_trial_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrialTmaLayout<T>::BYTES + 128);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_trial_tma<T>, NT, TrialTmaLayout<T>::BYTES + 128);
+    return n;
+}
+template <typename T>
+int gradient_tma_blocks_per_sm() {
+    int n = 0;
+    cudaFuncSetAttribute(k_gradient_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, GradTmaLayout<T>::BYTES + 128);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_gradient_tma<T>, NT, GradTmaLayout<T>::BYTES + 128);
+    return n;
+}
+
+#define DTB_INSTANTIATE_TMA(T)                                                                              \
+    template cudaError_t launch_trial_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
+                                             unsigned char *);                                              \
+    template cudaError_t launch_gradient_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t, \
+                                                unsigned char *);                                           \
+    template int trial_tma_blocks_per_sm<T>();                                                              \
+    template int gradient_tma_blocks_per_sm<T>();
+
+}  // namespace dtb
