@@ -351,11 +351,12 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     int total_tiles = 0;
     size_t need = 0;
     auto align = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const int tile_y = gradient ? TT_Y : BY;
     for (int i = 0; i < count; ++i) {
         const Geom g = pitched(vols[i].g);
         geo[i] = g;
         const int bz = pick_bz(g.nz);
-        const int t = ((g.nx + BX - 1) / BX) * ((g.ny + BY - 1) / BY) * ((g.nz + bz - 1) / bz);
+        const int t = ((g.nx + BX - 1) / BX) * ((g.ny + tile_y - 1) / tile_y) * ((g.nz + bz - 1) / bz);
         tiles[i] = t;
         tbegin[i] = total_tiles;
         total_tiles += t;
@@ -406,7 +407,7 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         d_maps[i] = cv.take<CUtensorMap>(7);
         const int bz = pick_bz(g.nz);
         d.tiles_x = (g.nx + BX - 1) / BX;
-        d.tiles_y = (g.ny + BY - 1) / BY;
+        d.tiles_y = (g.ny + tile_y - 1) / tile_y;
         d.tiles_z = (g.nz + bz - 1) / bz;
         d.tile_begin = tbegin[i];
         d.ntiles = tiles[i];
@@ -449,13 +450,15 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         if (gradient) {
             CUtensorMap h_maps[7];
             const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-            bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, BX + 8, BY + 4) &&
-                      encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, BX + 8, BY + 4) &&
-                      encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, BX + 8, BY + 4) &&
-                      encode_map(&h_maps[3], ft, sizeof(T), d.ep[0], g, 1, BX + 8, BY + 4) &&
-                      encode_map(&h_maps[4], ft, sizeof(T), d.ep[1], g, 1, BX + 8, BY + 4) &&
-                      encode_map(&h_maps[5], ft, sizeof(T), Jt, g, 1, BX, BY) &&
-                      encode_map(&h_maps[6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, g, 1, BX, BY);
+            // Boxes: the tile plus 4 voxels in x (16-byte aligned start) and 2
+            // rows in y for the stencil inputs; the bare tile for J_t and the mask.
+            bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, BX + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, BX + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, BX + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[3], ft, sizeof(T), d.ep[0], g, 1, BX + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[4], ft, sizeof(T), d.ep[1], g, 1, BX + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[5], ft, sizeof(T), Jt, g, 1, BX, TT_Y) &&
+                      encode_map(&h_maps[6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, g, 1, BX, TT_Y);
             if (!ok) DTB_FAIL(DTB_ERR_CUDA, "cannot encode the TMA descriptors (cuTensorMapEncodeTiled)");
             DTB_CUDA(cudaMemcpyAsync(d_maps[i], h_maps, sizeof h_maps, cudaMemcpyHostToDevice, stream));
             d.tm_field[0] = d_maps[i] + 0;

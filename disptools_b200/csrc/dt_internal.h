@@ -14,6 +14,8 @@ namespace dtb {
 constexpr int BX = 32;
 constexpr int BY = 8;
 constexpr int NT = BX * BY;
+// Tile height of the TMA kernels of the gradient method (two rows per thread).
+constexpr int TT_Y = 2 * BY;
 
 // Phases of the per-volume step-control state machine.
 enum Phase {

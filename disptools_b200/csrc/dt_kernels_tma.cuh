@@ -1,16 +1,20 @@
 // TMA-pipelined kernels of the gradient method (sm_100a).
 //
-// Both kernels march a BX x BY tile through its z range.  One elected thread
-// streams one box per input per plane into a ring of shared-memory stages
-// with cp.async.bulk.tensor (completion on an mbarrier per stage); the other
-// threads never issue global loads for the stencil inputs.  Shared-memory
-// boxes start 4 voxels left of the tile so the innermost TMA coordinate stays
-// 16-byte aligned; planes outside the volume arrive zero-filled.
+// Both kernels march a BX x TT_Y tile (two rows per thread) through its z
+// range.  One elected thread streams one box per input per plane into a ring
+// of shared-memory stages with cp.async.bulk.tensor, completion tracked by an
+// mbarrier per stage; the other threads issue no global loads for the stencil
+// inputs.  Boxes start 4 voxels left of the tile so the innermost TMA
+// coordinate stays 16-byte aligned; planes outside the volume arrive
+// zero-filled.
 //
-// k_trial_tma     candidate = field[old] - eta * grad (formed once per plane
-//                 in shared memory), written to field[1-old]; its Jacobian,
-//                 masked error and regularised error e' per voxel; FP64
-//                 partials and the on-device step control (last tile).
+// k_trial_tma     candidate = field[old] - eta * grad, formed once per plane
+//                 in shared memory and written to field[1-old]; each thread
+//                 keeps its own two columns of candidate values (five planes)
+//                 in registers for the z differences, so shared memory holds
+//                 three candidate planes.  Jacobian, masked error, regularised
+//                 error e' per voxel; FP64 partials and the on-device step
+//                 control in the last tile.
 // k_gradient_tma  g = sum_k +-ih_k (P_ik(p - e_k) - P_ik(p + e_k)) with
 //                 P_ik = e' * minor_ik(I + grad u) (second-order central
 //                 differences, src/displacement_field_gradient.c:26-145),
@@ -22,19 +26,20 @@
 
 namespace dtb {
 
-constexpr int TMA_HX = 4;               // x halo of the boxes (16-byte aligned start)
-constexpr int TMA_HY = 2;               // y halo
-constexpr int TMA_PX = BX + 2 * TMA_HX; // 40
-constexpr int TMA_PY = BY + 2 * TMA_HY; // 12
-constexpr int TMA_PLANE = TMA_PY * TMA_PX;  // elements of one component plane of a box
+constexpr int RY = TT_Y / BY;              // rows per thread
+constexpr int TMA_HX = 4;                  // x halo of the boxes (16-byte aligned start)
+constexpr int TMA_HY = 2;                  // y halo
+constexpr int TMA_PX = BX + 2 * TMA_HX;    // 40
+constexpr int TMA_PY = TT_Y + 2 * TMA_HY;  // 20
+constexpr int TMA_PLANE = TMA_PY * TMA_PX; // elements of one component plane of a box
 
 template <typename T>
 struct TrialTmaLayout {
     static constexpr int S = 3;  // pipeline stages
-    static constexpr int R = 6;  // candidate planes kept (z-2 .. z+2 plus the one being formed)
+    static constexpr int R = 3;  // candidate planes in shared memory (z, z+1, z+2)
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
-    static constexpr int JT_BYTES = BX * BY * (int) sizeof(T);
-    static constexpr int MASK_BYTES = BX * BY;
+    static constexpr int JT_BYTES = BX * TT_Y * (int) sizeof(T);
+    static constexpr int MASK_BYTES = BX * TT_Y;
     static constexpr int STAGE_BYTES = 2 * U_BYTES + JT_BYTES + MASK_BYTES;  // u, g, Jt, mask
     static constexpr int RING_OFF = S * STAGE_BYTES;
     static constexpr int BAR_OFF = RING_OFF + R * U_BYTES;
@@ -43,11 +48,11 @@ struct TrialTmaLayout {
 
 template <typename T>
 struct GradTmaLayout {
-    static constexpr int S = 6;  // stages double as the plane ring (u, e')
+    static constexpr int S = sizeof(T) == 4 ? 6 : 5;  // stages double as the plane ring (u, e')
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
     static constexpr int E_BYTES = TMA_PLANE * (int) sizeof(T);
     static constexpr int STAGE_BYTES = U_BYTES + E_BYTES;
-    static constexpr int PXP = BX + 2, PYP = BY + 2;
+    static constexpr int PXP = BX + 2, PYP = TT_Y + 2;
     static constexpr int P_OFF = S * STAGE_BYTES;  // P_x, P_y terms: [2][6][PYP][PXP]
     static constexpr int P_BYTES = 2 * 6 * PYP * PXP * (int) sizeof(T);
     static constexpr int BAR_OFF = P_OFF + P_BYTES;
@@ -75,8 +80,10 @@ __device__ __forceinline__ void tma_fault(SolverState *st, uint64_t *bars, uint3
     }
 }
 
+// Two resident blocks per SM for FP32 (shared memory allows no more), one for
+// FP64; the bound lets the compiler use up to 128 / 255 registers.
 template <typename T>
-__global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restrict__ vols,
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const VolumeDesc<T> *__restrict__ vols,
                                                   const int *__restrict__ tile_vol, int total_tiles,
                                                   unsigned char *__restrict__ work_flag) {
     using L = TrialTmaLayout<T>;
@@ -106,7 +113,7 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
         const bool trial = phase != PH_EVAL0;
         const int lt = tile - V.tile_begin;
         const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
-        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
+        const int x0 = txi * BX, y0 = tyi * TT_Y, z0 = tzi * V.bz;
         const int z1 = min(z0 + V.bz, g.nz);
         const int n_it = z1 - z0 + 4;  // candidate planes z0-2 .. z1+1
         const CUtensorMap *tm_u = V.tm_field[old_b];
@@ -126,7 +133,8 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
             unsigned char *sb = smem + s * L::STAGE_BYTES;
             const int q = z0 - 2 + j, ze = q - 2;
             const bool with_target = ze >= z0 && ze < z1;
-            uint32_t bytes = L::U_BYTES + (trial ? L::U_BYTES : 0) + (with_target ? L::JT_BYTES + L::MASK_BYTES : 0);
+            const uint32_t bytes =
+                L::U_BYTES + (trial ? L::U_BYTES : 0) + (with_target ? L::JT_BYTES + L::MASK_BYTES : 0);
             mbar_arrive_expect_tx(&bars[s], bytes);
             tma_load_4d(sb, tm_u, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
             if (trial) tma_load_4d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
@@ -144,8 +152,15 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
             for (int j = 0; j < min(L::S, n_it); ++j) issue(j);
         }
 
-        const int x = x0 + tx, y = y0 + ty;
-        const bool in_xy = x < g.nx && y < g.ny;
+        const int x = x0 + tx;
+        // Own columns: candidate values of planes q-4 .. q (z differences).
+        T zq[RY][3][5];
+#pragma unroll
+        for (int r = 0; r < RY; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 5; ++k) zq[r][c][k] = T(0);
         double acc_s = 0.0, acc_m = 0.0;
         bool failed = false;
         int fail_it = 0;
@@ -166,12 +181,10 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
             T *slot = ring + (size_t) ring_slot(q, L::R) * 3 * TMA_PLANE;
             // Candidate plane q (tile + halo): u - eta g, vectorised.
             {
-                const T *u = reinterpret_cast<const T *>(sb);
-                const T *gr = reinterpret_cast<const T *>(sb + L::U_BYTES);
                 constexpr int VEC = 16 / (int) sizeof(T);
                 using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-                const V4 *u4 = reinterpret_cast<const V4 *>(u);
-                const V4 *g4 = reinterpret_cast<const V4 *>(gr);
+                const V4 *u4 = reinterpret_cast<const V4 *>(sb);
+                const V4 *g4 = reinterpret_cast<const V4 *>(sb + L::U_BYTES);
                 V4 *c4 = reinterpret_cast<V4 *>(slot);
                 for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NT) {
                     V4 a = u4[i];
@@ -185,72 +198,85 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
                     c4[i] = a;
                 }
             }
-            T jt = T(0);
-            bool msk = false;
             const bool eval = ze >= z0 && ze < z1;
-            if (eval) {
-                jt = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid];
-                msk = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid] != 0;
+            T jt[RY];
+            bool msk[RY];
+#pragma unroll
+            for (int r = 0; r < RY; ++r) {
+                jt[r] = T(0);
+                msk[r] = false;
+                if (eval) {
+                    jt[r] = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid + r * NT];
+                    msk[r] = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid + r * NT] != 0;
+                }
             }
             __syncthreads();
             if (tid == 0 && it + L::S < n_it) issue(it + L::S);
-            // Store the candidate of core plane q.
-            if (trial && in_xy && q >= z0 && q < z1) {
-                const long long so = (long long) q * g.zs + (long long) y * g.ys + x;
+            // Shift the own-column queues by plane q; store the candidate.
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    dst[c * g.cs + so] = slot[(c * TMA_PY + ty + TMA_HY) * TMA_PX + tx + TMA_HX];
-            }
-            if (eval && in_xy) {
-                const int sl[5] = {ring_slot(ze - 2, L::R), ring_slot(ze - 1, L::R), ring_slot(ze, L::R),
-                                   ring_slot(ze + 1, L::R), ring_slot(ze + 2, L::R)};
-                const int lx = tx + TMA_HX, ly = ty + TMA_HY;
-                T a[3][3];
-                const bool fast = x0 >= 2 && x0 + BX <= g.nx - 2 && y >= 2 && y <= g.ny - 3 && ze >= 2 &&
-                                  ze <= g.nz - 3 && g.order == 4;
-                if (fast) {
+            for (int r = 0; r < RY; ++r) {
+                const int ly = ty + r * BY + TMA_HY;
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const T *p = ring + ((size_t) sl[2] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
-                        const T *zm2 = ring + ((size_t) sl[0] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
-                        const T *zm1 = ring + ((size_t) sl[1] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
-                        const T *zp1 = ring + ((size_t) sl[3] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
-                        const T *zp2 = ring + ((size_t) sl[4] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx;
-                        a[c][0] = fd_c4<T>(p[1], p[-1], p[2], p[-2], ih[0]);
-                        a[c][1] = fd_c4<T>(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], ih[1]);
-                        a[c][2] = fd_c4<T>(*zp1, *zm1, *zp2, *zm2, ih[2]);
-                    }
-                } else {
-                    int kk[3];
-                    schemes_at(x, y, ze, g, kk);
+                for (int c = 0; c < 3; ++c) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c)
-#pragma unroll
-                        for (int ax = 0; ax < 3; ++ax) {
-                            auto val = [&](int o) -> T {
-                                if (ax == 0) return ring[((size_t) sl[2] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx + o];
-                                if (ax == 1)
-                                    return ring[((size_t) sl[2] * 3 + c) * TMA_PLANE + (ly + o) * TMA_PX + lx];
-                                return ring[((size_t) sl[2 + o] * 3 + c) * TMA_PLANE + ly * TMA_PX + lx];
-                            };
-                            T d;
-                            switch (kk[ax]) {
-                            case S_FWD: d = fd_fwd<T>(val(0), val(1), val(2), ih[ax]); break;
-                            case S_BWD: d = fd_bwd<T>(val(0), val(-1), val(-2), ih[ax]); break;
-                            case S_C2: d = fd_c2<T>(val(1), val(-1), ih[ax]); break;
-                            default: d = fd_c4<T>(val(1), val(-1), val(2), val(-2), ih[ax]); break;
-                            }
-                            a[c][ax] = d;
-                        }
+                    for (int kk = 0; kk < 4; ++kk) zq[r][c][kk] = zq[r][c][kk + 1];
+                    zq[r][c][4] = slot[c * TMA_PLANE + ly * TMA_PX + tx + TMA_HX];
                 }
-                const T J = det_i_plus<T>(a);
-                const T vv = voxel_error<T>(J, jt, msk, tol);
-                acc_s += (double) vv * (double) vv;
-                const double av = fabs((double) vv);
-                if (msk && av > acc_m) acc_m = av;
-                T ep = vv;
-                if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
-                ep_out[(long long) ze * g.zs + (long long) y * g.ys + x] = ep;
+                const int y = y0 + ty + r * BY;
+                if (trial && x < g.nx && y < g.ny && q >= z0 && q < z1) {
+                    const long long so = (long long) q * g.zs + (long long) y * g.ys + x;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) dst[c * g.cs + so] = zq[r][c][4];
+                }
+            }
+            if (eval) {
+                const T *jp = ring + (size_t) ring_slot(ze, L::R) * 3 * TMA_PLANE;
+                const bool fast_xz = x0 >= 2 && x0 + BX <= g.nx - 2 && ze >= 2 && ze <= g.nz - 3 && g.order == 4;
+#pragma unroll
+                for (int r = 0; r < RY; ++r) {
+                    const int y = y0 + ty + r * BY;
+                    if (x >= g.nx || y >= g.ny) continue;
+                    const int lx = tx + TMA_HX, ly = ty + r * BY + TMA_HY;
+                    T a[3][3];
+                    if (fast_xz && y >= 2 && y <= g.ny - 3) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+                            a[c][0] = fd_c4<T>(p[1], p[-1], p[2], p[-2], ih[0]);
+                            a[c][1] = fd_c4<T>(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], ih[1]);
+                            a[c][2] = fd_c4<T>(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0], ih[2]);
+                        }
+                    } else {
+                        int kk[3];
+                        schemes_at(x, y, ze, g, kk);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+                            const T vx[5] = {p[-2], p[-1], p[0], p[1], p[2]};
+                            const T vy[5] = {p[-2 * TMA_PX], p[-TMA_PX], p[0], p[TMA_PX], p[2 * TMA_PX]};
+#pragma unroll
+                            for (int ax = 0; ax < 3; ++ax) {
+                                const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[r][c]);
+                                T d;
+                                switch (kk[ax]) {
+                                case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
+                                case S_BWD: d = fd_bwd<T>(w[2], w[1], w[0], ih[ax]); break;
+                                case S_C2: d = fd_c2<T>(w[3], w[1], ih[ax]); break;
+                                default: d = fd_c4<T>(w[3], w[1], w[4], w[0], ih[ax]); break;
+                                }
+                                a[c][ax] = d;
+                            }
+                        }
+                    }
+                    const T J = det_i_plus<T>(a);
+                    const T vv = voxel_error<T>(J, jt[r], msk[r], tol);
+                    acc_s += (double) vv * (double) vv;
+                    const double av = fabs((double) vv);
+                    if (msk[r] && av > acc_m) acc_m = av;
+                    T ep = vv;
+                    if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
+                    ep_out[(long long) ze * g.zs + (long long) y * g.ys + x] = ep;
+                }
             }
         }
         if (failed) {
@@ -260,14 +286,14 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
         }
         kbase += n_it;
 
-        const double2 r = block_reduce(acc_s, acc_m, red);
-        if (tid == 0) V.part_t[lt] = r;
+        const double2 rr = block_reduce(acc_s, acc_m, red);
+        if (tid == 0) V.part_t[lt] = rr;
         if (publish_partial(&st->ticket_t, V.ntiles, &s_flag)) {
             double ssum = 0.0, smax = 0.0;
             for (int i = tid; i < V.ntiles; i += NT) {
-                const double2 p = __ldcg(&V.part_t[i]);
-                ssum += p.x;
-                smax = fmax(smax, p.y);
+                const double2 pp = __ldcg(&V.part_t[i]);
+                ssum += pp.x;
+                smax = fmax(smax, pp.y);
             }
             const double2 tot = block_reduce(ssum, smax, red);
             if (tid == 0) {
@@ -282,7 +308,7 @@ __global__ void __launch_bounds__(NT) k_trial_tma(const VolumeDesc<T> *__restric
 }
 
 template <typename T>
-__global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
                                                      const int *__restrict__ tile_vol, int total_tiles,
                                                      unsigned char *__restrict__ work_flag) {
     using L = GradTmaLayout<T>;
@@ -293,7 +319,9 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
     T *pxy = reinterpret_cast<T *>(smem + L::P_OFF);
     __shared__ double red[2 * (NT / 32)];
     __shared__ int s_flag, s_ok;
-    auto PX_ = [&](int slot, int t, int ly, int lx) -> T & {  // t: 0..2 P_ix, 3..5 P_iy
+    // P terms of the x (t = 0..2) and y (t = 3..5) directions, cell (ly, lx)
+    // of the tile plus a halo of one.
+    auto PT = [&](int slot, int t, int ly, int lx) -> T & {
         return pxy[((slot * 6 + t) * PYP + ly) * PXP + lx];
     };
 
@@ -313,7 +341,7 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
         const int old_b = ldcg_int(&st->old_buf);
         const int lt = tile - V.tile_begin;
         const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
-        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
+        const int x0 = txi * BX, y0 = tyi * TT_Y, z0 = tzi * V.bz;
         const int z1 = min(z0 + V.bz, g.nz);
         const int n_it = z1 - z0 + 4;  // u planes z0-2 .. z1+1
         const CUtensorMap *tm_u = V.tm_field[old_b];
@@ -343,9 +371,12 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
             return reinterpret_cast<const T *>(smem + ((kbase + j) % L::S) * L::STAGE_BYTES + L::U_BYTES);
         };
 
-        const int x = x0 + tx, y = y0 + ty;
-        const bool interior_xy = x >= 1 && x < g.nx - 1 && y >= 1 && y < g.ny - 1;
-        T pz_m2[3] = {T(0), T(0), T(0)}, pz_m1[3] = {T(0), T(0), T(0)};
+        const int x = x0 + tx;
+        T pz_m2[RY][3], pz_m1[RY][3];
+#pragma unroll
+        for (int r = 0; r < RY; ++r)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) pz_m2[r][i] = pz_m1[r][i] = T(0);
         double acc = 0.0;
         bool failed = false;
         int fail_it = 0;
@@ -363,7 +394,11 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
             mbar_try_wait(&bars[s], par);
             const int q = z0 - 2 + it;
             const int p = q - 1;  // plane of P computed now (needs u(q-2..q), e'(q-1))
-            T pz_new[3] = {T(0), T(0), T(0)};
+            T pz_new[RY][3];
+#pragma unroll
+            for (int r = 0; r < RY; ++r)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) pz_new[r][i] = T(0);
             if (it >= 2) {
                 const T *um = stage_u(it - 2), *u0 = stage_u(it - 1), *up = stage_u(it);
                 const T *e0 = stage_e(it - 1);
@@ -372,7 +407,7 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
                 auto mat = [&](int lx, int ly, T m[3][3]) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        const int o = (c * TMA_PY + ly) * TMA_PX + lx;
+                        const int o = c * TMA_PLANE + ly * TMA_PX + lx;
                         m[c][0] = fd_c2<T>(u0[o + 1], u0[o - 1], ih[0]);
                         m[c][1] = fd_c2<T>(u0[o + TMA_PX], u0[o - TMA_PX], ih[1]);
                         m[c][2] = fd_c2<T>(up[o], um[o], ih[2]);
@@ -384,67 +419,75 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
                     const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
                     return m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
                 };
-                {   // own cell: all nine terms (P_z kept in registers)
-                    const int lx = tx + TMA_HX, ly = ty + TMA_HY;
+#pragma unroll
+                for (int r = 0; r < RY; ++r) {  // own cells: all nine terms (P_z in registers)
+                    const int lx = tx + TMA_HX, ly = ty + r * BY + TMA_HY;
                     T m[3][3];
                     mat(lx, ly, m);
                     const T ep = e0[ly * TMA_PX + lx];
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        PX_(ps, i, ty + 1, tx + 1) = ep * minor(m, i, 0);
-                        PX_(ps, 3 + i, ty + 1, tx + 1) = ep * minor(m, i, 1);
-                        pz_new[i] = ep * minor(m, i, 2);
+                        PT(ps, i, ty + r * BY + 1, tx + 1) = ep * minor(m, i, 0);
+                        PT(ps, 3 + i, ty + r * BY + 1, tx + 1) = ep * minor(m, i, 1);
+                        pz_new[r][i] = ep * minor(m, i, 2);
                     }
                 }
                 // halo cells: P_x on the two side columns, P_y on the two end rows
-                if (tid < 2 * BY) {
-                    const int side = tid / BY, row = tid % BY;
-                    const int lx1 = side ? BX + 1 : 0;  // P index
+                if (tid < 2 * TT_Y) {
+                    const int side = tid / TT_Y, row = tid % TT_Y;
+                    const int lx1 = side ? BX + 1 : 0;
                     const int lx = lx1 - 1 + TMA_HX, ly = row + TMA_HY;
                     T m[3][3];
                     mat(lx, ly, m);
                     const T ep = e0[ly * TMA_PX + lx];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) PX_(ps, i, row + 1, lx1) = ep * minor(m, i, 0);
-                } else if (tid < 2 * BY + 2 * BX) {
-                    const int t2 = tid - 2 * BY;
+                    for (int i = 0; i < 3; ++i) PT(ps, i, row + 1, lx1) = ep * minor(m, i, 0);
+                } else if (tid < 2 * TT_Y + 2 * BX) {
+                    const int t2 = tid - 2 * TT_Y;
                     const int side = t2 / BX, col = t2 % BX;
-                    const int ly1 = side ? BY + 1 : 0;
+                    const int ly1 = side ? TT_Y + 1 : 0;
                     const int lx = col + TMA_HX, ly = ly1 - 1 + TMA_HY;
                     T m[3][3];
                     mat(lx, ly, m);
                     const T ep = e0[ly * TMA_PX + lx];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) PX_(ps, 3 + i, ly1, col + 1) = ep * minor(m, i, 1);
+                    for (int i = 0; i < 3; ++i) PT(ps, 3 + i, ly1, col + 1) = ep * minor(m, i, 1);
                 }
             }
             __syncthreads();
             if (tid == 0 && it >= 2 && it - 2 + L::S < n_it) issue(it - 2 + L::S);
             const int z = q - 2;  // gradient plane: P(z-1), P(z), P(z+1) ready
-            if (it >= 3 && z >= z0 && z < z1 && interior_xy && z >= 1 && z < g.nz - 1) {
+            if (it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x >= 1 && x < g.nx - 1) {
                 const int ps = z & 1;
-                const int lx = tx + 1, ly = ty + 1;
-                T t[3][3];
+#pragma unroll
+                for (int r = 0; r < RY; ++r) {
+                    const int y = y0 + ty + r * BY;
+                    if (y < 1 || y >= g.ny - 1) continue;
+                    const int lx = tx + 1, ly = ty + r * BY + 1;
+                    T t[3][3];
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        t[i][0] = ih[0] * (PT(ps, i, ly, lx - 1) - PT(ps, i, ly, lx + 1));
+                        t[i][1] = ih[1] * (PT(ps, 3 + i, ly - 1, lx) - PT(ps, 3 + i, ly + 1, lx));
+                        t[i][2] = ih[2] * (pz_m2[r][i] - pz_new[r][i]);
+                    }
+                    const T gx = t[0][0] - t[0][1] + t[0][2];
+                    const T gy = -t[1][0] + t[1][1] - t[1][2];
+                    const T gz = t[2][0] - t[2][1] + t[2][2];
+                    const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
+                    V.grad[so] = gx;
+                    V.grad[g.cs + so] = gy;
+                    V.grad[2 * g.cs + so] = gz;
+                    acc += (double) (gx * gx + gy * gy + gz * gz);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RY; ++r)
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    t[i][0] = ih[0] * (PX_(ps, i, ly, lx - 1) - PX_(ps, i, ly, lx + 1));
-                    t[i][1] = ih[1] * (PX_(ps, 3 + i, ly - 1, lx) - PX_(ps, 3 + i, ly + 1, lx));
-                    t[i][2] = ih[2] * (pz_m2[i] - pz_new[i]);
+                    pz_m2[r][i] = pz_m1[r][i];
+                    pz_m1[r][i] = pz_new[r][i];
                 }
-                const T gx = t[0][0] - t[0][1] + t[0][2];
-                const T gy = -t[1][0] + t[1][1] - t[1][2];
-                const T gz = t[2][0] - t[2][1] + t[2][2];
-                const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
-                V.grad[so] = gx;
-                V.grad[g.cs + so] = gy;
-                V.grad[2 * g.cs + so] = gz;
-                acc += (double) (gx * gx + gy * gy + gz * gz);
-            }
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                pz_m2[i] = pz_m1[i];
-                pz_m1[i] = pz_new[i];
-            }
         }
         if (failed) {
             if (tid == 0) tma_fault<L::S>(st, bars, kbase, fail_it + 1, issued_n);
@@ -453,8 +496,8 @@ __global__ void __launch_bounds__(NT) k_gradient_tma(const VolumeDesc<T> *__rest
         }
         kbase += n_it;
 
-        const double2 r = block_reduce(acc, 0.0, red);
-        if (tid == 0) V.part_g[lt] = r.x;
+        const double2 rr = block_reduce(acc, 0.0, red);
+        if (tid == 0) V.part_g[lt] = rr.x;
         if (publish_partial(&st->ticket_g, V.ntiles, &s_flag)) {
             double ssum = 0.0;
             for (int i = tid; i < V.ntiles; i += NT) ssum += __ldcg(&V.part_g[i]);
@@ -498,16 +541,24 @@ cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, 
 
 template <typename T>
 int trial_tma_blocks_per_sm() {
-    int n = 0;
-    cudaFuncSetAttribute(k_trial_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrialTmaLayout<T>::BYTES + 128);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_trial_tma<T>, NT, TrialTmaLayout<T>::BYTES + 128);
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_trial_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TrialTmaLayout<T>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T>, NT, TrialTmaLayout<T>::BYTES + 128);
+        return v;
+    }();
     return n;
 }
 template <typename T>
 int gradient_tma_blocks_per_sm() {
-    int n = 0;
-    cudaFuncSetAttribute(k_gradient_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, GradTmaLayout<T>::BYTES + 128);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_gradient_tma<T>, NT, GradTmaLayout<T>::BYTES + 128);
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_gradient_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GradTmaLayout<T>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T>, NT, GradTmaLayout<T>::BYTES + 128);
+        return v;
+    }();
     return n;
 }
 

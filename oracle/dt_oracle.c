@@ -174,11 +174,18 @@ real oracle_compute_error(size_t N, const real *Jt, const real *Jf, const bool *
 }
 
 /* Second-order central-difference matrix I + grad(u) at voxel offset o,
- * the dfx_dx..dfz_dz macros of src/displacement_field_gradient.c:13-21. */
-static inline void m2_at(const grid_t *g, const real *f, size_t o, double m[3][3])
+ * the dfx_dx..dfz_dz macros of src/displacement_field_gradient.c:13-21.
+ * Column `skip` is not evaluated (set to 0): the cofactors taken at the
+ * neighbour p -/+ e_k never use the k column, and at p next to the boundary
+ * its differences would read outside the volume. */
+static inline void m2_at(const grid_t *g, const real *f, size_t o, int skip, double m[3][3])
 {
     for (int c = 0; c < 3; ++c)
         for (int ax = 0; ax < 3; ++ax) {
+            if (ax == skip) {
+                m[c][ax] = 0.0;
+                continue;
+            }
             const real *q = f + c * g->N + o;
             const ptrdiff_t s = (ptrdiff_t) g->st[ax];
             m[c][ax] = (q[s] - q[-s]) * g->ih[ax] * .5 + (c == ax ? 1.0 : 0.0);
@@ -216,8 +223,8 @@ void oracle_gradient(size_t nx, size_t ny, size_t nz, real dx, real dy, real dz,
                     if (Jf[ob] < delta) eb += zeta * (Jf[ob] - delta);
                     if (Jf[of] < delta) ef += zeta * (Jf[of] - delta);
                     double mb[3][3], mf[3][3];
-                    m2_at(&g, f, ob, mb);
-                    m2_at(&g, f, of, mf);
+                    m2_at(&g, f, ob, k, mb);
+                    m2_at(&g, f, of, k, mf);
                     for (int i = 0; i < 3; ++i)
                         t[i][k] = g.ih[k] * (+eb * minor2(mb, i, k) - ef * minor2(mf, i, k));
                 }
