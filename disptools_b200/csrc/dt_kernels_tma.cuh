@@ -36,7 +36,10 @@ constexpr int TMA_PLANE = TMA_PY * TMA_PX; // elements of one component plane of
 template <typename T>
 struct TrialTmaLayout {
     static constexpr int S = 3;  // pipeline stages
-    static constexpr int R = 3;  // candidate planes in shared memory (z, z+1, z+2)
+    // Candidate planes in shared memory: z (read by the stencil), z+1, z+2,
+    // and the one being formed, so forming the next plane needs no barrier
+    // against the current stencil reads.
+    static constexpr int R = 4;
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
     static constexpr int JT_BYTES = BX * TT_Y * (int) sizeof(T);
     static constexpr int MASK_BYTES = BX * TT_Y;
@@ -48,13 +51,14 @@ struct TrialTmaLayout {
 
 template <typename T>
 struct GradTmaLayout {
-    static constexpr int S = sizeof(T) == 4 ? 6 : 5;  // stages double as the plane ring (u, e')
+    static constexpr int S = sizeof(T) == 4 ? 5 : 4;  // stages double as the plane ring (u, e')
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
     static constexpr int E_BYTES = TMA_PLANE * (int) sizeof(T);
     static constexpr int STAGE_BYTES = U_BYTES + E_BYTES;
     static constexpr int PXP = BX + 2, PYP = TT_Y + 2;
-    static constexpr int P_OFF = S * STAGE_BYTES;  // P_x, P_y terms: [2][6][PYP][PXP]
-    static constexpr int P_BYTES = 2 * 6 * PYP * PXP * (int) sizeof(T);
+    static constexpr int NP = 3;  // planes of P_x, P_y terms (one barrier per plane)
+    static constexpr int P_OFF = S * STAGE_BYTES;  // P_x, P_y terms: [NP][6][PYP][PXP]
+    static constexpr int P_BYTES = NP * 6 * PYP * PXP * (int) sizeof(T);
     static constexpr int BAR_OFF = P_OFF + P_BYTES;
     static constexpr int BYTES = BAR_OFF + S * 8;
 };
@@ -92,12 +96,13 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     T *ring = reinterpret_cast<T *>(smem + L::RING_OFF);
     __shared__ double red[2 * (NT / 32)];
-    __shared__ int s_flag, s_ok;
+    __shared__ int s_flag, s_fault;
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
+        s_fault = 0;
     }
     __syncthreads();
     uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
@@ -168,19 +173,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
             const uint32_t k = kbase + it;
             const int s = k % L::S;
             const uint32_t par = (k / L::S) & 1u;
-            if (tid == 0) s_ok = mbar_wait_bounded(&bars[s], par);
-            __syncthreads();
-            if (!s_ok) {
-                failed = true;
-                fail_it = it;
-                break;
-            }
-            mbar_try_wait(&bars[s], par);  // completed: acquire the data for this thread
+            // Every thread waits for the stage itself (bounded); a timeout is
+            // agreed on after the barrier below, so all threads leave together.
+            const bool ok = mbar_wait_bounded(&bars[s], par);
+            if (!ok) s_fault = 1;
             const unsigned char *sb = smem + s * L::STAGE_BYTES;
             const int q = z0 - 2 + it, ze = q - 2;
             T *slot = ring + (size_t) ring_slot(q, L::R) * 3 * TMA_PLANE;
             // Candidate plane q (tile + halo): u - eta g, vectorised.
-            {
+            if (ok) {
                 constexpr int VEC = 16 / (int) sizeof(T);
                 using V4 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
                 const V4 *u4 = reinterpret_cast<const V4 *>(sb);
@@ -205,12 +206,17 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
             for (int r = 0; r < RY; ++r) {
                 jt[r] = T(0);
                 msk[r] = false;
-                if (eval) {
+                if (eval && ok) {
                     jt[r] = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid + r * NT];
                     msk[r] = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid + r * NT] != 0;
                 }
             }
             __syncthreads();
+            if (s_fault) {
+                failed = true;
+                fail_it = it;
+                break;
+            }
             if (tid == 0 && it + L::S < n_it) issue(it + L::S);
             // Shift the own-column queues by plane q; store the candidate.
 #pragma unroll
@@ -318,7 +324,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     T *pxy = reinterpret_cast<T *>(smem + L::P_OFF);
     __shared__ double red[2 * (NT / 32)];
-    __shared__ int s_flag, s_ok;
+    __shared__ int s_flag, s_fault;
     // P terms of the x (t = 0..2) and y (t = 3..5) directions, cell (ly, lx)
     // of the tile plus a halo of one.
     auto PT = [&](int slot, int t, int ly, int lx) -> T & {
@@ -329,6 +335,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
+        s_fault = 0;
     }
     __syncthreads();
     uint32_t kbase = 0;
@@ -384,14 +391,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
             const uint32_t k = kbase + it;
             const int s = k % L::S;
             const uint32_t par = (k / L::S) & 1u;
-            if (tid == 0) s_ok = mbar_wait_bounded(&bars[s], par);
-            __syncthreads();
-            if (!s_ok) {
-                failed = true;
-                fail_it = it;
-                break;
-            }
-            mbar_try_wait(&bars[s], par);
+            const bool ok = mbar_wait_bounded(&bars[s], par);
+            if (!ok) s_fault = 1;
             const int q = z0 - 2 + it;
             const int p = q - 1;  // plane of P computed now (needs u(q-2..q), e'(q-1))
             T pz_new[RY][3];
@@ -399,10 +400,10 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
             for (int r = 0; r < RY; ++r)
 #pragma unroll
                 for (int i = 0; i < 3; ++i) pz_new[r][i] = T(0);
-            if (it >= 2) {
+            if (it >= 2 && ok) {
                 const T *um = stage_u(it - 2), *u0 = stage_u(it - 1), *up = stage_u(it);
                 const T *e0 = stage_e(it - 1);
-                const int ps = p & 1;
+                const int ps = ring_slot(p, L::NP);
                 // M = I + grad u at box cell (lx, ly) of plane p, second order central.
                 auto mat = [&](int lx, int ly, T m[3][3]) {
 #pragma unroll
@@ -455,10 +456,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
                 }
             }
             __syncthreads();
+            if (s_fault) {
+                failed = true;
+                fail_it = it;
+                break;
+            }
             if (tid == 0 && it >= 2 && it - 2 + L::S < n_it) issue(it - 2 + L::S);
             const int z = q - 2;  // gradient plane: P(z-1), P(z), P(z+1) ready
             if (it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x >= 1 && x < g.nx - 1) {
-                const int ps = z & 1;
+                const int ps = ring_slot(z, L::NP);
 #pragma unroll
                 for (int r = 0; r < RY; ++r) {
                     const int y = y0 + ty + r * BY;
