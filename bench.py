@@ -274,6 +274,15 @@ def main():
 
     # ---- roofline of the dominant kernel (device time of the launches that did work)
     hbm, peak_kind = peaks()
+    # A trial is two launches: the interior (TMA) kernel and the boundary
+    # layers kernel; their summed time is the trial's duration.
+    if "boundary" in prof and "trial" in prof:
+        nb_, tb_ = prof.pop("boundary")
+        nt_, tt_ = prof["trial"]
+        prof["trial"] = (nt_, tt_ + tb_)
+        prof_boundary = (nb_, tb_)
+    else:
+        prof_boundary = None
     dom = max(prof, key=lambda k: prof[k][1]) if prof else "trial"
     nl, tot_ms = prof.get(dom, (0, 0.0))
     avg_ms = tot_ms / max(nl, 1)
@@ -292,6 +301,8 @@ def main():
                    if v[0] else None,
                    "share": v[1] / max(sum(x[1] for x in prof.values()), 1e-12)}
                for k, v in prof.items()}
+    if prof_boundary:
+        kernels["trial"]["boundary_avg_ms"] = prof_boundary[1] / max(prof_boundary[0], 1)
     path_achieved = (29 + 41 * tbar) * value / 1e9 / world
 
     # ---- plain FP64 path (same workload, fewer steps)
@@ -328,21 +339,27 @@ def main():
         stt = N.SolveStats()
 
         def e2e_step():
+            """One C-ABI call on host buffers; returns (stats, seconds).  The
+            zero initial guess is written before the timed call."""
             fh[...] = 0.0
+            t0 = time.perf_counter()
             rc = N.lib.dtb_generate_displacement(0, 0, n, n, n, 1.0, 1.0, 1.0, Jh.ctypes.data,
                                                  mh.ctypes.data, C.byref(p), fh.ctypes.data,
                                                  C.byref(stt))
+            dt_s = time.perf_counter() - t0
             N.check(rc)
-            return stt.as_dict()
+            return stt.as_dict(), dt_s
 
         e2e_step()
         barrier(world)
-        t0 = time.perf_counter()
+        te = 0.0
         ie = 0
         ke = max(1, min(args.steps, 3))
         for _ in range(ke):
-            ie += iterations_done(e2e_step())
-        te = max_over_ranks(world, time.perf_counter() - t0)
+            st_e, dt_s = e2e_step()
+            ie += iterations_done(st_e)
+            te += dt_s
+        te = max_over_ranks(world, te)
         e2e = {"value": sum_over_ranks(world, float(nvox) * ie) / te, "unit": UNIT,
                "h2d_bytes_per_step": int(Jh.nbytes + mh.nbytes + fh.nbytes),
                "d2h_bytes_per_step": int(fh.nbytes), "steps": ke,

@@ -243,39 +243,6 @@ struct DevVol {
     T *field;  // in: initial guess, out: result
 };
 
-// Device-resident solve of `vols` (all inputs already on the device).
-template <typename T>
-int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
-                    dtb_solve_stats *stats, int precision, cudaStream_t stream);
-
-// Runs the solve on a private non-blocking stream (graph capture is not
-// allowed on the legacy default stream), ordered after the caller's stream
-// and before anything the caller enqueues next.
-template <typename T>
-int solve_device(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
-                 dtb_solve_stats *stats, int precision, cudaStream_t user) {
-    cudaStream_t work;
-    DTB_CUDA(cudaStreamCreateWithFlags(&work, cudaStreamNonBlocking));
-    cudaEvent_t ev;
-    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
-        cudaStreamDestroy(work);
-        DTB_CUDA(cudaGetLastError());
-    }
-    int rc = DTB_OK;
-    if (cudaEventRecord(ev, user) != cudaSuccess || cudaStreamWaitEvent(work, ev, 0) != cudaSuccess) {
-        rc = DTB_ERR_CUDA;
-        set_error(__LINE__, __func__, "cannot order the solve after the caller's stream");
-    } else {
-        rc = solve_device_on<T>(algorithm, vols, p, stats, precision, work);
-        if (cudaEventRecord(ev, work) == cudaSuccess) cudaStreamWaitEvent(user, ev, 0);
-    }
-    cudaStreamSynchronize(work);
-    cudaEventDestroy(ev);
-    cudaStreamDestroy(work);
-    cudaGetLastError();
-    return rc;
-}
-
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // dependency on libcuda).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -339,10 +306,113 @@ int num_sms() {
     return n;
 }
 
+// Per-device resources that live across solves: the solver's own stream,
+// pinned host mirrors, events and the captured step graph (reused while the
+// launch configuration is unchanged).
+struct GraphKey {
+    size_t tsize = 0;
+    int algorithm = -1;
+    const void *desc = nullptr;
+    const int *tile_vol = nullptr;
+    int total_tiles = 0, grid_t = 0, grid_g = 0, grid_b = 0, K = 0, threads_y = 0;
+    const unsigned char *flags = nullptr;
+    bool operator==(const GraphKey &o) const {
+        return tsize == o.tsize && algorithm == o.algorithm && desc == o.desc && tile_vol == o.tile_vol &&
+               total_tiles == o.total_tiles && grid_t == o.grid_t && grid_g == o.grid_g && grid_b == o.grid_b &&
+               K == o.K && threads_y == o.threads_y && flags == o.flags;
+    }
+};
+
+struct Engine {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_order = nullptr;
+    SolverState *h_states = nullptr;
+    size_t states_cap = 0;
+    unsigned char *h_flags = nullptr;
+    unsigned char *d_flags = nullptr;
+    size_t flags_cap = 0;
+    std::vector<cudaEvent_t> evs;
+    cudaGraphExec_t exec = nullptr;
+    GraphKey key;
+};
+std::vector<Engine *> g_engines;
+
+// The engine of the current device (created on first use).
+int engine(Engine **out) {
+    int dev = 0;
+    DTB_CUDA(cudaGetDevice(&dev));
+    if ((int) g_engines.size() <= dev) g_engines.resize(dev + 1, nullptr);
+    Engine *e = g_engines[dev];
+    if (!e) {
+        e = new Engine();
+        e->device = dev;
+        DTB_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        DTB_CUDA(cudaEventCreate(&e->ev0));
+        DTB_CUDA(cudaEventCreate(&e->ev1));
+        DTB_CUDA(cudaEventCreateWithFlags(&e->ev_order, cudaEventDisableTiming));
+        g_engines[dev] = e;
+    }
+    *out = e;
+    return DTB_OK;
+}
+
+int ensure_host_states(Engine *e, size_t count) {
+    if (e->states_cap >= count) return DTB_OK;
+    if (e->h_states) cudaFreeHost(e->h_states);
+    e->h_states = nullptr;
+    e->states_cap = 0;
+    DTB_CUDA(cudaMallocHost(&e->h_states, count * sizeof(SolverState)));
+    e->states_cap = count;
+    return DTB_OK;
+}
+
+int ensure_profiling(Engine *e, size_t nk) {
+    if (e->flags_cap < nk) {
+        if (e->h_flags) cudaFreeHost(e->h_flags);
+        if (e->d_flags) cudaFree(e->d_flags);
+        e->h_flags = e->d_flags = nullptr;
+        e->flags_cap = 0;
+        DTB_CUDA(cudaMallocHost(&e->h_flags, nk));
+        DTB_CUDA(cudaMalloc(&e->d_flags, nk));
+        e->flags_cap = nk;
+    }
+    while (e->evs.size() < nk + 1) {
+        cudaEvent_t ev;
+        DTB_CUDA(cudaEventCreate(&ev));
+        e->evs.push_back(ev);
+    }
+    return DTB_OK;
+}
+
+// Tile and block shape of the TMA kernels.  FP32 tiles are 64 voxels wide
+// (long contiguous TMA rows); FP64 tiles 32 (their shared-memory footprint
+// doubles).  Blocks have 8 thread rows (two tile rows each) unless
+// DISPTOOLS_B200_THREADS_Y=16 (32-wide tiles only).
+int pick_tile_x(size_t tsize) {
+    const char *e = std::getenv("DISPTOOLS_B200_TILE_X");
+    if (e && tsize == 4) {
+        const int v = std::atoi(e);
+        if (v == 32 || v == 64) return v;
+    }
+    return tsize == 4 ? 64 : 32;
+}
+int pick_threads_y(int tile_x) {
+    const char *e = std::getenv("DISPTOOLS_B200_THREADS_Y");
+    if (e && tile_x == 32) {
+        const int v = std::atoi(e);
+        if (v == 8 || v == 16) return v;
+    }
+    return 8;
+}
+
 template <typename T>
-int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
-                    dtb_solve_stats *stats, int precision, cudaStream_t stream) {
+int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                    dtb_solve_stats *stats, int precision) {
+    cudaStream_t stream = e->stream;
     const int count = (int) vols.size();
+    const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? pick_tile_x(sizeof(T)) : BX;
+    const int threads_y = pick_threads_y(tile_x);
     const bool gradient = algorithm == DTB_ALGORITHM_GRADIENT;
     // ---- workspace layout: every buffer of the solve is the library's own,
     // in the pitched layout.
@@ -356,7 +426,7 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         const Geom g = pitched(vols[i].g);
         geo[i] = g;
         const int bz = pick_bz(g.nz);
-        const int t = ((g.nx + BX - 1) / BX) * ((g.ny + tile_y - 1) / tile_y) * ((g.nz + bz - 1) / bz);
+        const int t = ((g.nx + tile_x - 1) / tile_x) * ((g.ny + tile_y - 1) / tile_y) * ((g.nz + bz - 1) / bz);
         tiles[i] = t;
         tbegin[i] = total_tiles;
         total_tiles += t;
@@ -367,9 +437,8 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         need += align(t * sizeof(double2)) + align(t * sizeof(double));
         need += align(sizeof(SolverState)) + align(7 * sizeof(CUtensorMap));
     }
-    need += align(count * sizeof(VolumeDesc<T>)) + align(total_tiles * sizeof(int));
+    need += align(count * sizeof(VolumeDesc<T>)) + align(total_tiles * sizeof(int)) + align(2 * sizeof(TileQueue));
 
-    std::lock_guard<std::mutex> lock(g_ws_mutex);
     char *base = nullptr;
     int rc = workspace(need, &base);
     if (rc != DTB_OK) return rc;
@@ -406,7 +475,7 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         d.st = cv.take<SolverState>(1);
         d_maps[i] = cv.take<CUtensorMap>(7);
         const int bz = pick_bz(g.nz);
-        d.tiles_x = (g.nx + BX - 1) / BX;
+        d.tiles_x = (g.nx + tile_x - 1) / tile_x;
         d.tiles_y = (g.ny + tile_y - 1) / tile_y;
         d.tiles_z = (g.nz + bz - 1) / bz;
         d.tile_begin = tbegin[i];
@@ -452,14 +521,16 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
             const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
             // Boxes: the tile plus 4 voxels in x (16-byte aligned start) and 2
             // rows in y for the stencil inputs; the bare tile for J_t and the mask.
-            bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, BX + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, BX + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, BX + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[3], ft, sizeof(T), d.ep[0], g, 1, BX + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[4], ft, sizeof(T), d.ep[1], g, 1, BX + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[5], ft, sizeof(T), Jt, g, 1, BX, TT_Y) &&
-                      encode_map(&h_maps[6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, g, 1, BX, TT_Y);
+            const uint32_t bx = (uint32_t) tile_x;
+            bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, bx + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, bx + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, bx + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[3], ft, sizeof(T), d.ep[0], g, 1, bx + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[4], ft, sizeof(T), d.ep[1], g, 1, bx + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[5], ft, sizeof(T), Jt, g, 1, bx, TT_Y) &&
+                      encode_map(&h_maps[6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, g, 1, bx, TT_Y);
             if (!ok) DTB_FAIL(DTB_ERR_CUDA, "cannot encode the TMA descriptors (cuTensorMapEncodeTiled)");
+            // From pageable memory: the copy is staged before the call returns.
             DTB_CUDA(cudaMemcpyAsync(d_maps[i], h_maps, sizeof h_maps, cudaMemcpyHostToDevice, stream));
             d.tm_field[0] = d_maps[i] + 0;
             d.tm_field[1] = d_maps[i] + 1;
@@ -468,12 +539,12 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
             d.tm_ep[1] = d_maps[i] + 4;
             d.tm_Jt = d_maps[i] + 5;
             d.tm_mask = d_maps[i] + 6;
-            // The host copy of the maps must outlive the asynchronous copy.
-            DTB_CUDA(cudaStreamSynchronize(stream));
         }
     }
     VolumeDesc<T> *d_desc = cv.take<VolumeDesc<T>>(count);
     int *d_tile_vol = cv.take<int>(total_tiles);
+    TileQueue *d_queues = cv.take<TileQueue>(2);  // trial, gradient
+    DTB_CUDA(cudaMemsetAsync(d_queues, 0, 2 * sizeof(TileQueue), stream));
     std::vector<SolverState *> d_states(count);
     for (int i = 0; i < count; ++i) {
         d_states[i] = desc[i].st;
@@ -482,24 +553,23 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     DTB_CUDA(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(VolumeDesc<T>), cudaMemcpyHostToDevice, stream));
     DTB_CUDA(cudaMemcpyAsync(d_tile_vol, tile_vol.data(), total_tiles * sizeof(int), cudaMemcpyHostToDevice,
                              stream));
-    // Host vectors handed to async copies must stay alive until they ran.
-    DTB_CUDA(cudaStreamSynchronize(stream));
+
 
     // Persistent grids: as many blocks as fit on the device at once.
-    const int grid_t = gradient ? std::min(total_tiles, std::max(1, trial_tma_blocks_per_sm<T>()) * num_sms())
+    const int grid_t = gradient ? std::min(total_tiles, std::max(1, trial_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms())
                                 : total_tiles;
-    const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>()) * num_sms());
+    const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms());
     auto launch_t = [&](unsigned char *flag) -> cudaError_t {
-        if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
+        if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, threads_y,
+                                                    d_queues);
         return launch_trial<T>(MODE_GREEDY, d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
     };
     auto launch_g = [&](unsigned char *flag) -> cudaError_t {
-        return launch_gradient_tma<T>(d_desc, d_tile_vol, total_tiles, grid_g, stream, flag);
+        return launch_gradient_tma<T>(d_desc, d_tile_vol, total_tiles, grid_g, stream, flag, tile_x, threads_y,
+                                      d_queues + 1);
     };
 
-    cudaEvent_t ev0, ev1;
-    DTB_CUDA(cudaEventCreate(&ev0));
-    DTB_CUDA(cudaEventCreate(&ev1));
+    cudaEvent_t ev0 = e->ev0, ev1 = e->ev1;
     DTB_CUDA(cudaEventRecord(ev0, stream));
 
     // Evaluate the initial fields (launched once, outside the graph; this is
@@ -507,51 +577,69 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     DTB_CUDA(launch_t(nullptr));
     if (gradient) DTB_CUDA(launch_g(nullptr));
 
-    // Capture K steps into a graph.  With profiling on, event records are
-    // captured between the kernels and every kernel gets a flag that it sets
-    // when it did work.
+    // Capture K steps into a graph (reused while the configuration is the
+    // same).  With profiling on, event records are captured between the
+    // kernels and every kernel gets a flag that it sets when it did work.
     const int K = steps_per_graph();
     const bool prof = g_prof.on;
     const int kernels_per_step = gradient ? 2 : 1;
     const int nk = K * kernels_per_step;
-    std::vector<cudaEvent_t> evs(prof ? nk + 1 : 0);
-    unsigned char *d_flags = nullptr, *h_flags = nullptr;
     if (prof) {
-        for (auto &e : evs) DTB_CUDA(cudaEventCreate(&e));
-        DTB_CUDA(cudaMalloc(&d_flags, nk));
-        DTB_CUDA(cudaMallocHost(&h_flags, nk));
+        rc = ensure_profiling(e, nk);
+        if (rc != DTB_OK) return rc;
     }
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    set_capturing(true);
-    DTB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    // Inside a capture only cudaEventRecordExternal turns a record into an
-    // event-record node that fires on every replay.
-    if (prof) {
-        cudaMemsetAsync(d_flags, 0, nk, stream);
-        cudaEventRecordWithFlags(evs[0], stream, cudaEventRecordExternal);
-    }
-    for (int k = 0, j = 0; k < K; ++k) {
-        if (gradient) {
-            launch_g(prof ? d_flags + j : nullptr);
+    std::vector<cudaEvent_t> &evs = e->evs;
+    unsigned char *d_flags = prof ? e->d_flags : nullptr, *h_flags = prof ? e->h_flags : nullptr;
+    GraphKey key;
+    key.tsize = sizeof(T);
+    key.algorithm = algorithm;
+    key.desc = d_desc;
+    key.tile_vol = d_tile_vol;
+    key.total_tiles = total_tiles;
+    key.grid_t = grid_t;
+    key.grid_g = grid_g;
+    key.K = K;
+    key.threads_y = threads_y * 1000 + tile_x;
+    key.flags = d_flags;
+    if (!(e->exec && e->key == key)) {
+        if (e->exec) cudaGraphExecDestroy(e->exec);
+        e->exec = nullptr;
+        cudaGraph_t graph = nullptr;
+        set_capturing(true);
+        DTB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        // Inside a capture only cudaEventRecordExternal turns a record into an
+        // event-record node that fires on every replay.
+        if (prof) {
+            cudaMemsetAsync(d_flags, 0, nk, stream);
+            cudaEventRecordWithFlags(evs[0], stream, cudaEventRecordExternal);
+        }
+        for (int k = 0, j = 0; k < K; ++k) {
+            if (gradient) {
+                launch_g(prof ? d_flags + j : nullptr);
+                if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
+                ++j;
+            }
+            launch_t(prof ? d_flags + j : nullptr);
             if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
             ++j;
         }
-        launch_t(prof ? d_flags + j : nullptr);
-        if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
-        ++j;
+        cudaError_t cap = cudaStreamEndCapture(stream, &graph);
+        set_capturing(false);
+        if (cap != cudaSuccess) {
+            cudaGetLastError();
+            DTB_CUDA(cap);
+        }
+        cudaError_t inst = cudaGraphInstantiate(&e->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        DTB_CUDA(inst);
+        e->key = key;
     }
-    cudaError_t cap = cudaStreamEndCapture(stream, &graph);
-    set_capturing(false);
-    if (cap != cudaSuccess) {
-        cudaGetLastError();
-        DTB_CUDA(cap);
-    }
-    DTB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphExec_t exec = e->exec;
 
     // Host copy of the states, refreshed once per graph launch.
-    SolverState *h_states = nullptr;
-    DTB_CUDA(cudaMallocHost(&h_states, count * sizeof(SolverState)));
+    rc = ensure_host_states(e, count);
+    if (rc != DTB_OK) return rc;
+    SolverState *h_states = e->h_states;
     long long max_steps = 0;
     for (int i = 0; i < count; ++i) max_steps = std::max(max_steps, 64 * (p.it_max + 2) + 4096);
     long long steps = 0;
@@ -594,35 +682,18 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
         }
     }
     const cudaError_t rec_err = cudaEventRecord(ev1, stream);
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
-    if (prof) {
-        for (auto &e : evs) cudaEventDestroy(e);
-        cudaFree(d_flags);
-        cudaFreeHost(h_flags);
-    }
-    cudaGetLastError();  // nothing above may leave a stale error for the next call
     if (status == DTB_OK && rec_err != cudaSuccess) {
         status = DTB_ERR_CUDA;
         loop_err = rec_err;
     }
-    if (status == DTB_ERR_CUDA) {
-        cudaFreeHost(h_states);
-        DTB_CUDA(loop_err != cudaSuccess ? loop_err : cudaErrorUnknown);
-    }
-    if (status != DTB_OK) {
-        cudaFreeHost(h_states);
-        DTB_FAIL(status, "the solver did not terminate within its step bound");
-    }
+    if (status == DTB_ERR_CUDA) DTB_CUDA(loop_err != cudaSuccess ? loop_err : cudaErrorUnknown);
+    if (status != DTB_OK) DTB_FAIL(status, "the solver did not terminate within its step bound");
 
     // Results: the accepted field is field[old_buf]; copy it back into the
     // caller's dense buffer.
     for (int i = 0; i < count; ++i) {
         const SolverState &s = h_states[i];
-        if (s.fault) {
-            cudaFreeHost(h_states);
-            DTB_FAIL(DTB_ERR_CUDA, "a TMA transfer did not complete within its bound");
-        }
+        if (s.fault) DTB_FAIL(DTB_ERR_CUDA, "a TMA transfer did not complete within its bound");
         const Geom &gu = vols[i].g;
         DTB_CUDA(copy_rows<T>(vols[i].field, gu.ys, desc[i].field[s.old_buf], geo[i].ys, gu.nx,
                               3 * (size_t) gu.ny * gu.nz, stream));
@@ -630,8 +701,6 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
     DTB_CUDA(cudaEventSynchronize(ev1));
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ev0, ev1) != cudaSuccess) ms = -1.f;
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
     cudaGetLastError();
     if (stats) {
         for (int i = 0; i < count; ++i) {
@@ -650,8 +719,27 @@ int solve_device_on(int algorithm, const std::vector<DevVol<T>> &vols, const dtb
             o.device_ms = ms;
         }
     }
-    cudaFreeHost(h_states);
     return DTB_OK;
+}
+
+// Device-resident solve of `vols` (all inputs already on the device), on the
+// engine's own non-blocking stream (graph capture is not allowed on the
+// legacy default stream), ordered after the caller's stream and before
+// anything the caller enqueues next.
+template <typename T>
+int solve_device(int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                 dtb_solve_stats *stats, int precision, cudaStream_t user) {
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    Engine *e = nullptr;
+    int rc = engine(&e);
+    if (rc != DTB_OK) return rc;
+    DTB_CUDA(cudaEventRecord(e->ev_order, user));
+    DTB_CUDA(cudaStreamWaitEvent(e->stream, e->ev_order, 0));
+    rc = solve_device_on<T>(e, algorithm, vols, p, stats, precision);
+    if (cudaEventRecord(e->ev_order, e->stream) == cudaSuccess) cudaStreamWaitEvent(user, e->ev_order, 0);
+    cudaStreamSynchronize(e->stream);
+    cudaGetLastError();
+    return rc;
 }
 
 bool check_params(const dtb_params &p, const char **why) {

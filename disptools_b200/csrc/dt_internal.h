@@ -53,6 +53,14 @@ struct SolverState {
     int fault;               // a bounded wait gave up (reported as an error)
 };
 
+// Dynamic tile queue of one persistent launch: blocks take tiles with an
+// atomic counter; the last block to leave resets the queue for the next
+// launch (every block increments `exited` exactly once, after its last take).
+struct TileQueue {
+    unsigned int next;
+    unsigned int exited;
+};
+
 // Geometry of one volume on the device.
 struct Geom {
     int nx, ny, nz;
@@ -107,16 +115,19 @@ cudaError_t launch_trial(int mode, const VolumeDesc<T> *vols, const int *tile_vo
 template <typename T>
 cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
                             int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
+// TMA kernels of the gradient method; tiles are tile_x (64 or 32) by TT_Y
+// voxels, blocks tile_x by threads_y (8 or 16) threads.
 template <typename T>
 cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                             cudaStream_t s, unsigned char *work_flag = nullptr);
+                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *queue);
 template <typename T>
 cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                                cudaStream_t s, unsigned char *work_flag = nullptr);
+                                cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y,
+                                TileQueue *queue);
 template <typename T>
-int trial_tma_blocks_per_sm();
+int trial_tma_blocks_per_sm(int tile_x, int threads_y);
 template <typename T>
-int gradient_tma_blocks_per_sm();
+int gradient_tma_blocks_per_sm(int tile_x, int threads_y);
 template <typename T>
 cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s);
 template <typename T>

@@ -257,26 +257,67 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
-// Returns (sum, max) of the block in thread 0.
+// Returns (sum, max) of a block of NTH threads in thread 0; `red` holds
+// 2 * NTH / 32 doubles.
+template <int NTH = NT>
 __device__ __forceinline__ double2 block_reduce(double s, double m, double *red) {
+    static_assert(NTH <= 1024 && NTH % 32 == 0, "block size");
     const int tid = threadIdx.y * BX + threadIdx.x;
     s = warp_sum(s);
     m = warp_max(m);
     if ((tid & 31) == 0) {
         red[tid >> 5] = s;
-        red[NT / 32 + (tid >> 5)] = m;
+        red[NTH / 32 + (tid >> 5)] = m;
     }
     __syncthreads();
     double2 r = make_double2(0.0, 0.0);
     if (tid < 32) {
-        s = tid < NT / 32 ? red[tid] : 0.0;
-        m = tid < NT / 32 ? red[NT / 32 + tid] : 0.0;
+        s = tid < NTH / 32 ? red[tid] : 0.0;
+        m = tid < NTH / 32 ? red[NTH / 32 + tid] : 0.0;
         s = warp_sum(s);
         m = warp_max(m);
         r = make_double2(s, m);
     }
     __syncthreads();
     return r;
+}
+
+// block_reduce for blocks TXW threads wide.
+template <int NTH, int TXW>
+__device__ __forceinline__ double2 block_reduce_n(double s, double m, double *red) {
+    static_assert(NTH <= 1024 && NTH % 32 == 0, "block size");
+    const int tid = threadIdx.y * TXW + threadIdx.x;
+    s = warp_sum(s);
+    m = warp_max(m);
+    if ((tid & 31) == 0) {
+        red[tid >> 5] = s;
+        red[NTH / 32 + (tid >> 5)] = m;
+    }
+    __syncthreads();
+    double2 r = make_double2(0.0, 0.0);
+    if (tid < 32) {
+        s = tid < NTH / 32 ? red[tid] : 0.0;
+        m = tid < NTH / 32 ? red[NTH / 32 + tid] : 0.0;
+        s = warp_sum(s);
+        m = warp_max(m);
+        r = make_double2(s, m);
+    }
+    __syncthreads();
+    return r;
+}
+
+template <int TXW>
+__device__ __forceinline__ bool publish_partial_n(unsigned int *ticket, int ntiles, int *s_flag) {
+    const int tid = threadIdx.y * TXW + threadIdx.x;
+    if (tid == 0) {
+        __threadfence();
+        const unsigned int t = atomicAdd(ticket, 1u);
+        *s_flag = (t == (unsigned int) (ntiles - 1));
+    }
+    __syncthreads();
+    const bool last = *s_flag;
+    if (last) __threadfence();
+    return last;
 }
 
 // Publishes a tile partial and returns true in every thread of the block

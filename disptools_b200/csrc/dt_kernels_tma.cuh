@@ -1,7 +1,7 @@
 // TMA-pipelined kernels of the gradient method (sm_100a).
 //
-// Both kernels march a BX x TT_Y tile (two rows per thread) through its z
-// range.  One elected thread streams one box per input per plane into a ring
+// Both kernels march a TXW x TT_Y tile (TT_Y / TYT rows per thread) through
+// its z range.  One elected thread streams one box per input per plane into a ring
 // of shared-memory stages with cp.async.bulk.tensor, completion tracked by an
 // mbarrier per stage; the other threads issue no global loads for the stencil
 // inputs.  Boxes start 4 voxels left of the tile so the innermost TMA
@@ -26,42 +26,73 @@
 
 namespace dtb {
 
-constexpr int RY = TT_Y / BY;              // rows per thread
 constexpr int TMA_HX = 4;                  // x halo of the boxes (16-byte aligned start)
 constexpr int TMA_HY = 2;                  // y halo
-constexpr int TMA_PX = BX + 2 * TMA_HX;    // 40
 constexpr int TMA_PY = TT_Y + 2 * TMA_HY;  // 20
-constexpr int TMA_PLANE = TMA_PY * TMA_PX; // elements of one component plane of a box
 
-template <typename T>
+// Box geometry of a tile TXW voxels wide: TXW + 8 by TT_Y + 4 per plane.
+template <int TXW>
+struct Box {
+    static constexpr int PX = TXW + 2 * TMA_HX;
+    static constexpr int PLANE = TMA_PY * PX;  // elements of one component plane
+};
+
+template <typename T, int TXW>
 struct TrialTmaLayout {
+    static constexpr int TMA_PX = Box<TXW>::PX;
+    static constexpr int TMA_PLANE = Box<TXW>::PLANE;
     static constexpr int S = 3;  // pipeline stages
     // Candidate planes in shared memory: z (read by the stencil), z+1, z+2,
     // and the one being formed, so forming the next plane needs no barrier
     // against the current stencil reads.
     static constexpr int R = 4;
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
-    static constexpr int JT_BYTES = BX * TT_Y * (int) sizeof(T);
-    static constexpr int MASK_BYTES = BX * TT_Y;
+    static constexpr int JT_BYTES = TXW * TT_Y * (int) sizeof(T);
+    static constexpr int MASK_BYTES = TXW * TT_Y;
     static constexpr int STAGE_BYTES = 2 * U_BYTES + JT_BYTES + MASK_BYTES;  // u, g, Jt, mask
     static constexpr int RING_OFF = S * STAGE_BYTES;
     static constexpr int BAR_OFF = RING_OFF + R * U_BYTES;
     static constexpr int BYTES = BAR_OFF + S * 8;
 };
 
-template <typename T>
+template <typename T, int TXW>
 struct GradTmaLayout {
+    static constexpr int TMA_PX = Box<TXW>::PX;
+    static constexpr int TMA_PLANE = Box<TXW>::PLANE;
     static constexpr int S = sizeof(T) == 4 ? 5 : 4;  // stages double as the plane ring (u, e')
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
     static constexpr int E_BYTES = TMA_PLANE * (int) sizeof(T);
     static constexpr int STAGE_BYTES = U_BYTES + E_BYTES;
-    static constexpr int PXP = BX + 2, PYP = TT_Y + 2;
+    static constexpr int PXP = TXW + 2, PYP = TT_Y + 2;
     static constexpr int NP = 3;  // planes of P_x, P_y terms (one barrier per plane)
     static constexpr int P_OFF = S * STAGE_BYTES;  // P_x, P_y terms: [NP][6][PYP][PXP]
     static constexpr int P_BYTES = NP * 6 * PYP * PXP * (int) sizeof(T);
     static constexpr int BAR_OFF = P_OFF + P_BYTES;
     static constexpr int BYTES = BAR_OFF + S * 8;
 };
+
+// Takes the next tile of a persistent launch (-1 when none is left; the
+// block is then counted out and the last one resets the queue).
+template <int TXW>
+__device__ __forceinline__ int take_tile(TileQueue *q, int total, int *s_tile) {
+    const int tid = threadIdx.y * TXW + threadIdx.x;
+    __syncthreads();  // everyone has read the previous s_tile
+    if (tid == 0) {
+        int t = (int) atomicAdd(&q->next, 1u);
+        if (t >= total) {
+            t = -1;
+            __threadfence();
+            if (atomicAdd(&q->exited, 1u) == gridDim.x - 1) {
+                q->next = 0;
+                q->exited = 0;
+                __threadfence();
+            }
+        }
+        *s_tile = t;
+    }
+    __syncthreads();
+    return *s_tile;
+}
 
 // TMA destinations must be 128-byte aligned in the shared window; the launch
 // asks for 128 spare bytes.
@@ -84,21 +115,24 @@ __device__ __forceinline__ void tma_fault(SolverState *st, uint64_t *bars, uint3
     }
 }
 
-// Two resident blocks per SM for FP32 (shared memory allows no more), one for
-// FP64; the bound lets the compiler use up to 128 / 255 registers.
-template <typename T>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const VolumeDesc<T> *__restrict__ vols,
+// TYT threads along y (each thread owns TT_Y / TYT rows of the tile).  Two
+// resident blocks per SM for FP32 (shared memory allows no more), one for
+// FP64; the bound caps the registers accordingly.
+template <typename T, int TXW, int TYT>
+__global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 ? 2 : 1) k_trial_tma(const VolumeDesc<T> *__restrict__ vols,
                                                   const int *__restrict__ tile_vol, int total_tiles,
-                                                  unsigned char *__restrict__ work_flag) {
-    using L = TrialTmaLayout<T>;
+                                                  unsigned char *__restrict__ work_flag, TileQueue *queue) {
+    using L = TrialTmaLayout<T, TXW>;
+    constexpr int NTH = TXW * TYT, RYT = TT_Y / TYT;
+    constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char *smem = align_smem_128(smem_dyn);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     T *ring = reinterpret_cast<T *>(smem + L::RING_OFF);
-    __shared__ double red[2 * (NT / 32)];
+    __shared__ double red[2 * (NTH / 32)];
     __shared__ int s_flag, s_fault;
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TXW + tx;
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -107,7 +141,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
     __syncthreads();
     uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
 
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    __shared__ int s_tile;
+    for (int tile = take_tile<TXW>(queue, total_tiles, &s_tile); tile >= 0;
+         tile = take_tile<TXW>(queue, total_tiles, &s_tile)) {
         const VolumeDesc<T> &V = vols[tile_vol[tile]];
         SolverState *st = V.st;
         if (ldcg_int(&st->done)) continue;
@@ -118,7 +154,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
         const bool trial = phase != PH_EVAL0;
         const int lt = tile - V.tile_begin;
         const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
-        const int x0 = txi * BX, y0 = tyi * TT_Y, z0 = tzi * V.bz;
+        const int x0 = txi * TXW, y0 = tyi * TT_Y, z0 = tzi * V.bz;
         const int z1 = min(z0 + V.bz, g.nz);
         const int n_it = z1 - z0 + 4;  // candidate planes z0-2 .. z1+1
         const CUtensorMap *tm_u = V.tm_field[old_b];
@@ -159,14 +195,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
 
         const int x = x0 + tx;
         // Own columns: candidate values of planes q-4 .. q (z differences).
-        T zq[RY][3][5];
+        T zq[RYT][3][5];
 #pragma unroll
-        for (int r = 0; r < RY; ++r)
+        for (int r = 0; r < RYT; ++r)
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
                 for (int k = 0; k < 5; ++k) zq[r][c][k] = T(0);
-        double acc_s = 0.0, acc_m = 0.0;
+        double acc_s = 0.0;
+        T acc_mt = T(0);
         bool failed = false;
         int fail_it = 0;
         for (int it = 0; it < n_it; ++it) {
@@ -187,7 +224,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
                 const V4 *u4 = reinterpret_cast<const V4 *>(sb);
                 const V4 *g4 = reinterpret_cast<const V4 *>(sb + L::U_BYTES);
                 V4 *c4 = reinterpret_cast<V4 *>(slot);
-                for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NT) {
+                for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NTH) {
                     V4 a = u4[i];
                     if (trial) {
                         const V4 b = g4[i];
@@ -200,15 +237,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
                 }
             }
             const bool eval = ze >= z0 && ze < z1;
-            T jt[RY];
-            bool msk[RY];
+            T jt[RYT];
+            bool msk[RYT];
 #pragma unroll
-            for (int r = 0; r < RY; ++r) {
+            for (int r = 0; r < RYT; ++r) {
                 jt[r] = T(0);
                 msk[r] = false;
                 if (eval && ok) {
-                    jt[r] = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid + r * NT];
-                    msk[r] = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid + r * NT] != 0;
+                    jt[r] = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid + r * NTH];
+                    msk[r] = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid + r * NTH] != 0;
                 }
             }
             __syncthreads();
@@ -220,15 +257,15 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
             if (tid == 0 && it + L::S < n_it) issue(it + L::S);
             // Shift the own-column queues by plane q; store the candidate.
 #pragma unroll
-            for (int r = 0; r < RY; ++r) {
-                const int ly = ty + r * BY + TMA_HY;
+            for (int r = 0; r < RYT; ++r) {
+                const int ly = ty + r * TYT + TMA_HY;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) zq[r][c][kk] = zq[r][c][kk + 1];
                     zq[r][c][4] = slot[c * TMA_PLANE + ly * TMA_PX + tx + TMA_HX];
                 }
-                const int y = y0 + ty + r * BY;
+                const int y = y0 + ty + r * TYT;
                 if (trial && x < g.nx && y < g.ny && q >= z0 && q < z1) {
                     const long long so = (long long) q * g.zs + (long long) y * g.ys + x;
 #pragma unroll
@@ -237,22 +274,62 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
             }
             if (eval) {
                 const T *jp = ring + (size_t) ring_slot(ze, L::R) * 3 * TMA_PLANE;
-                const bool fast_xz = x0 >= 2 && x0 + BX <= g.nx - 2 && ze >= 2 && ze <= g.nz - 3 && g.order == 4;
+                // Fourth-order weights with the spacing folded in (FP32); the
+                // FP64 path keeps the reference's operation order.
+                const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
+                const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1],
+                                 FD<T>::one_twelfth * ih[2]};
+                auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
+                    if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+                    return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
+                };
+                // Three evaluators, chosen per warp (a warp is 32 voxels of one
+                // row): rows and planes inside [2, n-3] away from the x ends use
+                // the fourth-order stencil only; interior rows that reach an x
+                // end select the scheme per lane without branching; rows or
+                // planes on the two outer layers take the general path.
+                const bool plane_in = ze >= 2 && ze <= g.nz - 3;
+                const int xw0 = x0 + (tx & ~31);
+                const bool warp_x_in = xw0 >= 2 && xw0 + 31 <= g.nx - 3;
 #pragma unroll
-                for (int r = 0; r < RY; ++r) {
-                    const int y = y0 + ty + r * BY;
-                    if (x >= g.nx || y >= g.ny) continue;
-                    const int lx = tx + TMA_HX, ly = ty + r * BY + TMA_HY;
+                for (int r = 0; r < RYT; ++r) {
+                    const int y = y0 + ty + r * TYT;
+                    const bool row_in = plane_in && y >= 2 && y <= g.ny - 3;
+                    const int lx = tx + TMA_HX, ly = ty + r * TYT + TMA_HY;
                     T a[3][3];
-                    if (fast_xz && y >= 2 && y <= g.ny - 3) {
+                    if (row_in && warp_x_in) {
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
                             const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
-                            a[c][0] = fd_c4<T>(p[1], p[-1], p[2], p[-2], ih[0]);
-                            a[c][1] = fd_c4<T>(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], ih[1]);
-                            a[c][2] = fd_c4<T>(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0], ih[2]);
+                            a[c][0] = c4(p[1], p[-1], p[2], p[-2], 0);
+                            a[c][1] = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
+                            a[c][2] = c4(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0], 2);
+                        }
+                    } else if (row_in) {
+                        if (x >= g.nx) continue;
+                        // Interior row: the scheme depends on x only
+                        // (src/jacobian.c:113-241): outer column -> one-sided
+                        // in x and second-order central in y, z; penultimate
+                        // column -> second-order central; else fourth order.
+                        const bool xo_lo = x == 0, xo_hi = x == g.nx - 1;
+                        const bool second = xo_lo || xo_hi || x == 1 || x == g.nx - 2;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+                            const T fx = xo_lo ? fd_fwd<T>(p[0], p[1], p[2], ih[0])
+                                               : (xo_hi ? fd_bwd<T>(p[0], p[-1], p[-2], ih[0])
+                                                        : fd_c2<T>(p[1], p[-1], ih[0]));
+                            const T cx4 = c4(p[1], p[-1], p[2], p[-2], 0);
+                            a[c][0] = second ? fx : cx4;
+                            const T cy4 = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
+                            const T cy2 = fd_c2<T>(p[TMA_PX], p[-TMA_PX], ih[1]);
+                            a[c][1] = second ? cy2 : cy4;
+                            const T cz4 = c4(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0], 2);
+                            const T cz2 = fd_c2<T>(zq[r][c][3], zq[r][c][1], ih[2]);
+                            a[c][2] = second ? cz2 : cz4;
                         }
                     } else {
+                        if (x >= g.nx || y >= g.ny) continue;
                         int kk[3];
                         schemes_at(x, y, ze, g, kk);
 #pragma unroll
@@ -268,7 +345,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
                                 case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
                                 case S_BWD: d = fd_bwd<T>(w[2], w[1], w[0], ih[ax]); break;
                                 case S_C2: d = fd_c2<T>(w[3], w[1], ih[ax]); break;
-                                default: d = fd_c4<T>(w[3], w[1], w[4], w[0], ih[ax]); break;
+                                default: d = c4(w[3], w[1], w[4], w[0], ax); break;
                                 }
                                 a[c][ax] = d;
                             }
@@ -277,8 +354,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
                     const T J = det_i_plus<T>(a);
                     const T vv = voxel_error<T>(J, jt[r], msk[r], tol);
                     acc_s += (double) vv * (double) vv;
-                    const double av = fabs((double) vv);
-                    if (msk[r] && av > acc_m) acc_m = av;
+                    const T av = fabs(vv);  // the maximum is exact in the element type
+                    if (msk[r] && av > acc_mt) acc_mt = av;
                     T ep = vv;
                     if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
                     ep_out[(long long) ze * g.zs + (long long) y * g.ys + x] = ep;
@@ -292,16 +369,18 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
         }
         kbase += n_it;
 
-        const double2 rr = block_reduce(acc_s, acc_m, red);
+        const double2 rr = block_reduce_n<NTH, TXW>(acc_s, (double) acc_mt, red);
         if (tid == 0) V.part_t[lt] = rr;
-        if (publish_partial(&st->ticket_t, V.ntiles, &s_flag)) {
+        if (publish_partial_n<TXW>(&st->ticket_t, V.ntiles, &s_flag)) {
+            // Each thread folds a fixed subset of the tile partials, so the
+            // total does not depend on timing.
             double ssum = 0.0, smax = 0.0;
-            for (int i = tid; i < V.ntiles; i += NT) {
+            for (int i = tid; i < V.ntiles; i += NTH) {
                 const double2 pp = __ldcg(&V.part_t[i]);
                 ssum += pp.x;
                 smax = fmax(smax, pp.y);
             }
-            const double2 tot = block_reduce(ssum, smax, red);
+            const double2 tot = block_reduce_n<NTH, TXW>(ssum, smax, red);
             if (tid == 0) {
                 st->ticket_t = 0;
                 control_after_trial(st, tot.x, tot.y);
@@ -313,17 +392,19 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_trial_tma(const 
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
+template <typename T, int TXW, int TYT>
+__global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 ? 2 : 1) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
                                                      const int *__restrict__ tile_vol, int total_tiles,
-                                                     unsigned char *__restrict__ work_flag) {
-    using L = GradTmaLayout<T>;
+                                                     unsigned char *__restrict__ work_flag, TileQueue *queue) {
+    using L = GradTmaLayout<T, TXW>;
+    constexpr int NTH = TXW * TYT, RYT = TT_Y / TYT;
+    constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
     constexpr int PXP = L::PXP, PYP = L::PYP;
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char *smem = align_smem_128(smem_dyn);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     T *pxy = reinterpret_cast<T *>(smem + L::P_OFF);
-    __shared__ double red[2 * (NT / 32)];
+    __shared__ double red[2 * (NTH / 32)];
     __shared__ int s_flag, s_fault;
     // P terms of the x (t = 0..2) and y (t = 3..5) directions, cell (ly, lx)
     // of the tile plus a halo of one.
@@ -331,7 +412,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
         return pxy[((slot * 6 + t) * PYP + ly) * PXP + lx];
     };
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TXW + tx;
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -340,7 +421,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
     __syncthreads();
     uint32_t kbase = 0;
 
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    __shared__ int s_tile;
+    for (int tile = take_tile<TXW>(queue, total_tiles, &s_tile); tile >= 0;
+         tile = take_tile<TXW>(queue, total_tiles, &s_tile)) {
         const VolumeDesc<T> &V = vols[tile_vol[tile]];
         SolverState *st = V.st;
         if (ldcg_int(&st->done) || !ldcg_int(&st->need_gradient)) continue;
@@ -348,7 +431,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
         const int old_b = ldcg_int(&st->old_buf);
         const int lt = tile - V.tile_begin;
         const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
-        const int x0 = txi * BX, y0 = tyi * TT_Y, z0 = tzi * V.bz;
+        const int x0 = txi * TXW, y0 = tyi * TT_Y, z0 = tzi * V.bz;
         const int z1 = min(z0 + V.bz, g.nz);
         const int n_it = z1 - z0 + 4;  // u planes z0-2 .. z1+1
         const CUtensorMap *tm_u = V.tm_field[old_b];
@@ -379,9 +462,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
         };
 
         const int x = x0 + tx;
-        T pz_m2[RY][3], pz_m1[RY][3];
+        T pz_m2[RYT][3], pz_m1[RYT][3];
 #pragma unroll
-        for (int r = 0; r < RY; ++r)
+        for (int r = 0; r < RYT; ++r)
 #pragma unroll
             for (int i = 0; i < 3; ++i) pz_m2[r][i] = pz_m1[r][i] = T(0);
         double acc = 0.0;
@@ -395,9 +478,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
             if (!ok) s_fault = 1;
             const int q = z0 - 2 + it;
             const int p = q - 1;  // plane of P computed now (needs u(q-2..q), e'(q-1))
-            T pz_new[RY][3];
+            T pz_new[RYT][3];
 #pragma unroll
-            for (int r = 0; r < RY; ++r)
+            for (int r = 0; r < RYT; ++r)
 #pragma unroll
                 for (int i = 0; i < 3; ++i) pz_new[r][i] = T(0);
             if (it >= 2 && ok) {
@@ -421,31 +504,31 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
                     return m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
                 };
 #pragma unroll
-                for (int r = 0; r < RY; ++r) {  // own cells: all nine terms (P_z in registers)
-                    const int lx = tx + TMA_HX, ly = ty + r * BY + TMA_HY;
+                for (int r = 0; r < RYT; ++r) {  // own cells: all nine terms (P_z in registers)
+                    const int lx = tx + TMA_HX, ly = ty + r * TYT + TMA_HY;
                     T m[3][3];
                     mat(lx, ly, m);
                     const T ep = e0[ly * TMA_PX + lx];
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        PT(ps, i, ty + r * BY + 1, tx + 1) = ep * minor(m, i, 0);
-                        PT(ps, 3 + i, ty + r * BY + 1, tx + 1) = ep * minor(m, i, 1);
+                        PT(ps, i, ty + r * TYT + 1, tx + 1) = ep * minor(m, i, 0);
+                        PT(ps, 3 + i, ty + r * TYT + 1, tx + 1) = ep * minor(m, i, 1);
                         pz_new[r][i] = ep * minor(m, i, 2);
                     }
                 }
                 // halo cells: P_x on the two side columns, P_y on the two end rows
                 if (tid < 2 * TT_Y) {
                     const int side = tid / TT_Y, row = tid % TT_Y;
-                    const int lx1 = side ? BX + 1 : 0;
+                    const int lx1 = side ? TXW + 1 : 0;
                     const int lx = lx1 - 1 + TMA_HX, ly = row + TMA_HY;
                     T m[3][3];
                     mat(lx, ly, m);
                     const T ep = e0[ly * TMA_PX + lx];
 #pragma unroll
                     for (int i = 0; i < 3; ++i) PT(ps, i, row + 1, lx1) = ep * minor(m, i, 0);
-                } else if (tid < 2 * TT_Y + 2 * BX) {
+                } else if (tid < 2 * TT_Y + 2 * TXW) {
                     const int t2 = tid - 2 * TT_Y;
-                    const int side = t2 / BX, col = t2 % BX;
+                    const int side = t2 / TXW, col = t2 % TXW;
                     const int ly1 = side ? TT_Y + 1 : 0;
                     const int lx = col + TMA_HX, ly = ly1 - 1 + TMA_HY;
                     T m[3][3];
@@ -466,10 +549,10 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
             if (it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x >= 1 && x < g.nx - 1) {
                 const int ps = ring_slot(z, L::NP);
 #pragma unroll
-                for (int r = 0; r < RY; ++r) {
-                    const int y = y0 + ty + r * BY;
+                for (int r = 0; r < RYT; ++r) {
+                    const int y = y0 + ty + r * TYT;
                     if (y < 1 || y >= g.ny - 1) continue;
-                    const int lx = tx + 1, ly = ty + r * BY + 1;
+                    const int lx = tx + 1, ly = ty + r * TYT + 1;
                     T t[3][3];
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
@@ -488,7 +571,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
                 }
             }
 #pragma unroll
-            for (int r = 0; r < RY; ++r)
+            for (int r = 0; r < RYT; ++r)
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
                     pz_m2[r][i] = pz_m1[r][i];
@@ -502,12 +585,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
         }
         kbase += n_it;
 
-        const double2 rr = block_reduce(acc, 0.0, red);
+        const double2 rr = block_reduce_n<NTH, TXW>(acc, 0.0, red);
         if (tid == 0) V.part_g[lt] = rr.x;
-        if (publish_partial(&st->ticket_g, V.ntiles, &s_flag)) {
+        if (publish_partial_n<TXW>(&st->ticket_g, V.ntiles, &s_flag)) {
             double ssum = 0.0;
-            for (int i = tid; i < V.ntiles; i += NT) ssum += __ldcg(&V.part_g[i]);
-            const double2 tot = block_reduce(ssum, 0.0, red);
+            for (int i = tid; i < V.ntiles; i += NTH) ssum += __ldcg(&V.part_g[i]);
+            const double2 tot = block_reduce_n<NTH, TXW>(ssum, 0.0, red);
             if (tid == 0) {
                 st->ticket_g = 0;
                 st->gn2 = tot.x;
@@ -521,59 +604,95 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 2 : 1) k_gradient_tma(con
     }
 }
 
-template <typename T>
-cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                             cudaStream_t s, unsigned char *work_flag) {
-    constexpr int smem = TrialTmaLayout<T>::BYTES + 128;
+template <typename T, int TXW, int TYT>
+cudaError_t launch_trial_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                               cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
+    constexpr int smem = TrialTmaLayout<T, TXW>::BYTES + 128;
     static const cudaError_t attr =
-        cudaFuncSetAttribute(k_trial_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
-    k_trial_tma<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles, work_flag);
+    k_trial_tma<T, TXW, TYT><<<grid, dim3(TXW, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
     count_launch();
     return cudaGetLastError();
+}
+
+template <typename T, int TXW, int TYT>
+cudaError_t launch_gradient_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                                  cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
+    constexpr int smem = GradTmaLayout<T, TXW>::BYTES + 128;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr != cudaSuccess) return attr;
+    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, int TXW, int TYT>
+int trial_blocks_v() {
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TrialTmaLayout<T, TXW>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T, TXW, TYT>, TXW * TYT,
+                                                      TrialTmaLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return n;
+}
+template <typename T, int TXW, int TYT>
+int gradient_blocks_v() {
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GradTmaLayout<T, TXW>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T, TXW, TYT>, TXW * TYT,
+                                                      GradTmaLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return n;
+}
+
+// Tile shapes (tile_x x TT_Y voxels; threads_y rows of threads):
+//   tile_x 64, threads_y 8   FP32 default: long TMA rows, 512 threads
+//   tile_x 32, threads_y 8   FP64 default (shared memory), 256 threads
+//   tile_x 32, threads_y 16  512 threads of one row each
+template <typename T>
+cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
+    if (tile_x == 64 && sizeof(T) == 4)
+        return launch_trial_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    if (threads_y == 16) return launch_trial_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    return launch_trial_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
 }
 
 template <typename T>
 cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                                cudaStream_t s, unsigned char *work_flag) {
-    constexpr int smem = GradTmaLayout<T>::BYTES + 128;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_gradient_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (attr != cudaSuccess) return attr;
-    k_gradient_tma<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles, work_flag);
-    count_launch();
-    return cudaGetLastError();
+                                cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
+    if (tile_x == 64 && sizeof(T) == 4)
+        return launch_gradient_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    if (threads_y == 16)
+        return launch_gradient_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    return launch_gradient_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
 }
 
 template <typename T>
-int trial_tma_blocks_per_sm() {
-    static const int n = [] {
-        int v = 0;
-        cudaFuncSetAttribute(k_trial_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TrialTmaLayout<T>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T>, NT, TrialTmaLayout<T>::BYTES + 128);
-        return v;
-    }();
-    return n;
+int trial_tma_blocks_per_sm(int tile_x, int threads_y) {
+    if (tile_x == 64 && sizeof(T) == 4) return trial_blocks_v<T, 64, 8>();
+    return threads_y == 16 ? trial_blocks_v<T, 32, 16>() : trial_blocks_v<T, 32, 8>();
 }
 template <typename T>
-int gradient_tma_blocks_per_sm() {
-    static const int n = [] {
-        int v = 0;
-        cudaFuncSetAttribute(k_gradient_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             GradTmaLayout<T>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T>, NT, GradTmaLayout<T>::BYTES + 128);
-        return v;
-    }();
-    return n;
+int gradient_tma_blocks_per_sm(int tile_x, int threads_y) {
+    if (tile_x == 64 && sizeof(T) == 4) return gradient_blocks_v<T, 64, 8>();
+    return threads_y == 16 ? gradient_blocks_v<T, 32, 16>() : gradient_blocks_v<T, 32, 8>();
 }
 
 #define DTB_INSTANTIATE_TMA(T)                                                                              \
     template cudaError_t launch_trial_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
-                                             unsigned char *);                                              \
+                                             unsigned char *, int, int, TileQueue *);                       \
     template cudaError_t launch_gradient_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t, \
-                                                unsigned char *);                                           \
-    template int trial_tma_blocks_per_sm<T>();                                                              \
-    template int gradient_tma_blocks_per_sm<T>();
+                                                unsigned char *, int, int, TileQueue *);                    \
+    template int trial_tma_blocks_per_sm<T>(int, int);                                                      \
+    template int gradient_tma_blocks_per_sm<T>(int, int);
 
 }  // namespace dtb
