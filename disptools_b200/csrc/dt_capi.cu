@@ -385,17 +385,18 @@ int ensure_profiling(Engine *e, size_t nk) {
     return DTB_OK;
 }
 
-// Tile and block shape of the TMA kernels.  FP32 tiles are 64 voxels wide
-// (long contiguous TMA rows); FP64 tiles 32 (their shared-memory footprint
-// doubles).  Blocks have 8 thread rows (two tile rows each) unless
-// DISPTOOLS_B200_THREADS_Y=16 (32-wide tiles only).
+// Tile and block shape of the TMA kernels.  Tiles are 32 x 16 voxels, blocks
+// 32 x 8 threads (two tile rows each): measured fastest at 256^3 on B200
+// (two resident blocks per SM).  DISPTOOLS_B200_TILE_X=64 selects 64-wide
+// FP32 tiles (longer TMA rows, one 512-thread block per SM) and
+// DISPTOOLS_B200_THREADS_Y=16 one tile row per thread (32-wide tiles only).
 int pick_tile_x(size_t tsize) {
     const char *e = std::getenv("DISPTOOLS_B200_TILE_X");
     if (e && tsize == 4) {
         const int v = std::atoi(e);
         if (v == 32 || v == 64) return v;
     }
-    return tsize == 4 ? 64 : 32;
+    return 32;
 }
 int pick_threads_y(int tile_x) {
     const char *e = std::getenv("DISPTOOLS_B200_THREADS_Y");
