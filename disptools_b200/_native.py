@@ -116,6 +116,8 @@ lib.dtb_generate_displacement_batched_device.argtypes = [_I, _I, _I, C.POINTER(V
 lib.dtb_generate_displacement_batched_device.restype = _I
 lib.dtb_jacobian_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P]
 lib.dtb_jacobian_device.restype = _I
+lib.dtb_jacobian_device_noalloc.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P]
+lib.dtb_jacobian_device_noalloc.restype = _I
 lib.dtb_jacobian_adjoint_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
 lib.dtb_jacobian_adjoint_device.restype = _I
 lib.dtb_kernel_launch_count.restype = C.c_ulonglong
@@ -138,7 +140,7 @@ EXPORTED = [
     "dtb_generate_displacement", "dtb_generate_displacement_batched",
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
-    "dtb_get_profile",
+    "dtb_get_profile", "dtb_jacobian_device_noalloc",
 ]
 
 

@@ -32,6 +32,7 @@ UNITS = [
     ("dt_kernels_f32.cu", []),
     ("dt_kernels_f64.cu", ["-fmad=false"]),
     ("dt_capi.cu", []),
+    ("dt_noalloc.cu", []),
 ]
 HEADERS = ["dt_internal.h", "dt_kernels.cuh"]
 

@@ -229,6 +229,20 @@ int dtb_jacobian_adjoint_device(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, const void *grad_J, void *grad_field, void *stream);
 
+/* Jacobian determinant of a device-resident field, like dtb_jacobian_device,
+ * but without allocating any memory.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory when they need the map
+ * (during stream capture, or on hosts with a fixed memory budget).  Its
+ * launch descriptor and tile table live in a 65 KiB array in device memory
+ * that belongs to the library and is held by every GPU that loads it; the
+ * first call on a device looks up that array's address, so make it before
+ * any stream capture.  Volumes up to 16384 tiles of 32 x 8 x 32 voxels
+ * (512^3) are accepted; larger ones return DTB_ERR_ARGUMENT.  All calls on
+ * a device share the array: calls whose work overlaps on the GPU race. */
+int dtb_jacobian_device_noalloc(
+    int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+    const void *field, void *J, void *stream);
+
 /* Number of kernels this library has launched in the process (a counter
  * kept by the host code, for benchmarks that report launch counts; each
  * replay of a captured step graph counts the kernels it contains). */
