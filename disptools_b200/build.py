@@ -34,7 +34,7 @@ UNITS = [
     ("dt_capi.cu", []),
     ("dt_noalloc.cu", []),
 ]
-HEADERS = ["dt_internal.h", "dt_kernels.cuh"]
+HEADERS = ["dt_internal.h", "dt_kernels.cuh", "dt_kernels_tma.cuh", "dt_tma.cuh"]
 
 
 def _nvcc() -> str:

@@ -385,11 +385,14 @@ int ensure_profiling(Engine *e, size_t nk) {
     return DTB_OK;
 }
 
-// Tile and block shape of the TMA kernels.  Tiles are 32 x 16 voxels, blocks
-// 32 x 8 threads (two tile rows each): measured fastest at 256^3 on B200
-// (two resident blocks per SM).  DISPTOOLS_B200_TILE_X=64 selects 64-wide
-// FP32 tiles (longer TMA rows, one 512-thread block per SM) and
-// DISPTOOLS_B200_THREADS_Y=16 one tile row per thread (32-wide tiles only).
+// Tile and block shape of the TMA kernels.  Tiles are 32 x 16 voxels: the
+// gradient kernel runs blocks of 32 x 8 threads (two tile rows each), the
+// trial kernel 16 x 16 threads (two columns of one row each); both measured
+// fastest at 256^3 on B200 (two resident blocks per SM).
+// DISPTOOLS_B200_TILE_X=64 selects 64-wide FP32 tiles (longer TMA rows, one
+// 512-thread block per SM), DISPTOOLS_B200_THREADS_Y=16 one tile row per
+// gradient thread and DISPTOOLS_B200_TRIAL_THREADS_Y=8 two tile rows per
+// trial thread (32-wide tiles only).
 int pick_tile_x(size_t tsize) {
     const char *e = std::getenv("DISPTOOLS_B200_TILE_X");
     if (e && tsize == 4) {
@@ -406,6 +409,14 @@ int pick_threads_y(int tile_x) {
     }
     return 8;
 }
+int pick_trial_threads_y(int tile_x) {
+    const char *e = std::getenv("DISPTOOLS_B200_TRIAL_THREADS_Y");
+    if (e && tile_x == 32) {
+        const int v = std::atoi(e);
+        if (v == 8 || v == 16) return v;
+    }
+    return 16;
+}
 
 template <typename T>
 int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
@@ -414,6 +425,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     const int count = (int) vols.size();
     const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? pick_tile_x(sizeof(T)) : BX;
     const int threads_y = pick_threads_y(tile_x);
+    const int trial_ty = pick_trial_threads_y(tile_x);
     const bool gradient = algorithm == DTB_ALGORITHM_GRADIENT;
     // ---- workspace layout: every buffer of the solve is the library's own,
     // in the pitched layout.
@@ -557,11 +569,11 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
 
 
     // Persistent grids: as many blocks as fit on the device at once.
-    const int grid_t = gradient ? std::min(total_tiles, std::max(1, trial_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms())
+    const int grid_t = gradient ? std::min(total_tiles, std::max(1, trial_tma_blocks_per_sm<T>(tile_x, trial_ty)) * num_sms())
                                 : total_tiles;
     const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms());
     auto launch_t = [&](unsigned char *flag) -> cudaError_t {
-        if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, threads_y,
+        if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, trial_ty,
                                                     d_queues);
         return launch_trial<T>(MODE_GREEDY, d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
     };
@@ -600,7 +612,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     key.grid_t = grid_t;
     key.grid_g = grid_g;
     key.K = K;
-    key.threads_y = threads_y * 1000 + tile_x;
+    key.threads_y = (trial_ty * 100 + threads_y) * 1000 + tile_x;
     key.flags = d_flags;
     if (!(e->exec && e->key == key)) {
         if (e->exec) cudaGraphExecDestroy(e->exec);

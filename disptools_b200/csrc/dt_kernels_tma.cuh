@@ -1,7 +1,6 @@
 // TMA-pipelined kernels of the gradient method (sm_100a).
 //
-// Both kernels march a TXW x TT_Y tile (TT_Y / TYT rows per thread) through
-// its z range.  One elected thread streams one box per input per plane into a ring
+// Both kernels march a TXW x TT_Y tile through its z range.  One elected thread streams one box per input per plane into a ring
 // of shared-memory stages with cp.async.bulk.tensor, completion tracked by an
 // mbarrier per stage; the other threads issue no global loads for the stencil
 // inputs.  Boxes start 4 voxels left of the tile so the innermost TMA
@@ -72,10 +71,11 @@ struct GradTmaLayout {
 };
 
 // Takes the next tile of a persistent launch (-1 when none is left; the
-// block is then counted out and the last one resets the queue).
-template <int TXW>
+// block is then counted out and the last one resets the queue).  BDX is the
+// block's x dimension.
+template <int BDX>
 __device__ __forceinline__ int take_tile(TileQueue *q, int total, int *s_tile) {
-    const int tid = threadIdx.y * TXW + threadIdx.x;
+    const int tid = threadIdx.y * BDX + threadIdx.x;
     __syncthreads();  // everyone has read the previous s_tile
     if (tid == 0) {
         int t = (int) atomicAdd(&q->next, 1u);
@@ -115,16 +115,46 @@ __device__ __forceinline__ void tma_fault(SolverState *st, uint64_t *bars, uint3
     }
 }
 
-// TYT threads along y (each thread owns TT_Y / TYT rows of the tile).  Two
-// resident blocks per SM for FP32 (shared memory allows no more), one for
-// FP64; the bound caps the registers accordingly.
+// Two voxels adjacent in x, loaded or stored as one 8-byte (float) or
+// 16-byte (double) access.
+template <typename T>
+struct PairOf;
+template <>
+struct PairOf<float> {
+    using type = float2;
+};
+template <>
+struct PairOf<double> {
+    using type = double2;
+};
+template <typename T>
+__device__ __forceinline__ typename PairOf<T>::type ld_pair(const T *p) {
+    return *reinterpret_cast<const typename PairOf<T>::type *>(p);
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T *p, T a, T b) {
+    typename PairOf<T>::type v;
+    v.x = a;
+    v.y = b;
+    *reinterpret_cast<typename PairOf<T>::type *>(p) = v;
+}
+
+// Block of TXW / 2 x TYT threads; each thread owns two adjacent columns
+// (x, x + 1) of TT_Y / TYT rows of the tile, so every shared-memory read of
+// the stencil and every global store covers two voxels.  A warp spans the
+// whole tile width (TXW / 2 divides 32), which makes the evaluator choice
+// below uniform across a warp except on rows near the y ends.  Two resident
+// blocks per SM for FP32 (shared memory allows no more), one for FP64; the
+// bound caps the registers accordingly.
 template <typename T, int TXW, int TYT>
-__global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 ? 2 : 1) k_trial_tma(const VolumeDesc<T> *__restrict__ vols,
-                                                  const int *__restrict__ tile_vol, int total_tiles,
-                                                  unsigned char *__restrict__ work_flag, TileQueue *queue) {
+__global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof(T) == 4) ? 2 : 1)
+    k_trial_tma(const VolumeDesc<T> *__restrict__ vols, const int *__restrict__ tile_vol, int total_tiles,
+                unsigned char *__restrict__ work_flag, TileQueue *queue) {
     using L = TrialTmaLayout<T, TXW>;
-    constexpr int NTH = TXW * TYT, RYT = TT_Y / TYT;
+    constexpr int TPX = TXW / 2, NTH = TPX * TYT, RYT = TT_Y / TYT;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
+    static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
+    static_assert((L::R & (L::R - 1)) == 0, "ring size is a power of two");
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char *smem = align_smem_128(smem_dyn);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
@@ -132,7 +162,7 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
     __shared__ double red[2 * (NTH / 32)];
     __shared__ int s_flag, s_fault;
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TXW + tx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -142,8 +172,8 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
     uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
 
     __shared__ int s_tile;
-    for (int tile = take_tile<TXW>(queue, total_tiles, &s_tile); tile >= 0;
-         tile = take_tile<TXW>(queue, total_tiles, &s_tile)) {
+    for (int tile = take_tile<TPX>(queue, total_tiles, &s_tile); tile >= 0;
+         tile = take_tile<TPX>(queue, total_tiles, &s_tile)) {
         const VolumeDesc<T> &V = vols[tile_vol[tile]];
         SolverState *st = V.st;
         if (ldcg_int(&st->done)) continue;
@@ -193,20 +223,25 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
             for (int j = 0; j < min(L::S, n_it); ++j) issue(j);
         }
 
-        const int x = x0 + tx;
+        const int x = x0 + 2 * tx;     // this thread's columns: x, x + 1
+        const int lx = 2 * tx + TMA_HX;  // their box column
+        const bool pair_in = x + 1 < g.nx;
         // Own columns: candidate values of planes q-4 .. q (z differences).
-        T zq[RYT][3][5];
+        T zq[RYT][2][3][5];
 #pragma unroll
         for (int r = 0; r < RYT; ++r)
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+            for (int v = 0; v < 2; ++v)
 #pragma unroll
-                for (int k = 0; k < 5; ++k) zq[r][c][k] = T(0);
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
         double acc_s = 0.0;
         T acc_mt = T(0);
         bool failed = false;
         int fail_it = 0;
-        for (int it = 0; it < n_it; ++it) {
+        long long qoff = (long long) (z0 - 2) * g.zs;  // offset of plane q
+        for (int it = 0; it < n_it; ++it, qoff += g.zs) {
             const uint32_t k = kbase + it;
             const int s = k % L::S;
             const uint32_t par = (k / L::S) & 1u;
@@ -216,7 +251,7 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
             if (!ok) s_fault = 1;
             const unsigned char *sb = smem + s * L::STAGE_BYTES;
             const int q = z0 - 2 + it, ze = q - 2;
-            T *slot = ring + (size_t) ring_slot(q, L::R) * 3 * TMA_PLANE;
+            T *slot = ring + (size_t) (q & (L::R - 1)) * 3 * TMA_PLANE;
             // Candidate plane q (tile + halo): u - eta g, vectorised.
             if (ok) {
                 constexpr int VEC = 16 / (int) sizeof(T);
@@ -237,15 +272,21 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
                 }
             }
             const bool eval = ze >= z0 && ze < z1;
-            T jt[RYT];
-            bool msk[RYT];
+            T jt[RYT][2];
+            bool msk[RYT][2];
 #pragma unroll
             for (int r = 0; r < RYT; ++r) {
-                jt[r] = T(0);
-                msk[r] = false;
+                jt[r][0] = jt[r][1] = T(0);
+                msk[r][0] = msk[r][1] = false;
                 if (eval && ok) {
-                    jt[r] = reinterpret_cast<const T *>(sb + 2 * L::U_BYTES)[tid + r * NTH];
-                    msk[r] = (sb + 2 * L::U_BYTES + L::JT_BYTES)[tid + r * NTH] != 0;
+                    const int o = (ty + r * TYT) * TXW + 2 * tx;
+                    const auto j2 = ld_pair(reinterpret_cast<const T *>(sb + 2 * L::U_BYTES) + o);
+                    const unsigned short m2 =
+                        *reinterpret_cast<const unsigned short *>(sb + 2 * L::U_BYTES + L::JT_BYTES + o);
+                    jt[r][0] = j2.x;
+                    jt[r][1] = j2.y;
+                    msk[r][0] = (m2 & 0xffu) != 0;
+                    msk[r][1] = (m2 >> 8) != 0;
                 }
             }
             __syncthreads();
@@ -261,19 +302,29 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
                 const int ly = ty + r * TYT + TMA_HY;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
+                    const auto nv = ld_pair(slot + c * TMA_PLANE + ly * TMA_PX + lx);
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) zq[r][c][kk] = zq[r][c][kk + 1];
-                    zq[r][c][4] = slot[c * TMA_PLANE + ly * TMA_PX + tx + TMA_HX];
+                    for (int kk = 0; kk < 4; ++kk) {
+                        zq[r][0][c][kk] = zq[r][0][c][kk + 1];
+                        zq[r][1][c][kk] = zq[r][1][c][kk + 1];
+                    }
+                    zq[r][0][c][4] = nv.x;
+                    zq[r][1][c][4] = nv.y;
                 }
                 const int y = y0 + ty + r * TYT;
                 if (trial && x < g.nx && y < g.ny && q >= z0 && q < z1) {
-                    const long long so = (long long) q * g.zs + (long long) y * g.ys + x;
+                    T *o = dst + qoff + (long long) y * g.ys + x;
+                    if (pair_in) {
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) dst[c * g.cs + so] = zq[r][c][4];
+                        for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, zq[r][0][c][4], zq[r][1][c][4]);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) o[c * g.cs] = zq[r][0][c][4];
+                    }
                 }
             }
             if (eval) {
-                const T *jp = ring + (size_t) ring_slot(ze, L::R) * 3 * TMA_PLANE;
+                const T *jp = ring + (size_t) (ze & (L::R - 1)) * 3 * TMA_PLANE;
                 // Fourth-order weights with the spacing folded in (FP32); the
                 // FP64 path keeps the reference's operation order.
                 const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
@@ -283,82 +334,113 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
                     if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
                     return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
                 };
-                // Three evaluators, chosen per warp (a warp is 32 voxels of one
-                // row): rows and planes inside [2, n-3] away from the x ends use
-                // the fourth-order stencil only; interior rows that reach an x
-                // end select the scheme per lane without branching; rows or
+                // Three evaluators: rows and planes inside [2, n-3] of a tile
+                // whose columns all lie inside [2, nx-3] use the fourth-order
+                // stencil only; interior rows of a tile that reaches an x end
+                // select the scheme per voxel without branching; rows or
                 // planes on the two outer layers take the general path.
                 const bool plane_in = ze >= 2 && ze <= g.nz - 3;
-                const int xw0 = x0 + (tx & ~31);
-                const bool warp_x_in = xw0 >= 2 && xw0 + 31 <= g.nx - 3;
+                const bool tile_x_in = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3;
 #pragma unroll
                 for (int r = 0; r < RYT; ++r) {
                     const int y = y0 + ty + r * TYT;
                     const bool row_in = plane_in && y >= 2 && y <= g.ny - 3;
-                    const int lx = tx + TMA_HX, ly = ty + r * TYT + TMA_HY;
-                    T a[3][3];
-                    if (row_in && warp_x_in) {
+                    const int ly = ty + r * TYT + TMA_HY;
+                    if (x >= g.nx || y >= g.ny) continue;
+                    T epv[2];
+                    // Error terms of voxel v from its Jacobian matrix minus I.
+                    auto finish = [&](int v, const T (&a)[3][3]) {
+                        const T J = det_i_plus<T>(a);
+                        const T vv = voxel_error<T>(J, jt[r][v], msk[r][v], tol);
+                        acc_s += (double) vv * (double) vv;
+                        const T av = fabs(vv);  // the maximum is exact in the element type
+                        if (msk[r][v] && av > acc_mt) acc_mt = av;
+                        T ep = vv;
+                        if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
+                        epv[v] = ep;
+                    };
+                    if (row_in && tile_x_in) {
+                        T a0[3][3], a1[3][3];
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
                             const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
-                            a[c][0] = c4(p[1], p[-1], p[2], p[-2], 0);
-                            a[c][1] = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
-                            a[c][2] = c4(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0], 2);
+                            const auto xm = ld_pair(p - 2), xc = ld_pair(p), xp = ld_pair(p + 2);
+                            a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
+                            a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
+                            const auto ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
+                            const auto ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
+                            a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
+                            a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+                            const T *z0q = zq[r][0][c], *z1q = zq[r][1][c];
+                            a0[c][2] = c4(z0q[3], z0q[1], z0q[4], z0q[0], 2);
+                            a1[c][2] = c4(z1q[3], z1q[1], z1q[4], z1q[0], 2);
                         }
+                        finish(0, a0);
+                        finish(1, a1);
                     } else if (row_in) {
-                        if (x >= g.nx) continue;
                         // Interior row: the scheme depends on x only
                         // (src/jacobian.c:113-241): outer column -> one-sided
                         // in x and second-order central in y, z; penultimate
                         // column -> second-order central; else fourth order.
-                        const bool xo_lo = x == 0, xo_hi = x == g.nx - 1;
-                        const bool second = xo_lo || xo_hi || x == 1 || x == g.nx - 2;
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
-                            const T fx = xo_lo ? fd_fwd<T>(p[0], p[1], p[2], ih[0])
-                                               : (xo_hi ? fd_bwd<T>(p[0], p[-1], p[-2], ih[0])
-                                                        : fd_c2<T>(p[1], p[-1], ih[0]));
-                            const T cx4 = c4(p[1], p[-1], p[2], p[-2], 0);
-                            a[c][0] = second ? fx : cx4;
-                            const T cy4 = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
-                            const T cy2 = fd_c2<T>(p[TMA_PX], p[-TMA_PX], ih[1]);
-                            a[c][1] = second ? cy2 : cy4;
-                            const T cz4 = c4(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0], 2);
-                            const T cz2 = fd_c2<T>(zq[r][c][3], zq[r][c][1], ih[2]);
-                            a[c][2] = second ? cz2 : cz4;
+                        for (int v = 0; v < 2; ++v) {
+                            const int xv = x + v;
+                            if (xv >= g.nx) continue;
+                            const bool xo_lo = xv == 0, xo_hi = xv == g.nx - 1;
+                            const bool second = xo_lo || xo_hi || xv == 1 || xv == g.nx - 2;
+                            T a[3][3];
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx + v;
+                                const T fx = xo_lo ? fd_fwd<T>(p[0], p[1], p[2], ih[0])
+                                                   : (xo_hi ? fd_bwd<T>(p[0], p[-1], p[-2], ih[0])
+                                                            : fd_c2<T>(p[1], p[-1], ih[0]));
+                                const T cx4 = c4(p[1], p[-1], p[2], p[-2], 0);
+                                a[c][0] = second ? fx : cx4;
+                                const T cy4 = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
+                                const T cy2 = fd_c2<T>(p[TMA_PX], p[-TMA_PX], ih[1]);
+                                a[c][1] = second ? cy2 : cy4;
+                                const T *zv = zq[r][v][c];
+                                const T cz4 = c4(zv[3], zv[1], zv[4], zv[0], 2);
+                                const T cz2 = fd_c2<T>(zv[3], zv[1], ih[2]);
+                                a[c][2] = second ? cz2 : cz4;
+                            }
+                            finish(v, a);
                         }
                     } else {
-                        if (x >= g.nx || y >= g.ny) continue;
-                        int kk[3];
-                        schemes_at(x, y, ze, g, kk);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
-                            const T vx[5] = {p[-2], p[-1], p[0], p[1], p[2]};
-                            const T vy[5] = {p[-2 * TMA_PX], p[-TMA_PX], p[0], p[TMA_PX], p[2 * TMA_PX]};
+                        for (int v = 0; v < 2; ++v) {
+                            const int xv = x + v;
+                            if (xv >= g.nx) continue;
+                            int kk[3];
+                            schemes_at(xv, y, ze, g, kk);
+                            T a[3][3];
 #pragma unroll
-                            for (int ax = 0; ax < 3; ++ax) {
-                                const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[r][c]);
-                                T d;
-                                switch (kk[ax]) {
-                                case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
-                                case S_BWD: d = fd_bwd<T>(w[2], w[1], w[0], ih[ax]); break;
-                                case S_C2: d = fd_c2<T>(w[3], w[1], ih[ax]); break;
-                                default: d = c4(w[3], w[1], w[4], w[0], ax); break;
+                            for (int c = 0; c < 3; ++c) {
+                                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx + v;
+                                const T vx[5] = {p[-2], p[-1], p[0], p[1], p[2]};
+                                const T vy[5] = {p[-2 * TMA_PX], p[-TMA_PX], p[0], p[TMA_PX], p[2 * TMA_PX]};
+#pragma unroll
+                                for (int ax = 0; ax < 3; ++ax) {
+                                    const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[r][v][c]);
+                                    T d;
+                                    switch (kk[ax]) {
+                                    case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
+                                    case S_BWD: d = fd_bwd<T>(w[2], w[1], w[0], ih[ax]); break;
+                                    case S_C2: d = fd_c2<T>(w[3], w[1], ih[ax]); break;
+                                    default: d = c4(w[3], w[1], w[4], w[0], ax); break;
+                                    }
+                                    a[c][ax] = d;
                                 }
-                                a[c][ax] = d;
                             }
+                            finish(v, a);
                         }
                     }
-                    const T J = det_i_plus<T>(a);
-                    const T vv = voxel_error<T>(J, jt[r], msk[r], tol);
-                    acc_s += (double) vv * (double) vv;
-                    const T av = fabs(vv);  // the maximum is exact in the element type
-                    if (msk[r] && av > acc_mt) acc_mt = av;
-                    T ep = vv;
-                    if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
-                    ep_out[(long long) ze * g.zs + (long long) y * g.ys + x] = ep;
+                    T *o = ep_out + (qoff - 2 * g.zs) + (long long) y * g.ys + x;
+                    if (pair_in)
+                        st_pair(o, epv[0], epv[1]);
+                    else
+                        o[0] = epv[0];
                 }
             }
         }
@@ -369,9 +451,9 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
         }
         kbase += n_it;
 
-        const double2 rr = block_reduce_n<NTH, TXW>(acc_s, (double) acc_mt, red);
+        const double2 rr = block_reduce_n<NTH, TPX>(acc_s, (double) acc_mt, red);
         if (tid == 0) V.part_t[lt] = rr;
-        if (publish_partial_n<TXW>(&st->ticket_t, V.ntiles, &s_flag)) {
+        if (publish_partial_n<TPX>(&st->ticket_t, V.ntiles, &s_flag)) {
             // Each thread folds a fixed subset of the tile partials, so the
             // total does not depend on timing.
             double ssum = 0.0, smax = 0.0;
@@ -380,7 +462,7 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
                 ssum += pp.x;
                 smax = fmax(smax, pp.y);
             }
-            const double2 tot = block_reduce_n<NTH, TXW>(ssum, smax, red);
+            const double2 tot = block_reduce_n<NTH, TPX>(ssum, smax, red);
             if (tid == 0) {
                 st->ticket_t = 0;
                 control_after_trial(st, tot.x, tot.y);
@@ -611,7 +693,7 @@ cudaError_t launch_trial_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, i
     static const cudaError_t attr =
         cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
-    k_trial_tma<T, TXW, TYT><<<grid, dim3(TXW, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
+    k_trial_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
     count_launch();
     return cudaGetLastError();
 }
@@ -634,7 +716,7 @@ int trial_blocks_v() {
         int v = 0;
         cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TrialTmaLayout<T, TXW>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T, TXW, TYT>, TXW * TYT,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T, TXW, TYT>, TXW / 2 * TYT,
                                                       TrialTmaLayout<T, TXW>::BYTES + 128);
         return v;
     }();
@@ -653,24 +735,29 @@ int gradient_blocks_v() {
     return n;
 }
 
-// Tile shapes (tile_x x TT_Y voxels; threads_y rows of threads):
-//   tile_x 64, threads_y 8   FP32 default: long TMA rows, 512 threads
-//   tile_x 32, threads_y 8   FP64 default (shared memory), 256 threads
+// Tile shapes (tile_x x TT_Y voxels).  Trial kernel: tile_x / 2 x threads_y
+// threads of TT_Y / threads_y rows and two columns each:
+//   tile_x 32, threads_y 16  default, 256 threads (two blocks per SM for FP32)
+//   tile_x 32, threads_y 8   128 threads of two rows (four voxels) each
+//   tile_x 64, threads_y 16  FP32 only, 512 threads, one block per SM
+// Gradient kernel: tile_x x threads_y threads of TT_Y / threads_y rows each:
+//   tile_x 32, threads_y 8   default, 256 threads
 //   tile_x 32, threads_y 16  512 threads of one row each
+//   tile_x 64, threads_y 8   FP32 only, 512 threads
 template <typename T>
 cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                              cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
-    if (tile_x == 64 && sizeof(T) == 4)
-        return launch_trial_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
-    if (threads_y == 16) return launch_trial_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
-    return launch_trial_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    if constexpr (sizeof(T) == 4)
+        if (tile_x == 64) return launch_trial_tma_v<T, 64, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    if (threads_y == 8) return launch_trial_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    return launch_trial_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
 }
 
 template <typename T>
 cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                 cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
-    if (tile_x == 64 && sizeof(T) == 4)
-        return launch_gradient_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    if constexpr (sizeof(T) == 4)
+        if (tile_x == 64) return launch_gradient_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
     if (threads_y == 16)
         return launch_gradient_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
     return launch_gradient_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
@@ -678,12 +765,14 @@ cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, 
 
 template <typename T>
 int trial_tma_blocks_per_sm(int tile_x, int threads_y) {
-    if (tile_x == 64 && sizeof(T) == 4) return trial_blocks_v<T, 64, 8>();
-    return threads_y == 16 ? trial_blocks_v<T, 32, 16>() : trial_blocks_v<T, 32, 8>();
+    if constexpr (sizeof(T) == 4)
+        if (tile_x == 64) return trial_blocks_v<T, 64, 16>();
+    return threads_y == 8 ? trial_blocks_v<T, 32, 8>() : trial_blocks_v<T, 32, 16>();
 }
 template <typename T>
 int gradient_tma_blocks_per_sm(int tile_x, int threads_y) {
-    if (tile_x == 64 && sizeof(T) == 4) return gradient_blocks_v<T, 64, 8>();
+    if constexpr (sizeof(T) == 4)
+        if (tile_x == 64) return gradient_blocks_v<T, 64, 8>();
     return threads_y == 16 ? gradient_blocks_v<T, 32, 16>() : gradient_blocks_v<T, 32, 8>();
 }
 
