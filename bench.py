@@ -47,6 +47,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default="c2", choices=["c2", "c4"],
+                   help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
+                        "axes U{48..192} split over the ranks")
     return p.parse_args()
 
 
@@ -209,9 +212,106 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(out))
 
 
+def run_c4(args, world, rank, local):
+    """Config 4: 64 independent volumes (axes U{48..192}, 1-4 ellipsoids
+    each), FP32 fields.  The volumes are split over the ranks by voxel count
+    (disptools_b200.sharding.assign_volumes) and each rank solves its share
+    in one batched call per step: total work is fixed (strong scaling)."""
+    import numpy as np
+    import torch
+
+    import disptools_b200 as dt
+    from disptools_b200 import torch_ops
+    from disptools_b200.sharding import assign_volumes
+    from disptools_b200.synthetic import batch_sizes, ellipsoid_problem
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    IT = args.it_max
+    sizes = batch_sizes(64, 48, 192, seed=0)
+    total_vox = int(sum(np.prod(s) for s in sizes))
+    mine = assign_volumes([int(np.prod(s)) for s in sizes], world)[rank]
+    host = [ellipsoid_problem(sizes[i], seed=i) for i in mine]
+    vols = [(torch.from_numpy(J).float().to(dev), torch.from_numpy(m).to(dev),
+             torch.zeros((3,) + J.shape, dtype=torch.float32, device=dev)) for J, m in host]
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        for v in vols:
+            v[2].zero_()
+        return torch_ops.solve_batched(vols, it_max=IT) if vols else []
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = dt.kernel_launch_count()
+    vi = 0.0
+    trials = iters = 0
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            for (J, _, _), st in zip(vols, step()):
+                k = iterations_done(st)
+                vi += float(J.numel()) * k
+                iters += k
+                trials += st["trials"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    launches = dt.kernel_launch_count() - launches0
+    value = sum_over_ranks(world, vi) / (ms / 1000.0)
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        hv = [(pin(J), pin(m), pin(np.zeros((3,) + J.shape))) for J, m in host]
+        dt.solve_batched(hv, it_max=IT)
+        barrier(world)
+        te = 0.0
+        ve = 0.0
+        ke = max(1, min(args.steps, 2))
+        for _ in range(ke):
+            t0 = time.perf_counter()
+            res = dt.solve_batched(hv, it_max=IT) if hv else []
+            te += time.perf_counter() - t0
+            ve += sum(float(J.size) * iterations_done(st) for (J, _, _), (_, st) in zip(hv, res))
+        te = max_over_ranks(world, te)
+        nb = sum(J.nbytes + m.nbytes + f.nbytes for J, m, f in hv)
+        e2e = {"value": sum_over_ranks(world, ve) / te, "unit": UNIT,
+               "h2d_bytes_per_step": int(sum_over_ranks(world, nb)),
+               "d2h_bytes_per_step": int(sum_over_ranks(world, sum(f.nbytes for _, _, f in hv))),
+               "steps": ke, "path": "disptools_b200.solve_batched (C ABI, host float64 arrays)"}
+
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched gradient-descent voxel-iters/s, 64 volumes (config 4)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"config 4: 64 volumes, axes U{{48..192}}, 1-4 ellipsoids, "
+                                   f"FP32 fields, it_max={IT} per step",
+                       "voxels": total_vox, "volumes": len(sizes),
+                       "l2": "inputs larger than L2 (fields of all volumes 1.5 GB)",
+                       "iterations_per_step_rank0": iters / args.steps,
+                       "trials_per_iteration_rank0": trials / max(iters, 1),
+                       "parallelism": f"volumes split over {world} ranks by voxel count"},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+        }))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.workload == "c4" and args.impl == "b200":
+        run_c4(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
         if world > 1:
@@ -274,15 +374,6 @@ def main():
 
     # ---- roofline of the dominant kernel (device time of the launches that did work)
     hbm, peak_kind = peaks()
-    # A trial is two launches: the interior (TMA) kernel and the boundary
-    # layers kernel; their summed time is the trial's duration.
-    if "boundary" in prof and "trial" in prof:
-        nb_, tb_ = prof.pop("boundary")
-        nt_, tt_ = prof["trial"]
-        prof["trial"] = (nt_, tt_ + tb_)
-        prof_boundary = (nb_, tb_)
-    else:
-        prof_boundary = None
     dom = max(prof, key=lambda k: prof[k][1]) if prof else "trial"
     nl, tot_ms = prof.get(dom, (0, 0.0))
     avg_ms = tot_ms / max(nl, 1)
@@ -301,8 +392,6 @@ def main():
                    if v[0] else None,
                    "share": v[1] / max(sum(x[1] for x in prof.values()), 1e-12)}
                for k, v in prof.items()}
-    if prof_boundary:
-        kernels["trial"]["boundary_avg_ms"] = prof_boundary[1] / max(prof_boundary[0], 1)
     path_achieved = (29 + 41 * tbar) * value / 1e9 / world
 
     # ---- plain FP64 path (same workload, fewer steps)

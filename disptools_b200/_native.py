@@ -121,6 +121,8 @@ lib.dtb_jacobian_device_noalloc.restype = _I
 lib.dtb_jacobian_adjoint_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
 lib.dtb_jacobian_adjoint_device.restype = _I
 lib.dtb_kernel_launch_count.restype = C.c_ulonglong
+lib.dtb_release_device_memory.argtypes = []
+lib.dtb_release_device_memory.restype = _I
 
 
 class KernelProfile(C.Structure):
@@ -140,7 +142,7 @@ EXPORTED = [
     "dtb_generate_displacement", "dtb_generate_displacement_batched",
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
-    "dtb_get_profile", "dtb_jacobian_device_noalloc",
+    "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
 ]
 
 

@@ -137,6 +137,12 @@ def solve_batched(volumes: Iterable, algorithm: str = "gradient", precision: str
     return [(o, s.as_dict()) for o, s in zip(outs, stats)]
 
 
+def release_device_memory() -> None:
+    """Free the device memory the library keeps between calls on the current
+    device (workspace and staging area); the next call allocates again."""
+    N.check(N.lib.dtb_release_device_memory())
+
+
 def set_default_precision(precision) -> None:
     """Device precision used by the reference-named entry points."""
     N.check(N.lib.dtb_set_default_precision(N.precision_code(precision)))

@@ -151,33 +151,41 @@ namespace {
 struct Workspace {
     void *ptr = nullptr;
     size_t bytes = 0;
-    int device = -1;
 };
 std::mutex g_ws_mutex;
-Workspace g_ws;
+// Per device: the solver's scratch (pitched buffers, descriptors, partials)
+// and the staging area of host-array calls.  Both grow on demand and are
+// kept until dtb_release_device_memory() or the end of the process.
+std::vector<Workspace> g_ws, g_io;
 
-// Returns a device buffer of at least `bytes` on the current device.
-int workspace(size_t bytes, char **out) {
+int grow(std::vector<Workspace> &pool, size_t bytes, char **out) {
     int dev = 0;
     DTB_CUDA(cudaGetDevice(&dev));
-    if (g_ws.ptr && (g_ws.bytes < bytes || g_ws.device != dev)) {
-        if (g_ws.device == dev) cudaFree(g_ws.ptr);
-        g_ws.ptr = nullptr;
-        g_ws.bytes = 0;
+    if ((int) pool.size() <= dev) pool.resize(dev + 1);
+    Workspace &w = pool[dev];
+    if (w.ptr && w.bytes < bytes) {
+        cudaFree(w.ptr);
+        w.ptr = nullptr;
+        w.bytes = 0;
     }
-    if (!g_ws.ptr) {
+    if (!w.ptr) {
         const size_t want = bytes + bytes / 8;
-        if (cudaMalloc(&g_ws.ptr, want) != cudaSuccess) {
+        if (cudaMalloc(&w.ptr, want) != cudaSuccess) {
             cudaGetLastError();
-            g_ws.ptr = nullptr;
+            w.ptr = nullptr;
             DTB_FAIL(DTB_ERR_ALLOC, "cannot allocate the device workspace");
         }
-        g_ws.bytes = want;
-        g_ws.device = dev;
+        w.bytes = want;
     }
-    *out = static_cast<char *>(g_ws.ptr);
+    *out = static_cast<char *>(w.ptr);
     return DTB_OK;
 }
+
+// Returns a device buffer of at least `bytes` on the current device.
+int workspace(size_t bytes, char **out) { return grow(g_ws, bytes, out); }
+// Staging buffer of host-array calls (separate from the workspace, which the
+// solve itself carves up).
+int io_buffer(size_t bytes, char **out) { return grow(g_io, bytes, out); }
 
 // Bump allocator over a workspace region (256-byte alignment).
 struct Carve {
@@ -773,45 +781,44 @@ bool check_params(const dtb_params &p, const char **why) {
 }
 
 // Host-array solve: upload (converting to T), solve on the device, download.
+// Everything runs on the device's engine stream; the device buffers come from
+// the growing staging area, so a call allocates nothing once the area is large
+// enough, and the host waits once, when the results have arrived.
 template <typename T>
 int solve_host(int algorithm, int count, const dtb_volume *vols, const dtb_params &p, dtb_solve_stats *stats,
                int precision) {
-    cudaStream_t stream;
-    DTB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    struct Own {
-        std::vector<void *> ptrs;
-        cudaStream_t s;
-        ~Own() {
-            for (void *q : ptrs) cudaFree(q);
-            cudaStreamDestroy(s);
-        }
-    } own{{}, stream};
-    std::vector<DevVol<T>> dv(count);
-    size_t stage_elems = 0;
-    for (int i = 0; i < count; ++i) stage_elems = std::max(stage_elems, 3 * vols[i].nx * vols[i].ny * vols[i].nz);
-    double *stage = nullptr;
-    if (!std::is_same<T, double>::value) {
-        if (cudaMalloc(&stage, stage_elems * sizeof(double)) != cudaSuccess) {
-            cudaGetLastError();
-            DTB_FAIL(DTB_ERR_ALLOC, "cannot allocate the staging buffer");
-        }
-        own.ptrs.push_back(stage);
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    Engine *e = nullptr;
+    int rc = engine(&e);
+    if (rc != DTB_OK) return rc;
+    cudaStream_t stream = e->stream;
+    constexpr bool is_double = std::is_same<T, double>::value;
+    auto align = [](size_t b) { return (b + 255) & ~size_t(255); };
+    size_t need = 0, stage_elems = 0;
+    for (int i = 0; i < count; ++i) {
+        const size_t N = vols[i].nx * vols[i].ny * vols[i].nz;
+        need += align(3 * N * sizeof(T)) + align(N * sizeof(T)) + align(N);
+        stage_elems = std::max(stage_elems, 3 * N);
     }
+    if (!is_double) need += align(stage_elems * sizeof(double));
+    char *base = nullptr;
+    rc = io_buffer(need, &base);
+    if (rc != DTB_OK) return rc;
+    Carve cv{base};
+    double *stage = is_double ? nullptr : cv.take<double>(stage_elems);
+    std::vector<DevVol<T>> dv(count);
     for (int i = 0; i < count; ++i) {
         const dtb_volume &v = vols[i];
         const size_t N = v.nx * v.ny * v.nz;
-        T *field = nullptr, *Jt = nullptr;
-        uint8_t *mask = nullptr;
-        if (cudaMalloc(&field, 3 * N * sizeof(T)) != cudaSuccess || (own.ptrs.push_back(field), false) ||
-            cudaMalloc(&Jt, N * sizeof(T)) != cudaSuccess || (own.ptrs.push_back(Jt), false) ||
-            cudaMalloc(&mask, N) != cudaSuccess || (own.ptrs.push_back(mask), false)) {
-            cudaGetLastError();
-            DTB_FAIL(DTB_ERR_ALLOC, "cannot allocate device buffers for the volume");
-        }
-        if (std::is_same<T, double>::value) {
+        T *field = cv.take<T>(3 * N);
+        T *Jt = cv.take<T>(N);
+        uint8_t *mask = cv.take<uint8_t>(N);
+        if (is_double) {
             DTB_CUDA(cudaMemcpyAsync(field, v.field, 3 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
             DTB_CUDA(cudaMemcpyAsync(Jt, v.J, N * sizeof(double), cudaMemcpyHostToDevice, stream));
         } else {
+            // The stage is reused by every volume: stream order puts each
+            // copy after the previous conversion.
             DTB_CUDA(cudaMemcpyAsync(stage, v.field, 3 * N * sizeof(double), cudaMemcpyHostToDevice, stream));
             DTB_CUDA(launch_convert<T>(stage, 1, field, 3 * (long long) N, stream));
             DTB_CUDA(cudaMemcpyAsync(stage, v.J, N * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -821,19 +828,23 @@ int solve_host(int algorithm, int count, const dtb_volume *vols, const dtb_param
         DTB_CUDA(cudaMemcpyAsync(mask, v.mask, N, cudaMemcpyHostToDevice, stream));
         dv[i] = DevVol<T>{make_geom(v.nx, v.ny, v.nz, v.dx, v.dy, v.dz), Jt, mask, field};
     }
-    int rc = solve_device<T>(algorithm, dv, p, stats, precision, stream);
-    if (rc != DTB_OK) return rc;
+    rc = solve_device_on<T>(e, algorithm, dv, p, stats, precision);
+    if (rc != DTB_OK) {
+        cudaStreamSynchronize(stream);
+        cudaGetLastError();
+        return rc;
+    }
     for (int i = 0; i < count; ++i) {
         const dtb_volume &v = vols[i];
         const size_t N = v.nx * v.ny * v.nz;
-        if (std::is_same<T, double>::value) {
+        if (is_double) {
             DTB_CUDA(cudaMemcpyAsync(v.field, dv[i].field, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
         } else {
             DTB_CUDA(launch_to_double<T>(dv[i].field, stage, 3 * (long long) N, stream));
             DTB_CUDA(cudaMemcpyAsync(v.field, stage, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, stream));
         }
-        DTB_CUDA(cudaStreamSynchronize(stream));
     }
+    DTB_CUDA(cudaStreamSynchronize(stream));
     return DTB_OK;
 }
 
@@ -1038,6 +1049,27 @@ extern "C" int dtb_jacobian_adjoint_device(int precision, int order, size_t nx, 
         return adjoint_device_impl<float>(g, static_cast<const float *>(field), static_cast<const float *>(grad_J),
                                           static_cast<float *>(grad_field), s);
     DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
+extern "C" int dtb_release_device_memory(void) {
+    disptools_clear_error();
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    int dev = 0;
+    DTB_CUDA(cudaGetDevice(&dev));
+    for (std::vector<Workspace> *pool : {&g_ws, &g_io}) {
+        if ((int) pool->size() > dev && (*pool)[dev].ptr) {
+            cudaFree((*pool)[dev].ptr);
+            (*pool)[dev] = Workspace{};
+        }
+    }
+    // The cached step graph points into the freed workspace.
+    if ((int) g_engines.size() > dev && g_engines[dev] && g_engines[dev]->exec) {
+        cudaGraphExecDestroy(g_engines[dev]->exec);
+        g_engines[dev]->exec = nullptr;
+        g_engines[dev]->key = GraphKey{};
+    }
+    cudaGetLastError();
+    return DTB_OK;
 }
 
 // src/jacobian.c:7-21, on the device in FP64.

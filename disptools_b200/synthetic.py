@@ -51,19 +51,29 @@ def blob_problem(shape=(256, 256, 256), blobs: int = 16, seed: int = 0,
 
 def ellipsoid_problem(shape, seed: int = 0, count=None):
     """1-4 random ellipsoids (semi-axes U(4, 20) voxels) of J ~ U(0.80, 0.95);
-    J = 1 elsewhere; mask = the ellipsoids dilated by 2."""
+    J = 1 elsewhere; mask = the ellipsoids dilated by 2.
+
+    Each ellipsoid is evaluated and dilated inside its bounding box grown by
+    3 voxels: a dilation of a union is the union of the dilations, and no
+    voxel farther than 2 from an ellipsoid joins the mask."""
     rng = np.random.default_rng(seed)
     nz, ny, nx = shape
     J = np.ones(shape)
-    inside = np.zeros(shape, bool)
-    zz, yy, xx = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    mask = np.zeros(shape, bool)
     for _ in range(int(count or rng.integers(1, 5))):
         r = rng.uniform(4, 20, 3)
         c = rng.uniform([0, 0, 0], [nz, ny, nx])
-        e = ((zz - c[0]) / r[0]) ** 2 + ((yy - c[1]) / r[1]) ** 2 + ((xx - c[2]) / r[2]) ** 2 <= 1
-        J[e] = rng.uniform(0.80, 0.95)
-        inside |= e
-    return np.ascontiguousarray(J), np.ascontiguousarray(_dilate(inside, 2.0))
+        v = rng.uniform(0.80, 0.95)
+        lo = [max(0, int(np.floor(c[a] - r[a])) - 3) for a in range(3)]
+        hi = [min(shape[a], int(np.ceil(c[a] + r[a])) + 4) for a in range(3)]
+        z = np.arange(lo[0], hi[0])[:, None, None]
+        y = np.arange(lo[1], hi[1])[None, :, None]
+        x = np.arange(lo[2], hi[2])[None, None, :]
+        e = ((z - c[0]) / r[0]) ** 2 + ((y - c[1]) / r[1]) ** 2 + ((x - c[2]) / r[2]) ** 2 <= 1
+        box = tuple(slice(a, b) for a, b in zip(lo, hi))
+        J[box][e] = v
+        mask[box] |= _dilate(e, 2.0)
+    return np.ascontiguousarray(J), np.ascontiguousarray(mask)
 
 
 def batch_sizes(count: int = 64, low: int = 48, high: int = 192, seed: int = 0):

@@ -243,6 +243,15 @@ int dtb_jacobian_device_noalloc(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, void *J, void *stream);
 
+/* Frees the device memory the library keeps on the current device between
+ * calls: the solver's workspace (pitched field buffers, descriptors, tile
+ * partials) and the staging area of host-array calls, both of which grow to
+ * the largest solve seen and are otherwise kept until the process exits.  No
+ * counterpart in the reference, whose CUDA path allocates and frees its
+ * buffers in every call (cuda/displacement_field_gradient.cu:213-236,
+ * 458-467).  Returns DTB_OK; must not overlap a running call on the device. */
+int dtb_release_device_memory(void);
+
 /* Number of kernels this library has launched in the process (a counter
  * kept by the host code, for benchmarks that report launch counts; each
  * replay of a captured step graph counts the kernels it contains). */

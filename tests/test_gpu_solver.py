@@ -148,3 +148,55 @@ def test_full_size_256_mixed_properties(oracle):
     assert tot == pytest.approx(st["error"], rel=1e-4)
     _, s0 = dt.solve(Jt, mask, precision="mixed", it_max=0)
     assert st["error"] < s0["error"]
+
+
+def test_config4_batched_vs_oracle(oracle):
+    """Config-4 shaped batch (ellipsoid targets, one size per volume), scaled
+    down so the oracle finishes in seconds: the batched FP64 solve equals the
+    oracle's solve of each volume, the batched mixed solve meets the residual
+    rule."""
+    from disptools_b200.synthetic import batch_sizes, ellipsoid_problem
+    sizes = batch_sizes(6, low=16, high=40, seed=4)
+    vols = [ellipsoid_problem(s, seed=i) for i, s in enumerate(sizes)]
+    res64 = dt.solve_batched(vols, precision="fp64", it_max=80)
+    for (Jt, mask), (f64, s64) in zip(vols, res64):
+        ref, so = oracle.solve("gradient", Jt, mask, it_max=80)
+        assert s64["iterations"] == so.iterations and s64["reason"] == so.reason
+        assert np.max(np.abs(f64 - ref)) <= 1e-10
+    # final residuals of full solves (the residual rule holds at the end of
+    # a solve, not along the way)
+    res32 = dt.solve_batched(vols, precision="mixed", it_max=1000)
+    for (Jt, mask), (f32, _) in zip(vols, res32):
+        ref, _ = oracle.solve("gradient", Jt, mask, it_max=1000)
+        r_ref = masked_max(oracle.jacobian(ref), Jt, mask)
+        r_32 = masked_max(oracle.jacobian(f32), Jt, mask)
+        assert abs(r_32 - r_ref) <= 1e-4, (r_32, r_ref)
+
+
+def test_config4_batched_large_properties(oracle):
+    """Twelve volumes with axes in [48, 128] in one mixed batched solve: the
+    reported masked maximum of every volume matches an FP64 recomputation
+    and no volume's error grew."""
+    from disptools_b200.synthetic import batch_sizes, ellipsoid_problem
+    sizes = batch_sizes(12, low=48, high=128, seed=5)
+    vols = [ellipsoid_problem(s, seed=100 + i) for i, s in enumerate(sizes)]
+    res = dt.solve_batched(vols, precision="mixed", it_max=12)
+    res0 = dt.solve_batched(vols, precision="mixed", it_max=0)
+    for (Jt, mask), (f, st), (_, s0) in zip(vols, res, res0):
+        J = oracle.jacobian(f)
+        assert abs(masked_max(J, Jt, mask) - st["max_error"]) <= 1e-5
+        assert st["error"] <= s0["error"]
+
+
+def test_release_device_memory_then_solve_again():
+    """Freeing the cached device memory between solves changes no result."""
+    Jt, mask = ball_problem(20, 10, 5, 0.9)
+    a, sa = dt.solve(Jt, mask, precision="mixed", it_max=30)
+    dt.release_device_memory()
+    b, sb = dt.solve(Jt, mask, precision="mixed", it_max=30)
+    dt.release_device_memory()
+    c, sc = dt.solve_batched([(Jt, mask)], precision="fp64", it_max=30)[0]
+    d, sd = dt.solve(Jt, mask, precision="fp64", it_max=30)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(c, d)
+    assert sa["iterations"] == sb["iterations"] and sc["iterations"] == sd["iterations"]
