@@ -263,6 +263,7 @@ def run_c4(args, world, rank, local):
     barrier(world)
     ms = max_over_ranks(world, e0.elapsed_time(e1))
     launches = dt.kernel_launch_count() - launches0
+    tiles = dt.tile_config() if vols else None
     value = sum_over_ranks(world, vi) / (ms / 1000.0)
 
     e2e = None
@@ -298,7 +299,8 @@ def run_c4(args, world, rank, local):
                        "l2": "inputs larger than L2 (fields of all volumes 1.5 GB)",
                        "iterations_per_step_rank0": iters / args.steps,
                        "trials_per_iteration_rank0": trials / max(iters, 1),
-                       "parallelism": f"volumes split over {world} ranks by voxel count"},
+                       "parallelism": f"volumes split over {world} ranks by voxel count",
+                       "tiles": tiles},
             "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         }))
 
@@ -366,6 +368,7 @@ def main():
     ms = e0.elapsed_time(e1)
     launches = dt.kernel_launch_count() - launches0
     prof = dt.kernel_profile()
+    tiles = dt.tile_config()
     dt.set_profiling(False)
     ms_max = max_over_ranks(world, ms)
     total_vi = sum_over_ranks(world, float(nvox) * iters)
@@ -474,7 +477,8 @@ def main():
                        "size": [n, n, n], "it_max_per_step": IT,
                        "l2": "inputs larger than L2 (FP32 field 201 MB + gradient 201 MB)",
                        "iterations_per_step": iters / args.steps,
-                       "trials_per_iteration": tbar, "parallelism": f"{world} independent volumes"},
+                       "trials_per_iteration": tbar, "parallelism": f"{world} independent volumes",
+                       "tiles": tiles, "tiles_from": "autotuner (first solve of the shape, in warm-up)"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": peak_kind,

@@ -123,6 +123,10 @@ lib.dtb_jacobian_adjoint_device.restype = _I
 lib.dtb_kernel_launch_count.restype = C.c_ulonglong
 lib.dtb_release_device_memory.argtypes = []
 lib.dtb_release_device_memory.restype = _I
+lib.dtb_set_autotune.argtypes = [_I]
+lib.dtb_set_autotune.restype = _I
+lib.dtb_get_tile_config.argtypes = [C.POINTER(C.c_int)]
+lib.dtb_get_tile_config.restype = _I
 
 
 class KernelProfile(C.Structure):
@@ -143,6 +147,7 @@ EXPORTED = [
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
     "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
+    "dtb_set_autotune", "dtb_get_tile_config",
 ]
 
 

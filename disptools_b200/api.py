@@ -137,6 +137,19 @@ def solve_batched(volumes: Iterable, algorithm: str = "gradient", precision: str
     return [(o, s.as_dict()) for o, s in zip(outs, stats)]
 
 
+def set_autotune(on: bool) -> bool:
+    """Turn the tile-shape autotuner of gradient solves on or off; returns
+    the previous setting."""
+    return bool(N.lib.dtb_set_autotune(1 if on else 0))
+
+
+def tile_config() -> dict:
+    """Tile shape of the last solve on the current device."""
+    a = (C.c_int * 4)()
+    N.check(N.lib.dtb_get_tile_config(a))
+    return {"tile_x": a[0], "trial_threads_y": a[1], "gradient_threads_y": a[2], "bz": a[3]}
+
+
 def release_device_memory() -> None:
     """Free the device memory the library keeps between calls on the current
     device (workspace and staging area); the next call allocates again."""

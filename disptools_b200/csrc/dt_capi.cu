@@ -16,7 +16,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -224,14 +226,8 @@ Geom make_geom(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     return g;
 }
 
-int pick_bz(int nz) {
-    const char *e = std::getenv("DISPTOOLS_B200_BZ");
-    if (e) {
-        const int v = std::atoi(e);
-        if (v > 0) return v;
-    }
-    return nz < 32 ? nz : 32;
-}
+// Planes per tile along z for a volume of nz planes.
+int bz_for(int nz, int bz) { return nz < bz ? nz : bz; }
 
 int steps_per_graph() {
     const char *e = std::getenv("DISPTOOLS_B200_STEPS_PER_GRAPH");
@@ -343,6 +339,7 @@ struct Engine {
     std::vector<cudaEvent_t> evs;
     cudaGraphExec_t exec = nullptr;
     GraphKey key;
+    int last_cfg[4] = {0, 0, 0, 0};  // tile shapes of the last solve (TileConfig order)
 };
 std::vector<Engine *> g_engines;
 
@@ -393,47 +390,76 @@ int ensure_profiling(Engine *e, size_t nk) {
     return DTB_OK;
 }
 
-// Tile and block shape of the TMA kernels.  Tiles are 32 x 16 voxels: the
-// gradient kernel runs blocks of 32 x 8 threads (two tile rows each), the
-// trial kernel 16 x 16 threads (two columns of one row each); both measured
-// fastest at 256^3 on B200 (two resident blocks per SM).
-// DISPTOOLS_B200_TILE_X=64 selects 64-wide FP32 tiles (longer TMA rows, one
-// 512-thread block per SM), DISPTOOLS_B200_THREADS_Y=16 one tile row per
-// gradient thread and DISPTOOLS_B200_TRIAL_THREADS_Y=8 two tile rows per
-// trial thread (32-wide tiles only).
-int pick_tile_x(size_t tsize) {
-    const char *e = std::getenv("DISPTOOLS_B200_TILE_X");
-    if (e && tsize == 4) {
-        const int v = std::atoi(e);
-        if (v == 32 || v == 64) return v;
+// Tile and block shape of the TMA kernels (gradient method):
+//   tile_x    tile width in voxels (32, or 64 for FP32); tiles are TT_Y high
+//   trial_ty  thread rows of the trial kernel (16: one tile row and two
+//             columns per thread; 8: two rows)
+//   grad_ty   thread rows of the gradient kernel (8: two tile rows per
+//             thread; 16: one)
+//   bz        planes of a tile along z (capped at nz)
+// The greedy method runs BX x BY tiles of bz planes.
+struct TileConfig {
+    int tile_x = 32, trial_ty = 16, grad_ty = 8, bz = 32;
+    bool operator==(const TileConfig &o) const {
+        return tile_x == o.tile_x && trial_ty == o.trial_ty && grad_ty == o.grad_ty && bz == o.bz;
     }
-    return 32;
-}
-int pick_threads_y(int tile_x) {
-    const char *e = std::getenv("DISPTOOLS_B200_THREADS_Y");
-    if (e && tile_x == 32) {
+};
+
+// Explicit shapes from the environment (DISPTOOLS_B200_TILE_X = 32 | 64,
+// DISPTOOLS_B200_TRIAL_THREADS_Y = 8 | 16, DISPTOOLS_B200_THREADS_Y = 8 | 16,
+// DISPTOOLS_B200_BZ > 0).  Returns true when any is set; the autotuner is
+// then skipped.
+bool env_config(size_t tsize, TileConfig *c) {
+    bool any = false;
+    auto num = [&](const char *name, int *out, std::initializer_list<int> allowed) {
+        const char *e = std::getenv(name);
+        if (!e) return;
         const int v = std::atoi(e);
-        if (v == 8 || v == 16) return v;
-    }
-    return 8;
-}
-int pick_trial_threads_y(int tile_x) {
-    const char *e = std::getenv("DISPTOOLS_B200_TRIAL_THREADS_Y");
-    if (e && tile_x == 32) {
-        const int v = std::atoi(e);
-        if (v == 8 || v == 16) return v;
-    }
-    return 16;
+        bool ok = allowed.size() == 0 ? v > 0 : false;
+        for (int a : allowed) ok |= v == a;
+        if (ok) {
+            *out = v;
+            any = true;
+        }
+    };
+    num("DISPTOOLS_B200_TILE_X", &c->tile_x, {32, 64});
+    num("DISPTOOLS_B200_TRIAL_THREADS_Y", &c->trial_ty, {8, 16});
+    num("DISPTOOLS_B200_THREADS_Y", &c->grad_ty, {8, 16});
+    num("DISPTOOLS_B200_BZ", &c->bz, {});
+    if (tsize != 4) c->tile_x = 32;
+    if (c->tile_x == 64) c->trial_ty = 16, c->grad_ty = 8;
+    return any;
 }
 
 template <typename T>
+int choose_config(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                  int precision, TileConfig *out);
+
+// One solve of `vols` on the engine's stream with tile shapes `cfg` (chosen
+// by choose_config when null).  With `tune_ms` set it solves nothing: it
+// sets the solve up on zeroed inputs, times one gradient and one trial launch
+// of a mid-solve state (best of three after one warm-up) into *tune_ms and
+// returns; the caller's arrays are not read.
+template <typename T>
 int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
-                    dtb_solve_stats *stats, int precision) {
+                    dtb_solve_stats *stats, int precision, const TileConfig *cfg_in = nullptr,
+                    float *tune_ms = nullptr) {
     cudaStream_t stream = e->stream;
     const int count = (int) vols.size();
-    const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? pick_tile_x(sizeof(T)) : BX;
-    const int threads_y = pick_threads_y(tile_x);
-    const int trial_ty = pick_trial_threads_y(tile_x);
+    TileConfig cfg;
+    if (cfg_in) {
+        cfg = *cfg_in;
+    } else {
+        const int rc0 = choose_config<T>(e, algorithm, vols, p, precision, &cfg);
+        if (rc0 != DTB_OK) return rc0;
+    }
+    e->last_cfg[0] = cfg.tile_x;
+    e->last_cfg[1] = cfg.trial_ty;
+    e->last_cfg[2] = cfg.grad_ty;
+    e->last_cfg[3] = cfg.bz;
+    const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? cfg.tile_x : BX;
+    const int threads_y = cfg.grad_ty;
+    const int trial_ty = cfg.trial_ty;
     const bool gradient = algorithm == DTB_ALGORITHM_GRADIENT;
     // ---- workspace layout: every buffer of the solve is the library's own,
     // in the pitched layout.
@@ -446,7 +472,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     for (int i = 0; i < count; ++i) {
         const Geom g = pitched(vols[i].g);
         geo[i] = g;
-        const int bz = pick_bz(g.nz);
+        const int bz = bz_for(g.nz, cfg.bz);
         const int t = ((g.nx + tile_x - 1) / tile_x) * ((g.ny + tile_y - 1) / tile_y) * ((g.nz + bz - 1) / bz);
         tiles[i] = t;
         tbegin[i] = total_tiles;
@@ -495,7 +521,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         d.part_g = cv.take<double>(tiles[i]);
         d.st = cv.take<SolverState>(1);
         d_maps[i] = cv.take<CUtensorMap>(7);
-        const int bz = pick_bz(g.nz);
+        const int bz = bz_for(g.nz, cfg.bz);
         d.tiles_x = (g.nx + tile_x - 1) / tile_x;
         d.tiles_y = (g.ny + tile_y - 1) / tile_y;
         d.tiles_z = (g.nz + bz - 1) / bz;
@@ -524,11 +550,20 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         s.M_last = DBL_MAX;
         s.phase = PH_EVAL0;
 
-        // Inputs into the pitched layout.
-        const size_t rows = (size_t) gu.ny * gu.nz;
-        DTB_CUDA(copy_rows<T>(d.field[0], g.ys, vols[i].field, gu.ys, gu.nx, 3 * rows, stream));
-        DTB_CUDA(copy_rows<T>(Jt, g.ys, vols[i].Jt, gu.ys, gu.nx, rows, stream));
-        DTB_CUDA(copy_rows<uint8_t>(mask, g.ys, vols[i].mask, gu.ys, gu.nx, rows, stream));
+        if (tune_ms) {
+            // A step in the main loop: both kernels do all their work.
+            s.phase = gradient ? PH_MAIN : PH_GREEDY;
+            s.need_gradient = 1;
+            DTB_CUDA(cudaMemsetAsync(d.field[0], 0, 3 * N * sizeof(T), stream));
+            DTB_CUDA(cudaMemsetAsync(Jt, 0, N * sizeof(T), stream));
+            DTB_CUDA(cudaMemsetAsync(mask, 0, N, stream));
+        } else {
+            // Inputs into the pitched layout.
+            const size_t rows = (size_t) gu.ny * gu.nz;
+            DTB_CUDA(copy_rows<T>(d.field[0], g.ys, vols[i].field, gu.ys, gu.nx, 3 * rows, stream));
+            DTB_CUDA(copy_rows<T>(Jt, g.ys, vols[i].Jt, gu.ys, gu.nx, rows, stream));
+            DTB_CUDA(copy_rows<uint8_t>(mask, g.ys, vols[i].mask, gu.ys, gu.nx, rows, stream));
+        }
         // The second field buffer starts at zero: the greedy update never
         // writes boundary voxels, so they keep the buffer's content
         // (src/displacement_field_greedy.c:43-65 with calloc'd buffers).
@@ -591,6 +626,23 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     };
 
     cudaEvent_t ev0 = e->ev0, ev1 = e->ev1;
+    if (tune_ms) {
+        float best = FLT_MAX;
+        for (int r = 0; r < 4; ++r) {
+            for (int i = 0; i < count; ++i)
+                DTB_CUDA(cudaMemcpyAsync(desc[i].st, &hst[i], sizeof(SolverState), cudaMemcpyHostToDevice, stream));
+            DTB_CUDA(cudaEventRecord(ev0, stream));
+            if (gradient) DTB_CUDA(launch_g(nullptr));
+            DTB_CUDA(launch_t(nullptr));
+            DTB_CUDA(cudaEventRecord(ev1, stream));
+            DTB_CUDA(cudaEventSynchronize(ev1));
+            float ms = 0.f;
+            DTB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            if (r > 0) best = std::min(best, ms);
+        }
+        *tune_ms = best;
+        return DTB_OK;
+    }
     DTB_CUDA(cudaEventRecord(ev0, stream));
 
     // Evaluate the initial fields (launched once, outside the graph; this is
@@ -740,6 +792,86 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
             o.device_ms = ms;
         }
     }
+    return DTB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the tile shapes: the first gradient solve of a problem shape
+// on a device times each candidate shape on the solve's own geometry (see
+// solve_device_on's tuning mode) and keeps the fastest for later solves of
+// that shape.  Solves of fewer than AUTOTUNE_MIN_VOXELS voxels, greedy solves
+// and solves with shapes set in the environment take the fixed shapes.
+// ---------------------------------------------------------------------------
+struct TuneKey {
+    int device;
+    size_t tsize;
+    int count;
+    long long voxels;
+    int mx, my, mz;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(device, tsize, count, voxels, mx, my, mz) <
+               std::tie(o.device, o.tsize, o.count, o.voxels, o.mx, o.my, o.mz);
+    }
+};
+std::map<TuneKey, TileConfig> g_tuned;  // guarded by g_ws_mutex
+int g_autotune = -1;                     // -1: read DISPTOOLS_B200_AUTOTUNE on first use
+constexpr long long AUTOTUNE_MIN_VOXELS = 1ll << 21;
+
+bool autotune_enabled() {
+    if (g_autotune < 0) {
+        const char *v = std::getenv("DISPTOOLS_B200_AUTOTUNE");
+        g_autotune = (v && std::strcmp(v, "0") == 0) ? 0 : 1;
+    }
+    return g_autotune != 0;
+}
+
+// Candidate shapes, the fixed default first.
+std::vector<TileConfig> tile_candidates(size_t tsize) {
+    std::vector<TileConfig> c = {{32, 16, 8, 32}, {32, 16, 16, 32}, {32, 16, 8, 16}, {32, 16, 8, 64},
+                                 {32, 8, 8, 32}};
+    if (tsize == 4) c.push_back({64, 16, 8, 32});
+    return c;
+}
+
+template <typename T>
+int choose_config(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
+                  int precision, TileConfig *out) {
+    TileConfig c;
+    if (env_config(sizeof(T), &c) || algorithm != DTB_ALGORITHM_GRADIENT || !autotune_enabled()) {
+        *out = c;
+        return DTB_OK;
+    }
+    TuneKey key{e->device, sizeof(T), (int) vols.size(), 0, 0, 0, 0};
+    for (const DevVol<T> &v : vols) {
+        key.voxels += (long long) v.g.nx * v.g.ny * v.g.nz;
+        key.mx = std::max(key.mx, v.g.nx);
+        key.my = std::max(key.my, v.g.ny);
+        key.mz = std::max(key.mz, v.g.nz);
+    }
+    if (key.voxels < AUTOTUNE_MIN_VOXELS) {
+        *out = c;
+        return DTB_OK;
+    }
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+        *out = it->second;
+        return DTB_OK;
+    }
+    TileConfig best = c;
+    float best_ms = FLT_MAX;
+    for (const TileConfig &cand : tile_candidates(sizeof(T))) {
+        float ms = FLT_MAX;
+        const int rc = solve_device_on<T>(e, algorithm, vols, p, nullptr, precision, &cand, &ms);
+        if (rc != DTB_OK) return rc;
+        // A shape must beat the best so far by 1 % to replace it, so timing
+        // noise does not move the choice away from the default.
+        if (best_ms == FLT_MAX || ms < 0.99f * best_ms) {
+            best = cand;
+            best_ms = ms;
+        }
+    }
+    g_tuned[key] = best;
+    *out = best;
     return DTB_OK;
 }
 
@@ -977,7 +1109,7 @@ namespace {
 template <typename T>
 int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(g_ws_mutex);
-    const int bz = pick_bz(g.nz);
+    const int bz = bz_for(g.nz, 32);
     const int ntiles = ((g.nx + BX - 1) / BX) * ((g.ny + BY - 1) / BY) * ((g.nz + bz - 1) / bz);
     char *base = nullptr;
     int rc = workspace(1024 + sizeof(VolumeDesc<T>) + (size_t) ntiles * sizeof(int), &base);
@@ -1049,6 +1181,26 @@ extern "C" int dtb_jacobian_adjoint_device(int precision, int order, size_t nx, 
         return adjoint_device_impl<float>(g, static_cast<const float *>(field), static_cast<const float *>(grad_J),
                                           static_cast<float *>(grad_field), s);
     DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
+extern "C" int dtb_set_autotune(int on) {
+    disptools_clear_error();
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    const int prev = autotune_enabled() ? 1 : 0;
+    g_autotune = on ? 1 : 0;
+    return prev;
+}
+
+extern "C" int dtb_get_tile_config(int *shape) {
+    disptools_clear_error();
+    if (!shape) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    int dev = 0;
+    DTB_CUDA(cudaGetDevice(&dev));
+    if ((int) g_engines.size() <= dev || !g_engines[dev] || g_engines[dev]->last_cfg[0] == 0)
+        DTB_FAIL(DTB_ERR_ARGUMENT, "no solve has run on this device");
+    for (int k = 0; k < 4; ++k) shape[k] = g_engines[dev]->last_cfg[k];
+    return DTB_OK;
 }
 
 extern "C" int dtb_release_device_memory(void) {

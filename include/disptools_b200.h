@@ -243,6 +243,23 @@ int dtb_jacobian_device_noalloc(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, void *J, void *stream);
 
+/* Tile-shape autotuner of the gradient method.  When on (the default, or
+ * DISPTOOLS_B200_AUTOTUNE=0 in the environment at first use for off), the
+ * first solve of a problem shape on a device (shape = element type, volume
+ * count, total voxels, largest extent per axis) with at least 2^21 voxels
+ * times each candidate tile shape on the solve's own geometry, one gradient
+ * and one trial launch on zeroed inputs each, and keeps the fastest for
+ * that shape for the rest of the process.  Shapes set in the environment
+ * (DISPTOOLS_B200_TILE_X, _TRIAL_THREADS_Y, _THREADS_Y, _BZ) take
+ * precedence.  Returns the previous setting (0 or 1). */
+int dtb_set_autotune(int on);
+
+/* Tile shape of the last solve on the current device: shape[0] tile width
+ * in voxels, shape[1] thread rows of the trial kernel, shape[2] thread rows
+ * of the gradient kernel, shape[3] planes per tile along z.  Returns
+ * DTB_ERR_ARGUMENT before the first solve on the device. */
+int dtb_get_tile_config(int shape[4]);
+
 /* Frees the device memory the library keeps on the current device between
  * calls: the solver's workspace (pitched field buffers, descriptors, tile
  * partials) and the staging area of host-array calls, both of which grow to

@@ -200,3 +200,71 @@ def test_release_device_memory_then_solve_again():
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(c, d)
     assert sa["iterations"] == sb["iterations"] and sc["iterations"] == sd["iterations"]
+
+
+TILE_CANDIDATES = [
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 32},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 16},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 64},
+    {"tile_x": 32, "trial_threads_y": 8, "gradient_threads_y": 8, "bz": 32},
+    {"tile_x": 64, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
+]
+
+
+def test_autotuned_shapes(oracle, monkeypatch):
+    """A volume large enough for the autotuner (2.3 M voxels): the chosen
+    shapes are candidates; the FP64 solve with the tuned shapes equals the
+    oracle's; forcing the tuned shapes through the environment reproduces
+    the tuned mixed solve bit for bit."""
+    from disptools_b200.synthetic import blob_problem
+    Jt, mask = blob_problem((112, 128, 160), blobs=6, seed=3)
+    prev = dt.set_autotune(True)
+    try:
+        out64, _ = dt.solve(Jt, mask, precision="fp64", it_max=3)
+        cfg64 = dt.tile_config()
+        out32, _ = dt.solve(Jt, mask, precision="mixed", it_max=6)
+        cfg32 = dt.tile_config()
+    finally:
+        dt.set_autotune(prev)
+    assert cfg64 in TILE_CANDIDATES and cfg64["tile_x"] == 32
+    assert cfg32 in TILE_CANDIDATES
+    ref, _ = oracle.solve("gradient", Jt, mask, it_max=3)
+    assert np.max(np.abs(out64 - ref)) <= 1e-10
+    monkeypatch.setenv("DISPTOOLS_B200_TILE_X", str(cfg32["tile_x"]))
+    monkeypatch.setenv("DISPTOOLS_B200_TRIAL_THREADS_Y", str(cfg32["trial_threads_y"]))
+    monkeypatch.setenv("DISPTOOLS_B200_THREADS_Y", str(cfg32["gradient_threads_y"]))
+    monkeypatch.setenv("DISPTOOLS_B200_BZ", str(cfg32["bz"]))
+    again, _ = dt.solve(Jt, mask, precision="mixed", it_max=6)
+    assert dt.tile_config() == cfg32
+    np.testing.assert_array_equal(out32, again)
+
+
+@pytest.mark.parametrize("shape", TILE_CANDIDATES)
+def test_every_tile_shape_fp64_matches_oracle(oracle, monkeypatch, shape):
+    """Each candidate shape (forced through the environment) gives the
+    oracle's FP64 result on a volume with ragged tiles in every axis."""
+    if shape["tile_x"] == 64:
+        pytest.skip("64-wide tiles are FP32 only")
+    for k, v in (("TILE_X", "tile_x"), ("TRIAL_THREADS_Y", "trial_threads_y"),
+                 ("THREADS_Y", "gradient_threads_y"), ("BZ", "bz")):
+        monkeypatch.setenv("DISPTOOLS_B200_" + k, str(shape[v]))
+    Jt, mask = ball_problem(45, 20, 9, 0.9)
+    out, st = dt.solve(Jt, mask, precision="fp64", it_max=40)
+    assert dt.tile_config() == shape
+    ref, so = oracle.solve("gradient", Jt, mask, it_max=40)
+    assert st["iterations"] == so.iterations
+    assert np.max(np.abs(out - ref)) <= 1e-10
+
+
+@pytest.mark.parametrize("shape", TILE_CANDIDATES)
+def test_every_tile_shape_mixed_residual(oracle, monkeypatch, shape):
+    for k, v in (("TILE_X", "tile_x"), ("TRIAL_THREADS_Y", "trial_threads_y"),
+                 ("THREADS_Y", "gradient_threads_y"), ("BZ", "bz")):
+        monkeypatch.setenv("DISPTOOLS_B200_" + k, str(shape[v]))
+    Jt, mask = ball_problem(45, 20, 9, 0.9)
+    out, st = dt.solve(Jt, mask, precision="mixed", it_max=1000)
+    assert dt.tile_config() == shape
+    ref, _ = oracle.solve("gradient", Jt, mask, it_max=1000)
+    r_ref = masked_max(oracle.jacobian(ref), Jt, mask)
+    assert abs(masked_max(oracle.jacobian(out), Jt, mask) - r_ref) <= 1e-4
