@@ -47,9 +47,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="c2", choices=["c2", "c4"],
+    p.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"],
                    help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
-                        "axes U{48..192} split over the ranks")
+                        "axes U{48..192} split over the ranks; c5: one 512x512x384 volume per "
+                        "rank through a 3-level pyramid, plus greedy on the coarsest level")
     return p.parse_args()
 
 
@@ -305,9 +306,90 @@ def run_c4(args, world, rank, local):
         }))
 
 
+def run_c5(args, world, rank, local):
+    """Config 5: a 512x512x384 volume (64 blobs as in config 2) per rank,
+    FP32 fields.  One step = the 3-level pyramid of the gradient method
+    (disptools_b200.pyramid.displacement, it_max per level = --it-max) on
+    device tensors, then a greedy solve (it_max = --it-max) of the coarsest
+    level's target.  Metric: voxel-iterations of all solves in the step
+    (each level counted at its padded size) per second."""
+    import numpy as np
+    import torch
+
+    import disptools_b200 as dt
+    from disptools_b200 import pyramid, torch_ops
+    from disptools_b200.synthetic import blob_problem_device
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    IT = args.it_max
+    shape = (384, 512, 512)
+    J, mask = blob_problem_device(shape, blobs=64, seed=rank, device=dev)
+    sizes, spacings = pyramid.level_geometry(tuple(s + 2 for s in shape), (1.0, 1.0, 1.0), 3)
+    # the coarsest level's target and mask for the greedy solve, built once
+    Jp = torch.nn.functional.pad(J[None, None], (1,) * 6, mode="replicate")[0, 0]
+    mp = torch.nn.functional.pad(mask.double()[None, None], (1,) * 6, mode="constant", value=0.0)[0, 0]
+    Jc = pyramid.scale_image(Jp, spacings[0], sizes[2]).float().contiguous()
+    mc = (pyramid.scale_image(mp, spacings[0], sizes[2], nearest=True) != 0).contiguous()
+    fc = torch.zeros((3,) + sizes[2], dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        _, st = pyramid.displacement(J, mask=mask, levels=3, it_max=IT, return_stats=True)
+        fc.zero_()
+        sg = torch_ops.solve(Jc, mc, fc, spacing=spacings[2], algorithm="greedy", it_max=IT)
+        vi = 0.0
+        for s, size in zip(st, sizes[::-1]):
+            vi += float(np.prod(size)) * iterations_done(s)
+        vi += float(np.prod(sizes[2])) * iterations_done(sg)
+        return vi, [iterations_done(s) for s in st] + [iterations_done(sg)]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = dt.kernel_launch_count()
+    vi = 0.0
+    its = None
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            v, its = step()
+            vi += v
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    launches = dt.kernel_launch_count() - launches0
+    value = sum_over_ranks(world, vi) / (ms / 1000.0)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "pyramid gradient-descent voxel-iters/s, 512x512x384 (config 5)",
+            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"config 5: 512x512x384, 64 Gaussian blobs, 3-level pyramid "
+                                   f"(gradient, it_max={IT} per level) + greedy on the coarsest "
+                                   f"level (it_max={IT}), FP32 fields",
+                       "level_sizes_padded": [list(s) for s in sizes],
+                       "iterations_per_solve": its,
+                       "l2": "inputs larger than L2 (finest field 1.2 GB)",
+                       "parallelism": f"{world} independent volumes"},
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.workload == "c5" and args.impl == "b200":
+        run_c5(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "c4" and args.impl == "b200":
         run_c4(args, world, rank, local)
         if world > 1:

@@ -123,6 +123,10 @@ lib.dtb_jacobian_adjoint_device.restype = _I
 lib.dtb_kernel_launch_count.restype = C.c_ulonglong
 lib.dtb_release_device_memory.argtypes = []
 lib.dtb_release_device_memory.restype = _I
+lib.dtb_smooth_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
+lib.dtb_smooth_device.restype = _I
+lib.dtb_resample_device.argtypes = [_I, _I, _I, _SZ, _SZ, _SZ, _SZ, _SZ, _SZ, _P, _P, _P]
+lib.dtb_resample_device.restype = _I
 lib.dtb_set_autotune.argtypes = [_I]
 lib.dtb_set_autotune.restype = _I
 lib.dtb_get_tile_config.argtypes = [C.POINTER(C.c_int)]
@@ -147,7 +151,7 @@ EXPORTED = [
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
     "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
-    "dtb_set_autotune", "dtb_get_tile_config",
+    "dtb_set_autotune", "dtb_get_tile_config", "dtb_smooth_device", "dtb_resample_device",
 ]
 
 

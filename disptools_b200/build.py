@@ -33,6 +33,7 @@ UNITS = [
     ("dt_kernels_f64.cu", ["-fmad=false"]),
     ("dt_capi.cu", []),
     ("dt_noalloc.cu", []),
+    ("dt_resample.cu", []),
 ]
 HEADERS = ["dt_internal.h", "dt_kernels.cuh", "dt_kernels_tma.cuh", "dt_tma.cuh"]
 

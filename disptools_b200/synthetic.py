@@ -3,7 +3,8 @@
 These stand in for data sets (the reference publishes no benchmark data):
 
 * :func:`blob_problem` — target J = clip(exp(sum of isotropic Gaussian
-  blobs), 0.7, 1.4), mask = voxels with |log J| > 0.01 dilated by 3;
+  blobs), 0.7, 1.4), mask = voxels with |log J| > 0.01 dilated by 3
+  (:func:`blob_problem_device` computes it with torch on a device);
 * :func:`ellipsoid_problem` — 1 to 4 ellipsoids of J in [0.80, 0.95],
   J = 1 elsewhere, mask = ellipsoids dilated by 2;
 * :func:`smooth_field` — Gaussian-filtered white noise scaled to a maximum
@@ -47,6 +48,45 @@ def blob_problem(shape=(256, 256, 256), blobs: int = 16, seed: int = 0,
     J = np.clip(np.exp(logj), 0.7, 1.4)
     mask = _dilate(np.abs(logj) > 0.01, 3.0)
     return np.ascontiguousarray(J), np.ascontiguousarray(mask)
+
+
+def blob_problem_device(shape=(256, 256, 256), blobs: int = 16, seed: int = 0,
+                        sigma=(8.0, 24.0), amplitude: float = 0.25, device="cuda"):
+    """:func:`blob_problem` computed with torch on `device` (float64), for
+    volumes where the NumPy version is slow: the same random draws, the
+    same formulas, the dilation by 3 as a union of the mask shifted by every
+    integer offset of length <= 3 (which is what a Euclidean distance <= 3
+    to the mask means on the grid).  Returns (J float64, mask bool) tensors;
+    exp() may round differently from NumPy's in the last bit."""
+    import torch
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    dev = torch.device(device)
+    z = torch.arange(nz, dtype=torch.float64, device=dev)
+    y = torch.arange(ny, dtype=torch.float64, device=dev)
+    x = torch.arange(nx, dtype=torch.float64, device=dev)
+    logj = torch.zeros(shape, dtype=torch.float64, device=dev)
+    for _ in range(blobs):
+        c = rng.uniform([0, 0, 0], [nz, ny, nx])
+        s = rng.uniform(*sigma)
+        a = rng.uniform(-amplitude, amplitude)
+        ez = torch.exp(-(z - c[0]) ** 2 / (2 * s * s))
+        ey = torch.exp(-(y - c[1]) ** 2 / (2 * s * s))
+        ex = torch.exp(-(x - c[2]) ** 2 / (2 * s * s))
+        logj += a * ez[:, None, None] * (ey[:, None] * ex[None, :])[None]
+    J = torch.clamp(torch.exp(logj), 0.7, 1.4)
+    core = logj.abs() > 0.01
+    mask = core.clone()
+    r = 3
+    for dz in range(-r, r + 1):
+        for dy in range(-r, r + 1):
+            for dx in range(-r, r + 1):
+                if (dz, dy, dx) == (0, 0, 0) or dz * dz + dy * dy + dx * dx > r * r:
+                    continue
+                dst = tuple(slice(max(d, 0), n + min(d, 0)) for d, n in zip((dz, dy, dx), shape))
+                src = tuple(slice(max(-d, 0), n + min(-d, 0)) for d, n in zip((dz, dy, dx), shape))
+                mask[dst] |= core[src]
+    return J, mask
 
 
 def ellipsoid_problem(shape, seed: int = 0, count=None):

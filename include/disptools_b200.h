@@ -243,6 +243,38 @@ int dtb_jacobian_device_noalloc(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, void *J, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Multi-resolution pyramid: smoothing and resampling                  */
+/* ------------------------------------------------------------------ */
+
+enum {
+    DTB_RESAMPLE_LINEAR = 0,
+    DTB_RESAMPLE_NEAREST = 1
+};
+
+/* Gaussian smoothing of `comps` device volumes [comps][nz][ny][nx] (the
+ * anti-aliasing step of scale_image, disptools/drawing.py:62-66, which
+ * smooths by 2.0 physical units: sigma = 2.0 / spacing voxels per axis).
+ * Separable, weights exp(-k^2 / (2 sigma^2)) for |k| <= ceil(4 sigma)
+ * normalised to sum 1, zero-flux border; sigma <= 0 leaves an axis alone,
+ * sigma is at most 32 voxels.  Sums are formed in double.  `in`, `out` and
+ * `scratch` are device arrays of the precision's element type that must not
+ * overlap.  Enqueued on `stream` (a cudaStream_t or NULL). */
+int dtb_smooth_device(int precision, int comps, size_t nx, size_t ny, size_t nz,
+                      double sigma_x, double sigma_y, double sigma_z,
+                      const void *in, void *out, void *scratch, void *stream);
+
+/* Resampling of `comps` device volumes onto an nx2 x ny2 x nz2 grid that
+ * spans the same physical extent (the resampler of scale_image,
+ * disptools/drawing.py:54-68: output spacing s * n / n2, same origin):
+ * output voxel i samples the input at continuous index i * n / n2 per axis;
+ * points outside [-0.5, n - 0.5) on any axis get 0.  DTB_RESAMPLE_LINEAR
+ * interpolates (x, then y, then z, neighbour indices clamped into the
+ * volume), DTB_RESAMPLE_NEAREST takes floor(p + 0.5). */
+int dtb_resample_device(int precision, int mode, int comps, size_t nx, size_t ny, size_t nz,
+                        size_t nx2, size_t ny2, size_t nz2,
+                        const void *in, void *out, void *stream);
+
 /* Tile-shape autotuner of the gradient method.  When on (the default, or
  * DISPTOOLS_B200_AUTOTUNE=0 in the environment at first use for off), the
  * first solve of a problem shape on a device (shape = element type, volume

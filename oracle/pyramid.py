@@ -1,0 +1,156 @@
+"""CPU restatement of the multi-resolution wrapper (test infrastructure).
+
+This file is the checker of the device pyramid: only the tests, the smoke
+check and the benchmark's CPU leg use it.  It restates
+* the reference's ``displacement()`` driver (disptools/displacements.py:238-480),
+* its ``redistribute_volume_change`` (``:224-229``),
+* ``scale_image`` (disptools/drawing.py:23-69),
+on NumPy arrays, with the C oracle (dt_oracle.c) solving each level.
+
+Parity unpinned against the reference itself.  The reference smooths with
+ITK's SmoothingRecursiveGaussian and resamples with ITK's
+ResampleImageFilter, and SimpleITK is not installed here.  The filters below
+are the ones the device kernels implement:
+* a sampled Gaussian of 2.0 physical units, truncated at ceil(4 sigma) and
+  normalised, with zero-flux borders;
+* linear / nearest resampling over the same physical extent with ITK's
+  half-voxel inside rule.
+They are written operation for operation in the kernels' order, so the
+device results can be checked bit for bit.  The driver's steps (padding,
+redistribution, level sizes and spacings, mask reading, per-level it_max,
+initial guess, crop) follow the reference's Python code line by line.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .oracle import Oracle
+
+
+def gaussian_weights(sigma: float):
+    """(radius, weights): exp(-k^2 / (2 sigma^2)) for |k| <= ceil(4 sigma),
+    divided by their sum accumulated in increasing k."""
+    if not sigma > 0.0:
+        return 0, [1.0]
+    r = math.ceil(4.0 * sigma)
+    w = [math.exp(-(k * k) / (2.0 * sigma * sigma)) for k in range(-r, r + 1)]
+    s = 0.0
+    for v in w:
+        s += v
+    return r, [v / s for v in w]
+
+
+def _smooth_axis(v: np.ndarray, axis: int, r: int, w) -> np.ndarray:
+    n = v.shape[axis]
+    acc = np.zeros(v.shape)
+    for k in range(-r, r + 1):
+        idx = np.clip(np.arange(n) + k, 0, n - 1)
+        acc = acc + w[k + r] * np.take(v, idx, axis=axis)
+    return acc
+
+
+def smooth(vol: np.ndarray, sigma_xyz) -> np.ndarray:
+    """Separable Gaussian of a [C, nz, ny, nx] array (x, then y, then z);
+    each pass computes in float64 and rounds to the array's type."""
+    t = vol.dtype
+    v = vol
+    for axis, sigma in zip((3, 2, 1), sigma_xyz):
+        r, w = gaussian_weights(float(sigma))
+        v = _smooth_axis(v.astype(np.float64), axis, r, w).astype(t)
+    return v
+
+
+def _coords(n: int, n2: int):
+    p = (np.arange(n2, dtype=np.float64) * n) / n2
+    inside = (p >= -0.5) & (p < n - 0.5)
+    return p, inside
+
+
+def resample(vol: np.ndarray, size_zyx, nearest: bool = False) -> np.ndarray:
+    """Resampling of a [C, nz, ny, nx] array onto size_zyx voxels over the
+    same physical extent (continuous index i * n / n2; 0 outside
+    [-0.5, n - 0.5); linear along x, then y, then z, or nearest)."""
+    t = vol.dtype
+    v = vol.astype(np.float64)
+    _, nz, ny, nx = v.shape
+    nz2, ny2, nx2 = (int(s) for s in size_zyx)
+    pz, iz = _coords(nz, nz2)
+    py, iy = _coords(ny, ny2)
+    px, ix = _coords(nx, nx2)
+    inside = iz[:, None, None] & iy[None, :, None] & ix[None, None, :]
+    if nearest:
+        zi = np.minimum(np.floor(pz + 0.5).astype(np.int64), nz - 1).clip(0)
+        yi = np.minimum(np.floor(py + 0.5).astype(np.int64), ny - 1).clip(0)
+        xi = np.minimum(np.floor(px + 0.5).astype(np.int64), nx - 1).clip(0)
+        out = v[:, zi][:, :, yi][:, :, :, xi]
+    else:
+        def split(p, n):
+            f0 = np.floor(p)
+            frac = p - f0
+            i0 = np.maximum(f0.astype(np.int64), 0)
+            i1 = np.minimum(f0.astype(np.int64) + 1, n - 1)
+            return i0, i1, frac
+
+        z0, z1, fz = split(pz, nz)
+        y0, y1, fy = split(py, ny)
+        x0, x1, fx = split(px, nx)
+
+        def lerp(a, b, f):
+            return a + (b - a) * f
+
+        def plane(zi, yi):
+            g = v[:, zi][:, :, yi]
+            return lerp(g[..., x0], g[..., x1], fx[None, None, None, :])
+
+        c00, c10 = plane(z0, y0), plane(z0, y1)
+        c01, c11 = plane(z1, y0), plane(z1, y1)
+        fyb = fy[None, None, :, None]
+        c0 = lerp(c00, c10, fyb)
+        c1 = lerp(c01, c11, fyb)
+        out = lerp(c0, c1, fz[None, :, None, None])
+    out = np.where(inside[None], out, 0.0)
+    return out.astype(t)
+
+
+def scale_image(vol: np.ndarray, spacing_xyz, size_zyx, nearest: bool = False) -> np.ndarray:
+    """disptools/drawing.py:23-69: smooth by 2.0 physical units, resample."""
+    sig = [2.0 / float(s) for s in spacing_xyz]
+    return resample(smooth(vol, sig), size_zyx, nearest)
+
+
+def displacement(jacobian, *, levels=1, pad=0, redistribute=False, mask=None, initial_guess=None,
+                 spacing=(1.0, 1.0, 1.0), it_max=50000, algorithm="gradient", field_dtype=np.float64,
+                 **params):
+    """disptools/displacements.py:238-480 on NumPy arrays, each level solved
+    by the C oracle.  ``field_dtype`` float32 rounds the fields passed
+    between levels like the mixed-precision device path."""
+    o = Oracle(4)
+    J = np.array(jacobian, dtype=np.float64)
+    m = np.ones(J.shape) if mask is None else np.asarray(mask, dtype=np.float64)
+    its = list(it_max) if isinstance(it_max, (list, tuple)) else [it_max] * levels
+    p = pad + 1 if pad > 0 else 1                                   # :443-450
+    if redistribute:                                                 # :224-229
+        correction = -(np.sum(J) - J.size) / (J.size - np.count_nonzero(m))
+        J[m == 0.0] += correction
+    m = np.pad(m, p, mode="constant", constant_values=0.0)           # :455
+    J = np.pad(J, p, mode="edge")                                    # :456
+    sizes = [J.shape]                                                # :459-463
+    for _ in range(1, levels):
+        sizes.append(tuple(s // 2 for s in sizes[-1]))
+    n0 = J.shape[::-1]
+    spacings = [tuple(float(sp) * n / k for sp, n, k in zip(spacing, n0, sz[::-1])) for sz in sizes]
+    Js = [J] + [scale_image(J[None], spacings[0], sizes[i])[0] for i in range(1, levels)]
+    ms = [m] + [scale_image(m[None], spacings[0], sizes[i], nearest=True)[0] for i in range(1, levels)]
+    field = None if initial_guess is None else np.asarray(initial_guess, dtype=field_dtype)
+    field_spacing = spacing
+    for lv, it in zip(range(levels - 1, -1, -1), its):              # :476-480
+        if field is not None:
+            field = scale_image(field.astype(field_dtype), field_spacing, sizes[lv])
+        f0 = None if field is None else field.astype(np.float64)
+        out, _ = o.solve(algorithm, np.ascontiguousarray(Js[lv]), np.ascontiguousarray(ms[lv] != 0),
+                         field=f0, spacing=spacings[lv], it_max=it, **params)
+        field = out.astype(field_dtype)
+        field_spacing = spacings[lv]
+    return field[:, p:-p, p:-p, p:-p].astype(np.float64)             # :483

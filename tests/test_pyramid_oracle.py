@@ -1,0 +1,82 @@
+"""The CPU restatement of the pyramid filters (oracle/pyramid.py): basic
+properties that pin it independently of the device kernels."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import pyramid as P
+
+
+def test_gaussian_weights():
+    for sigma in (0.5, 1.0, 2.0, 3.3):
+        r, w = P.gaussian_weights(sigma)
+        assert r == int(np.ceil(4 * sigma)) and len(w) == 2 * r + 1
+        assert abs(sum(w) - 1.0) < 1e-15
+        assert w == w[::-1]
+        assert np.argmax(w) == r
+    assert P.gaussian_weights(0.0) == (0, [1.0])
+
+
+def test_smooth_keeps_constants_and_mass_of_interior_impulse():
+    v = np.full((2, 9, 10, 11), 3.25)
+    np.testing.assert_allclose(P.smooth(v, (1.0, 2.0, 0.5)), v, rtol=1e-15)
+    d = np.zeros((1, 31, 31, 31))
+    d[0, 15, 15, 15] = 1.0
+    s = P.smooth(d, (1.5, 1.0, 2.0))
+    assert abs(s.sum() - 1.0) < 1e-14
+    # separable: the x profile through the centre is the x kernel times the
+    # centre weights of y and z
+    rx, wx = P.gaussian_weights(1.5)
+    _, wy = P.gaussian_weights(1.0)
+    _, wz = P.gaussian_weights(2.0)
+    prof = s[0, 15, 15, 15 - rx:15 + rx + 1]
+    np.testing.assert_allclose(prof, np.array(wx) * wy[len(wy) // 2] * wz[len(wz) // 2], rtol=1e-13)
+
+
+def test_resample_identity_and_linear_ramp():
+    rng = np.random.default_rng(0)
+    v = rng.standard_normal((3, 7, 8, 9))
+    np.testing.assert_array_equal(P.resample(v, (7, 8, 9)), v)
+    np.testing.assert_array_equal(P.resample(v, (7, 8, 9), nearest=True), v)
+    # a linear function is reproduced inside the volume
+    z, y, x = np.meshgrid(np.arange(12.0), np.arange(10.0), np.arange(14.0), indexing="ij")
+    f = (2.0 * x - 0.5 * y + 3.0 * z)[None]
+    g = P.resample(f, (5, 4, 6))
+    pz, py, px = [np.arange(m) * n / m for n, m in ((12, 5), (10, 4), (14, 6))]
+    exact = 2.0 * px[None, None, :] - 0.5 * py[None, :, None] + 3.0 * pz[:, None, None]
+    np.testing.assert_allclose(g[0], exact, atol=1e-12)
+
+
+def test_resample_half_voxel_border():
+    """Upsampling 4 -> 8 samples the last output voxel at index 3.5, which
+    lies on the image border (n - 0.5) and is outside: it gets 0."""
+    v = np.ones((1, 4, 4, 4))
+    u = P.resample(v, (8, 8, 8))
+    assert np.all(u[0, :7, :7, :7] == 1.0)
+    assert np.all(u[0, 7] == 0.0) and np.all(u[0, :, 7] == 0.0) and np.all(u[0, :, :, 7] == 0.0)
+    n = P.resample(v, (8, 8, 8), nearest=True)
+    np.testing.assert_array_equal(n, u)
+
+
+def test_resample_keeps_dtype():
+    v = np.random.default_rng(1).standard_normal((1, 5, 6, 7)).astype(np.float32)
+    assert P.resample(v, (3, 3, 3)).dtype == np.float32
+    assert P.smooth(v, (1.0, 1.0, 1.0)).dtype == np.float32
+
+
+@pytest.mark.parametrize("levels", [1, 2])
+def test_driver_runs_and_crops(levels):
+    from tests.helpers import ball_problem
+    Jt, mask = ball_problem(16, 8, 4, 1.1)
+    out = P.displacement(Jt, mask=mask, levels=levels, it_max=5)
+    assert out.shape == (3, 16, 16, 16)
+    assert np.isfinite(out).all()
+
+
+def test_blob_problem_device_matches_numpy_on_cpu():
+    from disptools_b200.synthetic import blob_problem, blob_problem_device
+    J, m = blob_problem((23, 19, 27), blobs=5, seed=4, sigma=(2.0, 5.0))
+    Jd, md = blob_problem_device((23, 19, 27), blobs=5, seed=4, sigma=(2.0, 5.0), device="cpu")
+    np.testing.assert_allclose(Jd.numpy(), J, rtol=1e-14)
+    np.testing.assert_array_equal(md.numpy(), m)
