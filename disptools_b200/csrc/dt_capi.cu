@@ -336,8 +336,9 @@ struct Engine {
     unsigned char *h_flags = nullptr;
     unsigned char *d_flags = nullptr;
     size_t flags_cap = 0;
-    std::vector<cudaEvent_t> evs;
-    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> evs;      // profiling events: two sets of nk + 1
+    cudaEvent_t ev_done[2] = {nullptr, nullptr};
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // the same steps with either set of events and flags
     GraphKey key;
     int last_cfg[4] = {0, 0, 0, 0};  // tile shapes of the last solve (TileConfig order)
 };
@@ -356,13 +357,17 @@ int engine(Engine **out) {
         DTB_CUDA(cudaEventCreate(&e->ev0));
         DTB_CUDA(cudaEventCreate(&e->ev1));
         DTB_CUDA(cudaEventCreateWithFlags(&e->ev_order, cudaEventDisableTiming));
+        DTB_CUDA(cudaEventCreateWithFlags(&e->ev_done[0], cudaEventDisableTiming));
+        DTB_CUDA(cudaEventCreateWithFlags(&e->ev_done[1], cudaEventDisableTiming));
         g_engines[dev] = e;
     }
     *out = e;
     return DTB_OK;
 }
 
+// Host copies of the states: two sets of `count` (one per replay in flight).
 int ensure_host_states(Engine *e, size_t count) {
+    count *= 2;
     if (e->states_cap >= count) return DTB_OK;
     if (e->h_states) cudaFreeHost(e->h_states);
     e->h_states = nullptr;
@@ -372,17 +377,19 @@ int ensure_host_states(Engine *e, size_t count) {
     return DTB_OK;
 }
 
+// Work flags and events of the profiled step graphs: two sets (one per
+// replay in flight) of nk flags and nk + 1 events.
 int ensure_profiling(Engine *e, size_t nk) {
-    if (e->flags_cap < nk) {
+    if (e->flags_cap < 2 * nk) {
         if (e->h_flags) cudaFreeHost(e->h_flags);
         if (e->d_flags) cudaFree(e->d_flags);
         e->h_flags = e->d_flags = nullptr;
         e->flags_cap = 0;
-        DTB_CUDA(cudaMallocHost(&e->h_flags, nk));
-        DTB_CUDA(cudaMalloc(&e->d_flags, nk));
-        e->flags_cap = nk;
+        DTB_CUDA(cudaMallocHost(&e->h_flags, 2 * nk));
+        DTB_CUDA(cudaMalloc(&e->d_flags, 2 * nk));
+        e->flags_cap = 2 * nk;
     }
-    while (e->evs.size() < nk + 1) {
+    while (e->evs.size() < 2 * (nk + 1)) {
         cudaEvent_t ev;
         DTB_CUDA(cudaEventCreate(&ev));
         e->evs.push_back(ev);
@@ -397,11 +404,12 @@ int ensure_profiling(Engine *e, size_t nk) {
 //   grad_ty   thread rows of the gradient kernel (8: two tile rows per
 //             thread; 16: one)
 //   bz        planes of a tile along z (capped at nz)
+//   pf        L2 prefetch distance in planes beyond each TMA load (0: off)
 // The greedy method runs BX x BY tiles of bz planes.
 struct TileConfig {
-    int tile_x = 32, trial_ty = 16, grad_ty = 8, bz = 32;
+    int tile_x = 32, trial_ty = 16, grad_ty = 8, bz = 32, pf = 0;
     bool operator==(const TileConfig &o) const {
-        return tile_x == o.tile_x && trial_ty == o.trial_ty && grad_ty == o.grad_ty && bz == o.bz;
+        return tile_x == o.tile_x && trial_ty == o.trial_ty && grad_ty == o.grad_ty && bz == o.bz && pf == o.pf;
     }
 };
 
@@ -426,6 +434,16 @@ bool env_config(size_t tsize, TileConfig *c) {
     num("DISPTOOLS_B200_TRIAL_THREADS_Y", &c->trial_ty, {8, 16});
     num("DISPTOOLS_B200_THREADS_Y", &c->grad_ty, {8, 16});
     num("DISPTOOLS_B200_BZ", &c->bz, {});
+    {
+        const char *e = std::getenv("DISPTOOLS_B200_PREFETCH");
+        if (e) {
+            const int v = std::atoi(e);
+            if (v >= 0 && v <= 16) {
+                c->pf = v;
+                any = true;
+            }
+        }
+    }
     if (tsize != 4) c->tile_x = 32;
     if (c->tile_x == 64) c->trial_ty = 16, c->grad_ty = 8;
     return any;
@@ -564,13 +582,20 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
             DTB_CUDA(copy_rows<T>(Jt, g.ys, vols[i].Jt, gu.ys, gu.nx, rows, stream));
             DTB_CUDA(copy_rows<uint8_t>(mask, g.ys, vols[i].mask, gu.ys, gu.nx, rows, stream));
         }
-        // The second field buffer starts at zero: the greedy update never
-        // writes boundary voxels, so they keep the buffer's content
-        // (src/displacement_field_greedy.c:43-65 with calloc'd buffers).
-        DTB_CUDA(cudaMemsetAsync(d.field[1], 0, 3 * N * sizeof(T), stream));
+        // The gradient is zero on the boundary voxels, which the gradient
+        // kernel never writes (src/displacement_field_gradient.c:26-145 on
+        // calloc'd buffers).  For the greedy method the second field buffer
+        // and the error maps start at zero as well: its update never writes
+        // boundary voxels, so they keep the buffer's content
+        // (src/displacement_field_greedy.c:43-65).  The gradient method's
+        // trial writes every voxel of the candidate and of e' before they
+        // are read.
         DTB_CUDA(cudaMemsetAsync(d.grad, 0, 3 * N * sizeof(T), stream));
-        DTB_CUDA(cudaMemsetAsync(aux0, 0, N * sizeof(T), stream));
-        DTB_CUDA(cudaMemsetAsync(aux1, 0, N * sizeof(T), stream));
+        if (!gradient) {
+            DTB_CUDA(cudaMemsetAsync(d.field[1], 0, 3 * N * sizeof(T), stream));
+            DTB_CUDA(cudaMemsetAsync(aux0, 0, N * sizeof(T), stream));
+            DTB_CUDA(cudaMemsetAsync(aux1, 0, N * sizeof(T), stream));
+        }
 
         if (gradient) {
             CUtensorMap h_maps[7];
@@ -617,12 +642,12 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms());
     auto launch_t = [&](unsigned char *flag) -> cudaError_t {
         if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, trial_ty,
-                                                    d_queues);
+                                                    d_queues, cfg.pf);
         return launch_trial<T>(MODE_GREEDY, d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
     };
     auto launch_g = [&](unsigned char *flag) -> cudaError_t {
         return launch_gradient_tma<T>(d_desc, d_tile_vol, total_tiles, grid_g, stream, flag, tile_x, threads_y,
-                                      d_queues + 1);
+                                      d_queues + 1, cfg.pf);
     };
 
     cudaEvent_t ev0 = e->ev0, ev1 = e->ev1;
@@ -672,72 +697,88 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     key.grid_t = grid_t;
     key.grid_g = grid_g;
     key.K = K;
-    key.threads_y = (trial_ty * 100 + threads_y) * 1000 + tile_x;
+    key.threads_y = ((trial_ty * 100 + threads_y) * 1000 + tile_x) * 100 + cfg.pf;
     key.flags = d_flags;
-    if (!(e->exec && e->key == key)) {
-        if (e->exec) cudaGraphExecDestroy(e->exec);
-        e->exec = nullptr;
-        cudaGraph_t graph = nullptr;
-        set_capturing(true);
-        DTB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        // Inside a capture only cudaEventRecordExternal turns a record into an
-        // event-record node that fires on every replay.
-        if (prof) {
-            cudaMemsetAsync(d_flags, 0, nk, stream);
-            cudaEventRecordWithFlags(evs[0], stream, cudaEventRecordExternal);
+    // Two graphs of the same K steps, each with its own set of profiling
+    // events and work flags, so that one replay can be queued while the
+    // host reads the results of the other.
+    if (!(e->exec[0] && e->exec[1] && e->key == key)) {
+        for (cudaGraphExec_t &x : e->exec) {
+            if (x) cudaGraphExecDestroy(x);
+            x = nullptr;
         }
-        for (int k = 0, j = 0; k < K; ++k) {
-            if (gradient) {
-                launch_g(prof ? d_flags + j : nullptr);
-                if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
+        for (int b = 0; b < 2; ++b) {
+            cudaEvent_t *ev = prof ? &evs[b * (nk + 1)] : nullptr;
+            unsigned char *fl = prof ? d_flags + b * nk : nullptr;
+            cudaGraph_t graph = nullptr;
+            set_capturing(true);
+            DTB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            // Inside a capture only cudaEventRecordExternal turns a record
+            // into an event-record node that fires on every replay.
+            if (prof) {
+                cudaMemsetAsync(fl, 0, nk, stream);
+                cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
+            }
+            for (int k = 0, j = 0; k < K; ++k) {
+                if (gradient) {
+                    launch_g(prof ? fl + j : nullptr);
+                    if (prof) cudaEventRecordWithFlags(ev[j + 1], stream, cudaEventRecordExternal);
+                    ++j;
+                }
+                launch_t(prof ? fl + j : nullptr);
+                if (prof) cudaEventRecordWithFlags(ev[j + 1], stream, cudaEventRecordExternal);
                 ++j;
             }
-            launch_t(prof ? d_flags + j : nullptr);
-            if (prof) cudaEventRecordWithFlags(evs[j + 1], stream, cudaEventRecordExternal);
-            ++j;
+            cudaError_t cap = cudaStreamEndCapture(stream, &graph);
+            set_capturing(false);
+            if (cap != cudaSuccess) {
+                cudaGetLastError();
+                DTB_CUDA(cap);
+            }
+            cudaError_t inst = cudaGraphInstantiate(&e->exec[b], graph, 0);
+            cudaGraphDestroy(graph);
+            DTB_CUDA(inst);
         }
-        cudaError_t cap = cudaStreamEndCapture(stream, &graph);
-        set_capturing(false);
-        if (cap != cudaSuccess) {
-            cudaGetLastError();
-            DTB_CUDA(cap);
-        }
-        cudaError_t inst = cudaGraphInstantiate(&e->exec, graph, 0);
-        cudaGraphDestroy(graph);
-        DTB_CUDA(inst);
         e->key = key;
     }
-    cudaGraphExec_t exec = e->exec;
 
-    // Host copy of the states, refreshed once per graph launch.
+    // Replays alternate between the two graphs; replay r copies the states
+    // (and flags) into host set r % 2 and records ev_done[r % 2].  The host
+    // queues replay r + 1 before it waits for replay r, so the device never
+    // idles while the host checks.  Kernels of a finished volume return at
+    // once, so the one replay queued after the last useful one costs only
+    // its launches.
     rc = ensure_host_states(e, count);
     if (rc != DTB_OK) return rc;
-    SolverState *h_states = e->h_states;
     long long max_steps = 0;
     for (int i = 0; i < count; ++i) max_steps = std::max(max_steps, 64 * (p.it_max + 2) + 4096);
     long long steps = 0;
     int status = DTB_OK;
     cudaError_t loop_err = cudaSuccess;
-    for (;;) {
-        if ((loop_err = cudaGraphLaunch(exec, stream)) != cudaSuccess) {
-            status = DTB_ERR_CUDA;
-            break;
-        }
+    auto enqueue = [&](long long r) -> cudaError_t {
+        const int b = (int) (r & 1);
+        cudaError_t err = cudaGraphLaunch(e->exec[b], stream);
+        if (err != cudaSuccess) return err;
         count_launch(nk);
         steps += K;
+        SolverState *hs = e->h_states + (size_t) b * count;
         for (int i = 0; i < count; ++i)
-            cudaMemcpyAsync(&h_states[i], d_states[i], sizeof(SolverState), cudaMemcpyDeviceToHost, stream);
-        if (prof) cudaMemcpyAsync(h_flags, d_flags, nk, cudaMemcpyDeviceToHost, stream);
-        if ((loop_err = cudaStreamSynchronize(stream)) != cudaSuccess) {
-            status = DTB_ERR_CUDA;
-            break;
-        }
+            cudaMemcpyAsync(&hs[i], d_states[i], sizeof(SolverState), cudaMemcpyDeviceToHost, stream);
+        if (prof) cudaMemcpyAsync(h_flags + b * nk, d_flags + b * nk, nk, cudaMemcpyDeviceToHost, stream);
+        return cudaEventRecord(e->ev_done[b], stream);
+    };
+    // Waits for replay r, adds its profile; true when every volume is done.
+    auto finish = [&](long long r, bool *all_done) -> cudaError_t {
+        const int b = (int) (r & 1);
+        cudaError_t err = cudaEventSynchronize(e->ev_done[b]);
+        if (err != cudaSuccess) return err;
         if (prof) {
             std::lock_guard<std::mutex> lock(g_prof_mutex);
+            const cudaEvent_t *ev = &evs[b * (nk + 1)];
             for (int j = 0; j < nk; ++j) {
-                if (!h_flags[j]) continue;
+                if (!h_flags[b * nk + j]) continue;
                 float ms = 0.f;
-                if (cudaEventElapsedTime(&ms, evs[j], evs[j + 1]) != cudaSuccess) {
+                if (cudaEventElapsedTime(&ms, ev[j], ev[j + 1]) != cudaSuccess) {
                     cudaGetLastError();
                     continue;
                 }
@@ -746,14 +787,37 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
                 g_prof.ms[kind] += ms;
             }
         }
-        bool all_done = true;
-        for (int i = 0; i < count; ++i) all_done &= h_states[i].done != 0;
+        const SolverState *hs = e->h_states + (size_t) b * count;
+        bool done = true;
+        for (int i = 0; i < count; ++i) done &= hs[i].done != 0;
+        *all_done = done;
+        return cudaSuccess;
+    };
+    long long r = 0;
+    if ((loop_err = enqueue(0)) != cudaSuccess) status = DTB_ERR_CUDA;
+    while (status == DTB_OK) {
+        if ((loop_err = enqueue(r + 1)) != cudaSuccess) {
+            status = DTB_ERR_CUDA;
+            break;
+        }
+        bool all_done = false;
+        if ((loop_err = finish(r, &all_done)) != cudaSuccess) {
+            status = DTB_ERR_CUDA;
+            break;
+        }
+        ++r;
         if (all_done) break;
         if (steps > max_steps) {
             status = DTB_ERR_ARGUMENT;
             break;
         }
     }
+    // The replay queued last (r): wait for it so its states and profile are read.
+    if (status == DTB_OK) {
+        bool all_done = false;
+        if ((loop_err = finish(r, &all_done)) != cudaSuccess) status = DTB_ERR_CUDA;
+    }
+    const SolverState *h_states = e->h_states + (size_t) (r & 1) * count;
     const cudaError_t rec_err = cudaEventRecord(ev1, stream);
     if (status == DTB_OK && rec_err != cudaSuccess) {
         status = DTB_ERR_CUDA;
@@ -1215,9 +1279,11 @@ extern "C" int dtb_release_device_memory(void) {
         }
     }
     // The cached step graph points into the freed workspace.
-    if ((int) g_engines.size() > dev && g_engines[dev] && g_engines[dev]->exec) {
-        cudaGraphExecDestroy(g_engines[dev]->exec);
-        g_engines[dev]->exec = nullptr;
+    if ((int) g_engines.size() > dev && g_engines[dev]) {
+        for (cudaGraphExec_t &x : g_engines[dev]->exec) {
+            if (x) cudaGraphExecDestroy(x);
+            x = nullptr;
+        }
         g_engines[dev]->key = GraphKey{};
     }
     cudaGetLastError();

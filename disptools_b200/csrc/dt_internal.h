@@ -116,14 +116,16 @@ template <typename T>
 cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
                             int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
 // TMA kernels of the gradient method; tiles are tile_x (64 or 32) by TT_Y
-// voxels, blocks tile_x by threads_y (8 or 16) threads.
+// voxels; threads_y rows of threads (8 or 16).  `pf` > 0 prefetches into L2
+// the boxes of the plane pf iterations ahead of each load.
 template <typename T>
 cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *queue);
+                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *queue,
+                             int pf);
 template <typename T>
 cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                 cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y,
-                                TileQueue *queue);
+                                TileQueue *queue, int pf);
 template <typename T>
 int trial_tma_blocks_per_sm(int tile_x, int threads_y);
 template <typename T>

@@ -149,7 +149,7 @@ __device__ __forceinline__ void st_pair(T *p, T a, T b) {
 template <typename T, int TXW, int TYT>
 __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof(T) == 4) ? 2 : 1)
     k_trial_tma(const VolumeDesc<T> *__restrict__ vols, const int *__restrict__ tile_vol, int total_tiles,
-                unsigned char *__restrict__ work_flag, TileQueue *queue) {
+                unsigned char *__restrict__ work_flag, TileQueue *queue, int pf) {
     using L = TrialTmaLayout<T, TXW>;
     constexpr int TPX = TXW / 2, NTH = TPX * TYT, RYT = TT_Y / TYT;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
@@ -212,6 +212,16 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             if (with_target) {
                 tma_load_3d(sb + 2 * L::U_BYTES, V.tm_Jt, &bars[s], x0, y0, ze);
                 tma_load_3d(sb + 2 * L::U_BYTES + L::JT_BYTES, V.tm_mask, &bars[s], x0, y0, ze);
+            }
+            // Warm L2 with the boxes of iteration j + pf.
+            if (pf > 0 && j + pf < n_it) {
+                const int qp = q + pf, zp = qp - 2;
+                tma_prefetch_4d(tm_u, x0 - TMA_HX, y0 - TMA_HY, qp, 0);
+                if (trial) tma_prefetch_4d(tm_g, x0 - TMA_HX, y0 - TMA_HY, qp, 0);
+                if (zp >= z0 && zp < z1) {
+                    tma_prefetch_3d(V.tm_Jt, x0, y0, zp);
+                    tma_prefetch_3d(V.tm_mask, x0, y0, zp);
+                }
             }
         };
 
@@ -477,7 +487,8 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
 template <typename T, int TXW, int TYT>
 __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 ? 2 : 1) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
                                                      const int *__restrict__ tile_vol, int total_tiles,
-                                                     unsigned char *__restrict__ work_flag, TileQueue *queue) {
+                                                     unsigned char *__restrict__ work_flag, TileQueue *queue,
+                                                     int pf) {
     using L = GradTmaLayout<T, TXW>;
     constexpr int NTH = TXW * TYT, RYT = TT_Y / TYT;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
@@ -530,6 +541,11 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
             mbar_arrive_expect_tx(&bars[s], L::U_BYTES + L::E_BYTES);
             tma_load_4d(sb, tm_u, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
             tma_load_3d(sb + L::U_BYTES, tm_e, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q);
+            // Warm L2 with the boxes of iteration j + pf.
+            if (pf > 0 && j + pf < n_it) {
+                tma_prefetch_4d(tm_u, x0 - TMA_HX, y0 - TMA_HY, q + pf, 0);
+                tma_prefetch_3d(tm_e, x0 - TMA_HX, y0 - TMA_HY, q + pf);
+            }
         };
         if (tid == 0) {
             tmap_acquire(tm_u);
@@ -688,24 +704,26 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
 
 template <typename T, int TXW, int TYT>
 cudaError_t launch_trial_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                               cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
+                               cudaStream_t s, unsigned char *work_flag, TileQueue *queue, int pf) {
     constexpr int smem = TrialTmaLayout<T, TXW>::BYTES + 128;
     static const cudaError_t attr =
         cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
-    k_trial_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
+    k_trial_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue,
+                                                                     pf);
     count_launch();
     return cudaGetLastError();
 }
 
 template <typename T, int TXW, int TYT>
 cudaError_t launch_gradient_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                                  cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
+                                  cudaStream_t s, unsigned char *work_flag, TileQueue *queue, int pf) {
     constexpr int smem = GradTmaLayout<T, TXW>::BYTES + 128;
     static const cudaError_t attr =
         cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
-    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
+    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue,
+                                                                   pf);
     count_launch();
     return cudaGetLastError();
 }
@@ -746,21 +764,25 @@ int gradient_blocks_v() {
 //   tile_x 64, threads_y 8   FP32 only, 512 threads
 template <typename T>
 cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
+                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q,
+                             int pf) {
     if constexpr (sizeof(T) == 4)
-        if (tile_x == 64) return launch_trial_tma_v<T, 64, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
-    if (threads_y == 8) return launch_trial_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
-    return launch_trial_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+        if (tile_x == 64)
+            return launch_trial_tma_v<T, 64, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
+    if (threads_y == 8) return launch_trial_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
+    return launch_trial_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
 }
 
 template <typename T>
 cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                                cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
+                                cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q,
+                                int pf) {
     if constexpr (sizeof(T) == 4)
-        if (tile_x == 64) return launch_gradient_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+        if (tile_x == 64)
+            return launch_gradient_tma_v<T, 64, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
     if (threads_y == 16)
-        return launch_gradient_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
-    return launch_gradient_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+        return launch_gradient_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
+    return launch_gradient_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
 }
 
 template <typename T>
@@ -778,9 +800,9 @@ int gradient_tma_blocks_per_sm(int tile_x, int threads_y) {
 
 #define DTB_INSTANTIATE_TMA(T)                                                                              \
     template cudaError_t launch_trial_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
-                                             unsigned char *, int, int, TileQueue *);                       \
+                                             unsigned char *, int, int, TileQueue *, int);                  \
     template cudaError_t launch_gradient_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t, \
-                                                unsigned char *, int, int, TileQueue *);                    \
+                                                unsigned char *, int, int, TileQueue *, int);               \
     template int trial_tma_blocks_per_sm<T>(int, int);                                                      \
     template int gradient_tma_blocks_per_sm<T>(int, int);
 

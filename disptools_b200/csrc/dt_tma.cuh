@@ -80,4 +80,18 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// L2 prefetch of a tiled box (no shared memory, no completion to track):
+// warms L2 for a load issued later.  Same coordinate rules as the loads.
+__device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int x, int y, int z) {
+    asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(map), "r"(x), "r"(y),
+                 "r"(z)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_4d(const CUtensorMap *map, int x, int y, int z, int c) {
+    asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(map), "r"(x),
+                 "r"(y), "r"(z), "r"(c)
+                 : "memory");
+}
+
 }  // namespace dtb
