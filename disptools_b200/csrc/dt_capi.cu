@@ -401,13 +401,13 @@ int ensure_profiling(Engine *e, size_t nk) {
 //   tile_x    tile width in voxels (32, or 64 for FP32); tiles are TT_Y high
 //   trial_ty  thread rows of the trial kernel (16: one tile row and two
 //             columns per thread; 8: two rows)
-//   grad_ty   thread rows of the gradient kernel (8: two tile rows per
-//             thread; 16: one)
+//   grad_ty   thread rows of the gradient kernel (16: one tile row and two
+//             columns per thread; 8: two rows)
 //   bz        planes of a tile along z (capped at nz)
 //   pf        L2 prefetch distance in planes beyond each TMA load (0: off)
 // The greedy method runs BX x BY tiles of bz planes.
 struct TileConfig {
-    int tile_x = 32, trial_ty = 16, grad_ty = 8, bz = 32, pf = 0;
+    int tile_x = 32, trial_ty = 16, grad_ty = 16, bz = 32, pf = 0;
     bool operator==(const TileConfig &o) const {
         return tile_x == o.tile_x && trial_ty == o.trial_ty && grad_ty == o.grad_ty && bz == o.bz && pf == o.pf;
     }
@@ -891,8 +891,8 @@ bool autotune_enabled() {
 
 // Candidate shapes, the fixed default first.
 std::vector<TileConfig> tile_candidates(size_t tsize) {
-    std::vector<TileConfig> c = {{32, 16, 8, 32}, {32, 16, 16, 32}, {32, 16, 8, 16}, {32, 16, 8, 64},
-                                 {32, 8, 8, 32}};
+    std::vector<TileConfig> c = {{32, 16, 16, 32}, {32, 16, 8, 32}, {32, 16, 16, 16}, {32, 16, 16, 64},
+                                 {32, 8, 16, 32}};
     if (tsize == 4) c.push_back({64, 16, 8, 32});
     return c;
 }

@@ -62,7 +62,7 @@ struct GradTmaLayout {
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
     static constexpr int E_BYTES = TMA_PLANE * (int) sizeof(T);
     static constexpr int STAGE_BYTES = U_BYTES + E_BYTES;
-    static constexpr int PXP = TXW + 2, PYP = TT_Y + 2;
+    static constexpr int PXP = TXW + 4, PYP = TT_Y + 2;  // P terms: tile + 1 each side, pair-aligned columns
     static constexpr int NP = 3;  // planes of P_x, P_y terms (one barrier per plane)
     static constexpr int P_OFF = S * STAGE_BYTES;  // P_x, P_y terms: [NP][6][PYP][PXP]
     static constexpr int P_BYTES = NP * 6 * PYP * PXP * (int) sizeof(T);
@@ -484,28 +484,33 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     }
 }
 
+// Block of TXW / 2 x TYT threads; each thread owns two adjacent columns
+// (x, x + 1) of TT_Y / TYT rows of the tile, so the field, e' and P-term
+// reads and the gradient stores are pairs.  Two resident blocks per SM for
+// FP32 (shared memory allows no more), one for FP64.
 template <typename T, int TXW, int TYT>
-__global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 ? 2 : 1) k_gradient_tma(const VolumeDesc<T> *__restrict__ vols,
-                                                     const int *__restrict__ tile_vol, int total_tiles,
-                                                     unsigned char *__restrict__ work_flag, TileQueue *queue,
-                                                     int pf) {
+__global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof(T) == 4) ? 2 : 1)
+    k_gradient_tma(const VolumeDesc<T> *__restrict__ vols, const int *__restrict__ tile_vol, int total_tiles,
+                   unsigned char *__restrict__ work_flag, TileQueue *queue, int pf) {
     using L = GradTmaLayout<T, TXW>;
-    constexpr int NTH = TXW * TYT, RYT = TT_Y / TYT;
+    constexpr int TPX = TXW / 2, NTH = TPX * TYT, RYT = TT_Y / TYT;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
     constexpr int PXP = L::PXP, PYP = L::PYP;
+    constexpr int NHALO = 2 * TT_Y + TXW;  // halo threads: x sides (one cell each), y sides (two cells each)
+    static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
+    static_assert(NHALO <= NTH, "halo threads");
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char *smem = align_smem_128(smem_dyn);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     T *pxy = reinterpret_cast<T *>(smem + L::P_OFF);
     __shared__ double red[2 * (NTH / 32)];
     __shared__ int s_flag, s_fault;
-    // P terms of the x (t = 0..2) and y (t = 3..5) directions, cell (ly, lx)
-    // of the tile plus a halo of one.
-    auto PT = [&](int slot, int t, int ly, int lx) -> T & {
-        return pxy[((slot * 6 + t) * PYP + ly) * PXP + lx];
-    };
+    // P terms of the x (t = 0..2) and y (t = 3..5) directions.  P column c
+    // holds x = x0 + c - 2 (so the own pairs start at even columns), P row r
+    // holds y = y0 + r - 1.
+    auto PT = [&](int slot, int t, int r, int c) -> T * { return pxy + ((slot * 6 + t) * PYP + r) * PXP + c; };
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TXW + tx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -515,8 +520,8 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
     uint32_t kbase = 0;
 
     __shared__ int s_tile;
-    for (int tile = take_tile<TXW>(queue, total_tiles, &s_tile); tile >= 0;
-         tile = take_tile<TXW>(queue, total_tiles, &s_tile)) {
+    for (int tile = take_tile<TPX>(queue, total_tiles, &s_tile); tile >= 0;
+         tile = take_tile<TPX>(queue, total_tiles, &s_tile)) {
         const VolumeDesc<T> &V = vols[tile_vol[tile]];
         SolverState *st = V.st;
         if (ldcg_int(&st->done) || !ldcg_int(&st->need_gradient)) continue;
@@ -529,7 +534,7 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
         const int n_it = z1 - z0 + 4;  // u planes z0-2 .. z1+1
         const CUtensorMap *tm_u = V.tm_field[old_b];
         const CUtensorMap *tm_e = V.tm_ep[old_b];
-        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+        const T ihx = (T) g.ih[0], ihy = (T) g.ih[1], ihz = (T) g.ih[2];
 
         int issued_n = 0;
         auto issue = [&](int j) {
@@ -559,16 +564,22 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
             return reinterpret_cast<const T *>(smem + ((kbase + j) % L::S) * L::STAGE_BYTES + L::U_BYTES);
         };
 
-        const int x = x0 + tx;
-        T pz_m2[RYT][3], pz_m1[RYT][3];
+        const int x = x0 + 2 * tx;       // this thread's columns: x, x + 1
+        const int lx = 2 * tx + TMA_HX;  // their box column
+        const int cp = 2 * tx + 2;       // their P column
+        // P_z terms of the own cells: planes p-2, p-1 and the one computed now.
+        T pz_m2[RYT][2][3], pz_m1[RYT][2][3];
 #pragma unroll
         for (int r = 0; r < RYT; ++r)
 #pragma unroll
-            for (int i = 0; i < 3; ++i) pz_m2[r][i] = pz_m1[r][i] = T(0);
+            for (int v = 0; v < 2; ++v)
+#pragma unroll
+                for (int i = 0; i < 3; ++i) pz_m2[r][v][i] = pz_m1[r][v][i] = T(0);
         double acc = 0.0;
         bool failed = false;
         int fail_it = 0;
-        for (int it = 0; it < n_it; ++it) {
+        long long zoff = (long long) (z0 - 4) * g.zs;  // offset of gradient plane z = q - 2
+        for (int it = 0; it < n_it; ++it, zoff += g.zs) {
             const uint32_t k = kbase + it;
             const int s = k % L::S;
             const uint32_t par = (k / L::S) & 1u;
@@ -576,64 +587,89 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
             if (!ok) s_fault = 1;
             const int q = z0 - 2 + it;
             const int p = q - 1;  // plane of P computed now (needs u(q-2..q), e'(q-1))
-            T pz_new[RYT][3];
+            T pz_new[RYT][2][3];
 #pragma unroll
             for (int r = 0; r < RYT; ++r)
 #pragma unroll
-                for (int i = 0; i < 3; ++i) pz_new[r][i] = T(0);
+                for (int v = 0; v < 2; ++v)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) pz_new[r][v][i] = T(0);
             if (it >= 2 && ok) {
                 const T *um = stage_u(it - 2), *u0 = stage_u(it - 1), *up = stage_u(it);
                 const T *e0 = stage_e(it - 1);
                 const int ps = ring_slot(p, L::NP);
-                // M = I + grad u at box cell (lx, ly) of plane p, second order central.
-                auto mat = [&](int lx, int ly, T m[3][3]) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const int o = c * TMA_PLANE + ly * TMA_PX + lx;
-                        m[c][0] = fd_c2<T>(u0[o + 1], u0[o - 1], ih[0]);
-                        m[c][1] = fd_c2<T>(u0[o + TMA_PX], u0[o - TMA_PX], ih[1]);
-                        m[c][2] = fd_c2<T>(up[o], um[o], ih[2]);
-                        m[c][c] += T(1.0);
-                    }
-                };
                 auto minor = [](const T m[3][3], int i, int kk) -> T {
                     const int r0 = i == 0 ? 1 : 0, r1 = i == 2 ? 1 : 2;
                     const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
                     return m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
                 };
+                // M = I + grad u (second-order central) at box cell (cx, cy).
+                auto mat = [&](int cx, int cy, T m[3][3]) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int o = c * TMA_PLANE + cy * TMA_PX + cx;
+                        m[c][0] = fd_c2<T>(u0[o + 1], u0[o - 1], ihx);
+                        m[c][1] = fd_c2<T>(u0[o + TMA_PX], u0[o - TMA_PX], ihy);
+                        m[c][2] = fd_c2<T>(up[o], um[o], ihz);
+                        m[c][c] += T(1.0);
+                    }
+                };
+                // The same for the pair of box cells (cx, cy), (cx + 1, cy); cx even.
+                auto mat_pair = [&](int cx, int cy, T m0[3][3], T m1[3][3]) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const int o = c * TMA_PLANE + cy * TMA_PX + cx;
+                        const auto xm = ld_pair(u0 + o - 2), xc = ld_pair(u0 + o), xp = ld_pair(u0 + o + 2);
+                        const auto ym = ld_pair(u0 + o - TMA_PX), yp = ld_pair(u0 + o + TMA_PX);
+                        const auto zm = ld_pair(um + o), zp = ld_pair(up + o);
+                        m0[c][0] = fd_c2<T>(xc.y, xm.y, ihx);
+                        m1[c][0] = fd_c2<T>(xp.x, xc.x, ihx);
+                        m0[c][1] = fd_c2<T>(yp.x, ym.x, ihy);
+                        m1[c][1] = fd_c2<T>(yp.y, ym.y, ihy);
+                        m0[c][2] = fd_c2<T>(zp.x, zm.x, ihz);
+                        m1[c][2] = fd_c2<T>(zp.y, zm.y, ihz);
+                        m0[c][c] += T(1.0);
+                        m1[c][c] += T(1.0);
+                    }
+                };
 #pragma unroll
                 for (int r = 0; r < RYT; ++r) {  // own cells: all nine terms (P_z in registers)
-                    const int lx = tx + TMA_HX, ly = ty + r * TYT + TMA_HY;
-                    T m[3][3];
-                    mat(lx, ly, m);
-                    const T ep = e0[ly * TMA_PX + lx];
+                    const int ly = ty + r * TYT + TMA_HY, rp = ty + r * TYT + 1;
+                    T m0[3][3], m1[3][3];
+                    mat_pair(lx, ly, m0, m1);
+                    const auto ep = ld_pair(e0 + ly * TMA_PX + lx);
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        PT(ps, i, ty + r * TYT + 1, tx + 1) = ep * minor(m, i, 0);
-                        PT(ps, 3 + i, ty + r * TYT + 1, tx + 1) = ep * minor(m, i, 1);
-                        pz_new[r][i] = ep * minor(m, i, 2);
+                        st_pair(PT(ps, i, rp, cp), ep.x * minor(m0, i, 0), ep.y * minor(m1, i, 0));
+                        st_pair(PT(ps, 3 + i, rp, cp), ep.x * minor(m0, i, 1), ep.y * minor(m1, i, 1));
+                        pz_new[r][0][i] = ep.x * minor(m0, i, 2);
+                        pz_new[r][1][i] = ep.y * minor(m1, i, 2);
                     }
                 }
-                // halo cells: P_x on the two side columns, P_y on the two end rows
-                if (tid < 2 * TT_Y) {
-                    const int side = tid / TT_Y, row = tid % TT_Y;
-                    const int lx1 = side ? TXW + 1 : 0;
-                    const int lx = lx1 - 1 + TMA_HX, ly = row + TMA_HY;
+                // Halo cells, on the last threads of the block (thread 0
+                // issues the loads): P_x on the two side columns, P_y on the
+                // two end rows (pairs).
+                const int h = tid - (NTH - NHALO);
+                if (h >= 0 && h < 2 * TT_Y) {
+                    const int side = h / TT_Y, row = h % TT_Y;
+                    const int c = side ? TXW + 2 : 1;
+                    const int cx = c - 2 + TMA_HX, cy = row + TMA_HY;
                     T m[3][3];
-                    mat(lx, ly, m);
-                    const T ep = e0[ly * TMA_PX + lx];
+                    mat(cx, cy, m);
+                    const T ep = e0[cy * TMA_PX + cx];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) PT(ps, i, row + 1, lx1) = ep * minor(m, i, 0);
-                } else if (tid < 2 * TT_Y + 2 * TXW) {
-                    const int t2 = tid - 2 * TT_Y;
-                    const int side = t2 / TXW, col = t2 % TXW;
-                    const int ly1 = side ? TT_Y + 1 : 0;
-                    const int lx = col + TMA_HX, ly = ly1 - 1 + TMA_HY;
-                    T m[3][3];
-                    mat(lx, ly, m);
-                    const T ep = e0[ly * TMA_PX + lx];
+                    for (int i = 0; i < 3; ++i) *PT(ps, i, row + 1, c) = ep * minor(m, i, 0);
+                } else if (h >= 2 * TT_Y) {
+                    const int h2 = h - 2 * TT_Y;
+                    const int side = h2 / TPX, col = 2 * (h2 % TPX);
+                    const int r = side ? TT_Y + 1 : 0;
+                    const int cx = col + TMA_HX, cy = r - 1 + TMA_HY;
+                    T m0[3][3], m1[3][3];
+                    mat_pair(cx, cy, m0, m1);
+                    const auto ep = ld_pair(e0 + cy * TMA_PX + cx);
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) PT(ps, 3 + i, ly1, col + 1) = ep * minor(m, i, 1);
+                    for (int i = 0; i < 3; ++i)
+                        st_pair(PT(ps, 3 + i, r, col + 2), ep.x * minor(m0, i, 1), ep.y * minor(m1, i, 1));
                 }
             }
             __syncthreads();
@@ -644,37 +680,61 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
             }
             if (tid == 0 && it >= 2 && it - 2 + L::S < n_it) issue(it - 2 + L::S);
             const int z = q - 2;  // gradient plane: P(z-1), P(z), P(z+1) ready
-            if (it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x >= 1 && x < g.nx - 1) {
+            if (it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x < g.nx - 1 && x + 1 >= 1) {
                 const int ps = ring_slot(z, L::NP);
+                const bool in0 = x >= 1, in1 = x + 1 < g.nx - 1;
 #pragma unroll
                 for (int r = 0; r < RYT; ++r) {
                     const int y = y0 + ty + r * TYT;
                     if (y < 1 || y >= g.ny - 1) continue;
-                    const int lx = tx + 1, ly = ty + r * TYT + 1;
-                    T t[3][3];
+                    const int rp = ty + r * TYT + 1;
+                    T gv[2][3];
+                    T t[2][3][3];
 #pragma unroll
                     for (int i = 0; i < 3; ++i) {
-                        t[i][0] = ih[0] * (PT(ps, i, ly, lx - 1) - PT(ps, i, ly, lx + 1));
-                        t[i][1] = ih[1] * (PT(ps, 3 + i, ly - 1, lx) - PT(ps, 3 + i, ly + 1, lx));
-                        t[i][2] = ih[2] * (pz_m2[r][i] - pz_new[r][i]);
+                        const auto a = ld_pair(PT(ps, i, rp, cp - 2)), b = ld_pair(PT(ps, i, rp, cp)),
+                                   c = ld_pair(PT(ps, i, rp, cp + 2));
+                        t[0][i][0] = ihx * (a.y - b.y);
+                        t[1][i][0] = ihx * (b.x - c.x);
+                        const auto ym = ld_pair(PT(ps, 3 + i, rp - 1, cp)), yp = ld_pair(PT(ps, 3 + i, rp + 1, cp));
+                        t[0][i][1] = ihy * (ym.x - yp.x);
+                        t[1][i][1] = ihy * (ym.y - yp.y);
+                        t[0][i][2] = ihz * (pz_m2[r][0][i] - pz_new[r][0][i]);
+                        t[1][i][2] = ihz * (pz_m2[r][1][i] - pz_new[r][1][i]);
                     }
-                    const T gx = t[0][0] - t[0][1] + t[0][2];
-                    const T gy = -t[1][0] + t[1][1] - t[1][2];
-                    const T gz = t[2][0] - t[2][1] + t[2][2];
-                    const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
-                    V.grad[so] = gx;
-                    V.grad[g.cs + so] = gy;
-                    V.grad[2 * g.cs + so] = gz;
-                    acc += (double) (gx * gx + gy * gy + gz * gz);
+#pragma unroll
+                    for (int v = 0; v < 2; ++v) {
+                        gv[v][0] = t[v][0][0] - t[v][0][1] + t[v][0][2];
+                        gv[v][1] = -t[v][1][0] + t[v][1][1] - t[v][1][2];
+                        gv[v][2] = t[v][2][0] - t[v][2][1] + t[v][2][2];
+                    }
+                    T *o = V.grad + zoff + (long long) y * g.ys + x;
+                    if (in0 && in1) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, gv[0][c], gv[1][c]);
+                        acc += (double) (gv[0][0] * gv[0][0] + gv[0][1] * gv[0][1] + gv[0][2] * gv[0][2]);
+                        acc += (double) (gv[1][0] * gv[1][0] + gv[1][1] * gv[1][1] + gv[1][2] * gv[1][2]);
+                    } else {
+                        // one voxel of the pair is on the boundary (x = 0 or nx - 1)
+                        T w[3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            w[c] = in0 ? gv[0][c] : gv[1][c];
+                            o[(in0 ? 0 : 1) + c * g.cs] = w[c];
+                        }
+                        acc += (double) (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+                    }
                 }
             }
 #pragma unroll
             for (int r = 0; r < RYT; ++r)
 #pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    pz_m2[r][i] = pz_m1[r][i];
-                    pz_m1[r][i] = pz_new[r][i];
-                }
+                for (int v = 0; v < 2; ++v)
+#pragma unroll
+                    for (int i = 0; i < 3; ++i) {
+                        pz_m2[r][v][i] = pz_m1[r][v][i];
+                        pz_m1[r][v][i] = pz_new[r][v][i];
+                    }
         }
         if (failed) {
             if (tid == 0) tma_fault<L::S>(st, bars, kbase, fail_it + 1, issued_n);
@@ -683,12 +743,12 @@ __global__ void __launch_bounds__(TXW * TYT, TXW * TYT <= 256 && sizeof(T) == 4 
         }
         kbase += n_it;
 
-        const double2 rr = block_reduce_n<NTH, TXW>(acc, 0.0, red);
+        const double2 rr = block_reduce_n<NTH, TPX>(acc, 0.0, red);
         if (tid == 0) V.part_g[lt] = rr.x;
-        if (publish_partial_n<TXW>(&st->ticket_g, V.ntiles, &s_flag)) {
+        if (publish_partial_n<TPX>(&st->ticket_g, V.ntiles, &s_flag)) {
             double ssum = 0.0;
             for (int i = tid; i < V.ntiles; i += NTH) ssum += __ldcg(&V.part_g[i]);
-            const double2 tot = block_reduce_n<NTH, TXW>(ssum, 0.0, red);
+            const double2 tot = block_reduce_n<NTH, TPX>(ssum, 0.0, red);
             if (tid == 0) {
                 st->ticket_g = 0;
                 st->gn2 = tot.x;
@@ -722,8 +782,8 @@ cudaError_t launch_gradient_tma_v(const VolumeDesc<T> *vols, const int *tile_vol
     static const cudaError_t attr =
         cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
-    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue,
-                                                                   pf);
+    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag,
+                                                                       queue, pf);
     count_launch();
     return cudaGetLastError();
 }
@@ -746,7 +806,7 @@ int gradient_blocks_v() {
         int v = 0;
         cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              GradTmaLayout<T, TXW>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T, TXW, TYT>, TXW * TYT,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T, TXW, TYT>, TXW / 2 * TYT,
                                                       GradTmaLayout<T, TXW>::BYTES + 128);
         return v;
     }();
@@ -758,10 +818,11 @@ int gradient_blocks_v() {
 //   tile_x 32, threads_y 16  default, 256 threads (two blocks per SM for FP32)
 //   tile_x 32, threads_y 8   128 threads of two rows (four voxels) each
 //   tile_x 64, threads_y 16  FP32 only, 512 threads, one block per SM
-// Gradient kernel: tile_x x threads_y threads of TT_Y / threads_y rows each:
-//   tile_x 32, threads_y 8   default, 256 threads
-//   tile_x 32, threads_y 16  512 threads of one row each
-//   tile_x 64, threads_y 8   FP32 only, 512 threads
+// Gradient kernel: tile_x / 2 x threads_y threads of TT_Y / threads_y rows
+// and two columns each:
+//   tile_x 32, threads_y 16  default, 256 threads of one row
+//   tile_x 32, threads_y 8   128 threads of two rows
+//   tile_x 64, threads_y 8   FP32 only, 256 threads of two rows
 template <typename T>
 cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                              cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q,

@@ -203,11 +203,11 @@ def test_release_device_memory_then_solve_again():
 
 
 TILE_CANDIDATES = [
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
     {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 32},
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 16},
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 64},
-    {"tile_x": 32, "trial_threads_y": 8, "gradient_threads_y": 8, "bz": 32},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 16},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 64},
+    {"tile_x": 32, "trial_threads_y": 8, "gradient_threads_y": 16, "bz": 32},
     {"tile_x": 64, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
 ]
 
