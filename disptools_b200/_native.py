@@ -28,6 +28,8 @@ OK = 0
 ERR_ARGUMENT = -1
 ERR_CUDA = -2
 ERR_ALLOC = -3
+ERR_DEVICE = -4
+ERR_IO = -5
 
 STOP_REASONS = {
     0: "it_max",
@@ -127,6 +129,25 @@ lib.dtb_smooth_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P,
 lib.dtb_smooth_device.restype = _I
 lib.dtb_resample_device.argtypes = [_I, _I, _I, _SZ, _SZ, _SZ, _SZ, _SZ, _SZ, _P, _P, _P]
 lib.dtb_resample_device.restype = _I
+_SZP, _DP = C.POINTER(C.c_size_t), C.POINTER(C.c_double)
+lib.dtb_write_rvf.argtypes = [C.c_char_p, _SZ, _SZ, _SZ, _D, _D, _D, _P]
+lib.dtb_write_rvf.restype = _I
+lib.dtb_read_rvf_header.argtypes = [C.c_char_p, _SZP, _SZP, _SZP, _DP, _DP, _DP]
+lib.dtb_read_rvf_header.restype = _I
+lib.dtb_read_rvf.argtypes = [C.c_char_p, _P, _SZ]
+lib.dtb_read_rvf.restype = _I
+lib.dtb_write_vtk.argtypes = [C.c_char_p, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P]
+lib.dtb_write_vtk.restype = _I
+lib.dtb_read_vtk_header.argtypes = [C.c_char_p, C.POINTER(C.c_int), _SZP, _SZP, _SZP, _DP, _DP, _DP]
+lib.dtb_read_vtk_header.restype = _I
+lib.dtb_read_vtk.argtypes = [C.c_char_p, _P, _SZ]
+lib.dtb_read_vtk.restype = _I
+lib.dtb_volume_change_device.argtypes = [_I, _SZ, _D, _P, _P, _P]
+lib.dtb_volume_change_device.restype = _I
+lib.dtb_log_jacobian_accumulate_device.argtypes = [_I, _I, _SZ, _D, _P, _P, _P]
+lib.dtb_log_jacobian_accumulate_device.restype = _I
+lib.dtb_exp_mean_device.argtypes = [_I, _SZ, _D, _P, _P, _P]
+lib.dtb_exp_mean_device.restype = _I
 lib.dtb_set_autotune.argtypes = [_I]
 lib.dtb_set_autotune.restype = _I
 lib.dtb_get_tile_config.argtypes = [C.POINTER(C.c_int)]
@@ -152,6 +173,9 @@ EXPORTED = [
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
     "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
     "dtb_set_autotune", "dtb_get_tile_config", "dtb_smooth_device", "dtb_resample_device",
+    "dtb_write_rvf", "dtb_read_rvf_header", "dtb_read_rvf", "dtb_write_vtk", "dtb_read_vtk_header",
+    "dtb_read_vtk", "dtb_volume_change_device", "dtb_log_jacobian_accumulate_device",
+    "dtb_exp_mean_device",
 ]
 
 
@@ -170,6 +194,8 @@ def check(rc: int) -> None:
         msg = last_error() or f"error code {rc}"
         if rc == ERR_ARGUMENT:
             raise ValueError(msg)
+        if rc == ERR_IO:
+            raise OSError(msg)
         raise DisptoolsError(msg)
 
 

@@ -34,6 +34,8 @@ UNITS = [
     ("dt_capi.cu", []),
     ("dt_noalloc.cu", []),
     ("dt_resample.cu", []),
+    ("dt_io.cpp", []),
+    ("dt_maps.cu", []),
 ]
 HEADERS = ["dt_internal.h", "dt_kernels.cuh", "dt_kernels_tma.cuh", "dt_tma.cuh"]
 
@@ -69,11 +71,12 @@ def build_library(force: bool = False) -> str:
     objs = []
     for src, extra in UNITS:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        stem = os.path.splitext(src)[0]
+        o = os.path.join(BUILD, stem + ".o")
         objs.append(o)
         if force or _stale(o, [s, *headers, __file__]):
             _run([nvcc, *NVCC_FLAGS, *extra, "-c", s, "-o", o],
-                 log=os.path.join(BUILD, src.replace(".cu", ".ptxas.txt")))
+                 log=os.path.join(BUILD, stem + ".ptxas.txt"))
     if force or _stale(LIB, objs):
         _run([nvcc, "-shared", *ARCH, "-o", LIB, *objs])
     return LIB

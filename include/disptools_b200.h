@@ -124,7 +124,8 @@ enum {
     DTB_ERR_ARGUMENT = -1,
     DTB_ERR_CUDA = -2,
     DTB_ERR_ALLOC = -3,
-    DTB_ERR_DEVICE = -4
+    DTB_ERR_DEVICE = -4,
+    DTB_ERR_IO = -5 /* a file could not be opened, read, written or parsed */
 };
 
 /* Why a solve stopped; the stopping conditions of
@@ -274,6 +275,72 @@ int dtb_smooth_device(int precision, int comps, size_t nx, size_t ny, size_t nz,
 int dtb_resample_device(int precision, int mode, int comps, size_t nx, size_t ny, size_t nz,
                         size_t nx2, size_t ny2, size_t nz2,
                         const void *in, void *out, void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Jacobian-map utilities (device)                                     */
+/* ------------------------------------------------------------------ */
+
+enum {
+    DTB_CLAMP_THRESHOLD = 0, /* values outside [epsilon, 1e9] become epsilon */
+    DTB_CLAMP_REGULARISE = 1 /* values below epsilon become epsilon */
+};
+
+/* Volume-change map of a Jacobian map (jacobian_to_volume_change,
+ * disptools/displacements.py:628-668): J <= epsilon is replaced by epsilon,
+ * then out = J - 1 where J >= 1 and 1 - 1/J where J < 1.  `J` and `out` are
+ * n device values of the precision's element type. */
+int dtb_volume_change_device(int precision, size_t n, double epsilon, const void *J, void *out,
+                             void *stream);
+
+/* acc[i] += log(clamp(J[i])) over n values, acc in FP64: one map of the
+ * geometric means of average_jacobian (mode DTB_CLAMP_THRESHOLD,
+ * disptools/displacements.py:571-625) and
+ * average_jacobian_from_displacements (DTB_CLAMP_REGULARISE, :486-568). */
+int dtb_log_jacobian_accumulate_device(int precision, int mode, size_t n, double epsilon,
+                                       const void *J, double *acc, void *stream);
+
+/* out[i] = exp(scale * acc[i]): the geometric mean, scale = 1 / maps. */
+int dtb_exp_mean_device(int precision, size_t n, double scale, const double *acc, void *out,
+                        void *stream);
+
+/* ------------------------------------------------------------------ */
+/* Field files (host)                                                  */
+/* ------------------------------------------------------------------ */
+
+/* Replaces write_rvf (src/headers/rvf_io.h:9-12, src/rvf_io.c:11-50): the
+ * header lines "nx ny nz" and "dx dy dz" (%f), then 3 native-endian doubles
+ * per voxel (x fastest, components together).  `field` is [3][nz][ny][nx].
+ * The file functions return DTB_OK, DTB_ERR_ARGUMENT (invalid arguments, an
+ * output array too small) or DTB_ERR_IO (the file cannot be opened, read or
+ * written, is too short or malformed), with the error state set. */
+int dtb_write_rvf(const char *filename, size_t nx, size_t ny, size_t nz,
+                  double dx, double dy, double dz, const double *field);
+
+/* Size and spacing of an RVF file (the spacing is parsed as float, as the
+ * reference's read_rvf does, src/rvf_io.c:57-90). */
+int dtb_read_rvf_header(const char *filename, size_t *nx, size_t *ny, size_t *nz,
+                        double *dx, double *dy, double *dz);
+
+/* Replaces read_rvf (src/headers/rvf_io.h:17-21, src/rvf_io.c:57-125):
+ * reads the field into `field` [3][nz][ny][nx]; `capacity` is its length in
+ * elements. */
+int dtb_read_rvf(const char *filename, double *field, size_t capacity);
+
+/* Replaces write_vtk (src/headers/vtk_io.h, src/vtk_io.c:74-133): legacy VTK,
+ * BINARY, STRUCTURED_POINTS, origin 0, spacing (%f), SCALARS image_data
+ * double nd, big-endian doubles, nd components per voxel (x fastest).
+ * `data` is [nd][nz][ny][nx]. */
+int dtb_write_vtk(const char *filename, int nd, size_t nx, size_t ny, size_t nz,
+                  double dx, double dy, double dz, const double *data);
+
+/* Components, size and spacing of a legacy VTK file written as above. */
+int dtb_read_vtk_header(const char *filename, int *nd, size_t *nx, size_t *ny, size_t *nz,
+                        double *dx, double *dy, double *dz);
+
+/* Replaces read_vtk (src/vtk_io.c:138-215): reads the data into `data`
+ * [nd][nz][ny][nx]; `capacity` is its length in elements.  Float data is
+ * rejected, as by the reference. */
+int dtb_read_vtk(const char *filename, double *data, size_t capacity);
 
 /* Tile-shape autotuner of the gradient method.  When on (the default, or
  * DISPTOOLS_B200_AUTOTUNE=0 in the environment at first use for off), the
