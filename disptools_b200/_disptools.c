@@ -10,9 +10,10 @@
  *  - the GIL is released while the device works;
  *  - None is returned with its reference counted;
  *  - there is no CPU path: gpu_id >= 0 selects that device, gpu_id < 0 the
- *    current one.  `matching` is rejected as the reference GPU path does
- *    (python_c_extension/_disptools.c:368-373); shape_descriptor is not part
- *    of this build and raises NotImplementedError.
+ *    current one.  `matching` runs volume_matching_3d on the device (the
+ *    reference has it on the CPU only, python_c_extension/_disptools.c:368-373);
+ *    shape_descriptor is not part of this build and raises
+ *    NotImplementedError.
  */
 #define PY_SSIZE_T_CLEAN
 #define NPY_NO_DEPRECATED_API NPY_1_14_API_VERSION
@@ -159,8 +160,7 @@ static PyObject *method_displacement(PyObject *self, PyObject *args)
     } else if (!strcmp(algorithm, "greedy")) {
         alg = DTB_ALGORITHM_GREEDY;
     } else if (!strcmp(algorithm, "matching")) {
-        PyErr_Format(PyExc_ValueError, "Algorithm '%s' not supported on GPU", algorithm);
-        return NULL;
+        alg = DTB_ALGORITHM_MATCHING;
     } else {
         PyErr_Format(PyExc_ValueError, "Invalid algorithm '%s'.", algorithm);
         return NULL;
@@ -200,11 +200,15 @@ static PyObject *method_displacement(PyObject *self, PyObject *args)
                                             epsilon, tolerance, eta, eta_max, alpha, beta, gamma,
                                             delta, zeta, theta, iota, strict != 0, (size_t) it_max,
                                             fd);
-    else
+    else if (alg == DTB_ALGORITHM_GREEDY)
         generate_displacement_greedy_cuda(nx, ny, nz, spacing[0], spacing[1], spacing[2], Jd, md,
                                           epsilon, tolerance, eta, eta_max, alpha, beta, gamma,
                                           delta, zeta, theta, iota, strict != 0, (size_t) it_max,
                                           fd);
+    else
+        volume_matching_3d(nx, ny, nz, spacing[0], spacing[1], spacing[2], Jd, md, epsilon, tolerance,
+                           eta, eta_max, alpha, beta, gamma, delta, zeta, theta, iota, strict != 0,
+                           (size_t) it_max, fd);
     Py_END_ALLOW_THREADS
     if (disptools_has_error()) return raise_library_error();
     Py_RETURN_NONE;

@@ -23,6 +23,7 @@ PRECISION_MIXED = 0
 PRECISION_FP64 = 1
 ALGORITHM_GRADIENT = 0
 ALGORITHM_GREEDY = 1
+ALGORITHM_MATCHING = 2
 
 OK = 0
 ERR_ARGUMENT = -1
@@ -148,6 +149,11 @@ lib.dtb_log_jacobian_accumulate_device.argtypes = [_I, _I, _SZ, _D, _P, _P, _P]
 lib.dtb_log_jacobian_accumulate_device.restype = _I
 lib.dtb_exp_mean_device.argtypes = [_I, _SZ, _D, _P, _P, _P]
 lib.dtb_exp_mean_device.restype = _I
+lib.volume_matching_3d.argtypes = [_SZ, _SZ, _SZ, _D, _D, _D, _P, _P] + [_D] * 11 + [C.c_bool, _SZ, _P]
+lib.volume_matching_3d.restype = None
+lib.dtb_volume_matching.argtypes = [_SZ, _SZ, _SZ, _D, _D, _D, _P, _P, C.POINTER(Params), _P,
+                                    C.POINTER(SolveStats)]
+lib.dtb_volume_matching.restype = _I
 lib.dtb_set_autotune.argtypes = [_I]
 lib.dtb_set_autotune.restype = _I
 lib.dtb_get_tile_config.argtypes = [C.POINTER(C.c_int)]
@@ -175,7 +181,7 @@ EXPORTED = [
     "dtb_set_autotune", "dtb_get_tile_config", "dtb_smooth_device", "dtb_resample_device",
     "dtb_write_rvf", "dtb_read_rvf_header", "dtb_read_rvf", "dtb_write_vtk", "dtb_read_vtk_header",
     "dtb_read_vtk", "dtb_volume_change_device", "dtb_log_jacobian_accumulate_device",
-    "dtb_exp_mean_device",
+    "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching",
 ]
 
 
@@ -212,4 +218,6 @@ def algorithm_code(algorithm) -> int:
         return ALGORITHM_GRADIENT
     if algorithm in (ALGORITHM_GREEDY, "greedy"):
         return ALGORITHM_GREEDY
+    if algorithm in (ALGORITHM_MATCHING, "matching"):
+        return ALGORITHM_MATCHING
     raise ValueError(f"Invalid algorithm '{algorithm}'.")

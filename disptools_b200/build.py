@@ -26,8 +26,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                      f"-I{INCLUDE}", "-Xptxas", "-v"]
 
-# (source, extra flags): the FP64 kernels are built without multiply-add
-# contraction so their per-voxel arithmetic rounds like the reference C code.
+# (source, extra flags): the FP64 kernels and the matching solver (FP32, like
+# its reference) are built without multiply-add contraction so their
+# per-voxel arithmetic rounds like the reference C code.
 UNITS = [
     ("dt_kernels_f32.cu", []),
     ("dt_kernels_f64.cu", ["-fmad=false"]),
@@ -36,6 +37,7 @@ UNITS = [
     ("dt_resample.cu", []),
     ("dt_io.cpp", []),
     ("dt_maps.cu", []),
+    ("dt_matching.cu", ["-fmad=false"]),
 ]
 HEADERS = ["dt_internal.h", "dt_kernels.cuh", "dt_kernels_tma.cuh", "dt_tma.cuh"]
 

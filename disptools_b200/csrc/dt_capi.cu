@@ -1080,6 +1080,13 @@ extern "C" int dtb_generate_displacement_batched(int algorithm, int precision, i
 extern "C" int dtb_generate_displacement(int algorithm, int precision, size_t nx, size_t ny, size_t nz, double dx,
                                          double dy, double dz, const double *J, const bool *mask,
                                          const dtb_params *params, double *field, dtb_solve_stats *stats) {
+    if (algorithm == DTB_ALGORITHM_MATCHING) {
+        disptools_clear_error();
+        if (!params) DTB_FAIL(DTB_ERR_ARGUMENT, "null parameters");
+        const char *why = nullptr;
+        if (!check_params(*params, &why)) DTB_FAIL(DTB_ERR_ARGUMENT, why);
+        return dtb_volume_matching(nx, ny, nz, dx, dy, dz, J, mask, params, field, stats);
+    }
     const dtb_volume v = {nx, ny, nz, dx, dy, dz, J, mask, field};
     return dtb_generate_displacement_batched(algorithm, precision, 1, &v, params, stats);
 }

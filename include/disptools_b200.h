@@ -93,6 +93,21 @@ void generate_displacement_greedy_cuda(
     const double zeta, const double theta, const double iota,
     const bool strict, const size_t it_max, double *field);
 
+/* Replaces volume_matching_3d (src/headers/VolumeMatching3D.h,
+ * src/VolumeMatching3D.c:689-796), the `matching` algorithm, on the current
+ * device.  As in the reference, only epsilon (stop when the maximum voxel
+ * error of the last cost evaluation is below it), delta and zeta (the
+ * Jacobian barrier) and it_max are used, the arithmetic is FP32, and the
+ * mask is not used. */
+void volume_matching_3d(
+    const size_t nx, const size_t ny, const size_t nz,
+    const double dx, const double dy, const double dz,
+    const double *J, const bool *mask,
+    const double epsilon, const double tolerance, double eta, const double eta_max,
+    const double alpha, const double beta, const double gamma, const double delta,
+    const double zeta, const double theta, const double iota,
+    const bool strict, const size_t it_max, double *field);
+
 /* Replaces jacobian_dynamic (src/headers/jacobian.h:24-33,
  * src/jacobian.c:7-21), computed on the current device in FP64. */
 void jacobian_dynamic(
@@ -116,7 +131,8 @@ enum {
 
 enum {
     DTB_ALGORITHM_GRADIENT = 0,
-    DTB_ALGORITHM_GREEDY = 1
+    DTB_ALGORITHM_GREEDY = 1,
+    DTB_ALGORITHM_MATCHING = 2 /* single volumes, FP32 (dtb_volume_matching) */
 };
 
 enum {
@@ -211,6 +227,14 @@ typedef struct dtb_device_volume {
 int dtb_generate_displacement_batched_device(
     int algorithm, int precision, int count, const dtb_device_volume *volumes,
     const dtb_params *params, dtb_solve_stats *stats, void *stream);
+
+/* The matching solver (volume_matching_3d) with statistics: iterations,
+ * final cost (error), maximum voxel error of the last cost evaluation
+ * (max_error), final step (eta), stop reason.  Host arrays, current
+ * device; needs at least 2 voxels per axis. */
+int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+                        const double *J, const bool *mask, const dtb_params *params,
+                        double *field, dtb_solve_stats *stats);
 
 /* Jacobian determinant of a device-resident field (reference stencil and
  * boundary rules, src/jacobian.c:70-242).  `field` is [3][nz][ny][nx] and

@@ -194,7 +194,8 @@ def solver_params(**params):
 
 class Reference:
     """The reference C library compiled from its own sources (FP64 or FP32
-    FLOATING; ORDER_PD 4, or 2 for ``libdisptools_ref64_pd2``)."""
+    FLOATING; ORDER_PD 4, or 2 for ``libdisptools_ref64_pd2``;
+    ``libdisptools_ref64_match`` holds the matching solver)."""
 
     def __init__(self, flavour: str = "ref64"):
         path = os.path.join(REF_DIR, f"libdisptools_{flavour}.so")
@@ -203,11 +204,15 @@ class Reference:
         lib = C.CDLL(path)
         self.dtype = np.float64 if lib.get_float_type_size() == 64 else np.float32
         R = C.c_double if self.dtype == np.float64 else C.c_float
-        lib.jacobian_dynamic.argtypes = [_SZ, _SZ, _SZ, R, R, R, _P, _P]
-        lib.regularise.argtypes = [_SZ, _SZ, _SZ, _P, R]
+        if hasattr(lib, "jacobian_dynamic"):
+            lib.jacobian_dynamic.argtypes = [_SZ, _SZ, _SZ, R, R, R, _P, _P]
+            lib.regularise.argtypes = [_SZ, _SZ, _SZ, _P, R]
         args = [_SZ, _SZ, _SZ, R, R, R, _P, _P] + [R] * 11 + [C.c_bool, _SZ, _P]
-        lib.generate_displacement_gradient.argtypes = args
-        lib.generate_displacement_greedy.argtypes = args
+        if hasattr(lib, "generate_displacement_gradient"):
+            lib.generate_displacement_gradient.argtypes = args
+            lib.generate_displacement_greedy.argtypes = args
+        if hasattr(lib, "volume_matching_3d"):
+            lib.volume_matching_3d.argtypes = args
         lib.disptools_has_error.restype = C.c_bool
         self.lib = lib
 
@@ -234,8 +239,9 @@ class Reference:
         mask = np.ascontiguousarray(mask, dtype=np.bool_)
         out = (np.zeros((3, nz, ny, nx), self.dtype) if field is None
                else np.ascontiguousarray(field, dtype=self.dtype).copy())
-        fn = {"gradient": self.lib.generate_displacement_gradient,
-              "greedy": self.lib.generate_displacement_greedy}[algorithm]
+        fn = {"gradient": lambda: self.lib.generate_displacement_gradient,
+              "greedy": lambda: self.lib.generate_displacement_greedy,
+              "matching": lambda: self.lib.volume_matching_3d}[algorithm]()
         fn(nx, ny, nz, *map(float, spacing), _ptr(Jt), _ptr(mask), *solver_params(**params),
            _ptr(out))
         if self.lib.disptools_has_error():

@@ -4,7 +4,8 @@ The reference library (disptools v0.4.1, src/*.c) is compiled from its own
 sources into oracle/_ref/ by oracle/Makefile (FLOAT_SIZE=64, ORDER_PD=4, and
 ORDER_PD=2 for the gradient check).  This script calls it through its C ABI
 (jacobian_dynamic, generate_displacement_gradient,
-generate_displacement_greedy) on seeded inputs and stores inputs and outputs
+generate_displacement_greedy, and volume_matching_3d from
+libdisptools_ref64_match) on seeded inputs and stores inputs and outputs
 as small .npz files.  Run it where the reference sources are available:
 
     python tests/golden/make_golden.py
@@ -66,6 +67,10 @@ def small_problem(seed: int, shape):
 
 
 def main() -> None:
+    if os.environ.get("MALLOC_PERTURB_") != "255":
+        # zero-filled mallocs for the reference matching solver (see below)
+        os.execve(sys.executable, [sys.executable, os.path.abspath(__file__)],
+                  {**os.environ, "MALLOC_PERTURB_": "255"})
     build(ref=True)
     ref = Reference("ref64")
     ref2 = Reference("ref64_pd2")
@@ -126,6 +131,36 @@ def main() -> None:
     }
     with open(os.path.join(HERE, "solver_cases.json"), "w") as fh:
         json.dump({"cases": cases, "config1": c1}, fh, indent=1)
+
+    # Matching solver (src/VolumeMatching3D.c), FP32 arithmetic.  Its first
+    # gradient accumulates into malloc'd buffers it never clears
+    # (src/VolumeMatching3D.c:422-427 and :445): with whatever the allocator
+    # hands back its results are NaN or depend on earlier allocations.  This
+    # script therefore runs with MALLOC_PERTURB_=255 (see main), under which
+    # glibc fills every malloc'd block with zero bytes, i.e. the buffers
+    # start cleared, as every later gradient of the reference does.
+    refm = Reference("ref64_match")
+    mat = {}
+    for k, (shape, init, spacing, it_max) in enumerate([
+        ((20, 20, 20), False, (1.0, 1.0, 1.0), 60),
+        ((14, 12, 10), True, (1.0, 1.0, 1.0), 40),
+        ((12, 13, 11), False, (0.8, 1.1, 1.25), 40),
+    ]):
+        if k == 0:
+            mask = ball(20, 10, 5)
+            Jt = np.where(mask, 1.1, 1.0)
+        else:
+            Jt, mask = small_problem(300 + k, shape)
+        field0 = (np.random.default_rng(400 + k).normal(scale=0.05, size=(3,) + shape)
+                  if init else np.zeros((3,) + shape))
+        out = refm.solve("matching", Jt, mask, field=field0, spacing=spacing, it_max=it_max)
+        mat[f"m{k}_Jt"] = Jt
+        mat[f"m{k}_mask"] = mask
+        mat[f"m{k}_field0"] = field0
+        mat[f"m{k}_spacing"] = np.array(spacing)
+        mat[f"m{k}_it_max"] = np.array(it_max)
+        mat[f"m{k}_out"] = out
+    np.savez_compressed(os.path.join(HERE, "matching.npz"), **mat)
     print("golden fixtures written to", HERE)
 
 

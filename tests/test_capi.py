@@ -89,6 +89,10 @@ def test_python_api_argument_checks():
     with pytest.raises(ValueError):
         dt.solve(np.ones((4, 4, 4)), np.ones((4, 4, 5), bool))
     with pytest.raises(ValueError):
-        dt.solve(np.ones((4, 4, 4)), np.ones((4, 4, 4), bool), algorithm="matching")
+        dt.solve(np.ones((4, 4, 4)), np.ones((4, 4, 4), bool), algorithm="bogus")
+    with pytest.raises(ValueError):  # matching needs two voxels per axis
+        dt.solve(np.ones((1, 4, 4)), np.ones((1, 4, 4), bool), algorithm="matching")
+    with pytest.raises(ValueError):
+        dt.solve(np.ones((4, 4, 4)), np.ones((4, 4, 4), bool), algorithm="matching", zeta=-1.0)
     with pytest.raises(TypeError):
         dt.solve(np.ones((4, 4, 4)), np.ones((4, 4, 4), bool), bogus=1)

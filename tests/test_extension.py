@@ -35,8 +35,8 @@ def test_displacement_argument_errors():
     f = np.zeros((3, 5, 5, 5))
     with pytest.raises(ValueError, match="Invalid algorithm"):
         call(J, m, f, algorithm="bogus")
-    with pytest.raises(ValueError, match="not supported on GPU"):
-        call(J, m, f, algorithm="matching")
+    with pytest.raises(RuntimeError, match="at least 2 voxels"):  # matching: host-side check
+        call(np.ones((1, 5, 5)), np.ones((1, 5, 5), bool), np.zeros((3, 1, 5, 5)), algorithm="matching")
     with pytest.raises(TypeError):
         call(J.astype(np.float32), m, f)
     with pytest.raises(TypeError):
