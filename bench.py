@@ -271,14 +271,16 @@ def run_c4(args, world, rank, local):
     if not args.no_e2e:
         pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
         hv = [(pin(J), pin(m), pin(np.zeros((3,) + J.shape))) for J, m in host]
-        dt.solve_batched(hv, it_max=IT)
+        dt.solve_batched(hv, it_max=IT, inplace=True)
         barrier(world)
         te = 0.0
         ve = 0.0
         ke = max(1, min(args.steps, 2))
         for _ in range(ke):
+            for _, _, f in hv:
+                f[...] = 0.0  # zero initial guess, written before the timed call
             t0 = time.perf_counter()
-            res = dt.solve_batched(hv, it_max=IT) if hv else []
+            res = dt.solve_batched(hv, it_max=IT, inplace=True) if hv else []
             te += time.perf_counter() - t0
             ve += sum(float(J.size) * iterations_done(st) for (J, _, _), (_, st) in zip(hv, res))
         te = max_over_ranks(world, te)
@@ -286,7 +288,8 @@ def run_c4(args, world, rank, local):
         e2e = {"value": sum_over_ranks(world, ve) / te, "unit": UNIT,
                "h2d_bytes_per_step": int(sum_over_ranks(world, nb)),
                "d2h_bytes_per_step": int(sum_over_ranks(world, sum(f.nbytes for _, _, f in hv))),
-               "steps": ke, "path": "disptools_b200.solve_batched (C ABI, host float64 arrays)"}
+               "steps": ke, "path": "disptools_b200.solve_batched(inplace=True) (C ABI, host float64 "
+                                     "arrays in pinned memory)"}
 
     if rank == 0:
         print(json.dumps({

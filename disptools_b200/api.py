@@ -105,12 +105,15 @@ def solve(J: np.ndarray, mask: np.ndarray, field: np.ndarray | None = None,
 
 
 def solve_batched(volumes: Iterable, algorithm: str = "gradient", precision: str = "mixed",
-                  **params):
+                  inplace: bool = False, **params):
     """Solve several independent volumes of any sizes in one batched run.
 
     ``volumes`` is an iterable of ``(J, mask)``, ``(J, mask, field)`` or
     ``(J, mask, field, spacing)`` tuples.  Returns a list of
-    ``(field, stats)``."""
+    ``(field, stats)``.  With ``inplace`` each given field (C-contiguous
+    float64) is the initial guess and receives the result, as the reference
+    C API's in/out field does, with no copy; fields in pinned memory then
+    move at full link speed."""
     vols = list(volumes)
     arr = (N.Volume * len(vols))()
     keep = []
@@ -122,8 +125,14 @@ def solve_batched(volumes: Iterable, algorithm: str = "gradient", precision: str
         J = _f64(J, "J")
         nz, ny, nx = J.shape
         mask = _mask(mask, J.shape)
-        out = (np.zeros((3, nz, ny, nx)) if field is None
-               else _f64(field, "field", (3, nz, ny, nx)).copy())
+        if inplace:
+            if (not isinstance(field, np.ndarray) or field.dtype != np.float64
+                    or not field.flags.c_contiguous or field.shape != (3, nz, ny, nx)):
+                raise ValueError("inplace needs C-contiguous float64 fields of shape (3, nz, ny, nx)")
+            out = field
+        else:
+            out = (np.zeros((3, nz, ny, nx)) if field is None
+                   else _f64(field, "field", (3, nz, ny, nx)).copy())
         keep += [J, mask]
         outs.append(out)
         arr[i] = N.Volume(nx, ny, nz, *map(float, spacing), J.ctypes.data, mask.ctypes.data,

@@ -268,3 +268,20 @@ def test_every_tile_shape_mixed_residual(oracle, monkeypatch, shape):
     ref, _ = oracle.solve("gradient", Jt, mask, it_max=1000)
     r_ref = masked_max(oracle.jacobian(ref), Jt, mask)
     assert abs(masked_max(oracle.jacobian(out), Jt, mask) - r_ref) <= 1e-4
+
+
+def test_batched_inplace_equals_copying():
+    rng = np.random.default_rng(12)
+    vols = []
+    for n in [(10, 12, 9), (16, 8, 11)]:
+        Jt = np.ascontiguousarray(1.0 + 0.1 * rng.standard_normal(n))
+        mask = np.ascontiguousarray(rng.random(n) < 0.4)
+        vols.append((Jt, mask, np.zeros((3,) + n)))
+    copied = dt.solve_batched(vols, it_max=20)
+    res = dt.solve_batched(vols, it_max=20, inplace=True)
+    for (a, sa), (b, sb), v in zip(copied, res, vols):
+        assert b is v[2]
+        np.testing.assert_array_equal(a, b)
+        assert sa["iterations"] == sb["iterations"]
+    with pytest.raises(ValueError):
+        dt.solve_batched([(vols[0][0], vols[0][1], np.zeros((3, 10, 12, 9), np.float32))], inplace=True)
