@@ -14,6 +14,6 @@ hand-written CUDA kernels in ``libdisptools_b200.so``; there is no CPU path.
 from ._native import DisptoolsError, lib  # noqa: F401  (loads the CUDA library)
 from .api import (jacobian, kernel_launch_count, kernel_profile, regularise,  # noqa: F401
                   release_device_memory, set_autotune, set_default_precision, set_profiling,
-                  solve, solve_batched, tile_config)
+                  set_verbose, solve, solve_batched, tile_config)
 
 __version__ = "0.1.0"

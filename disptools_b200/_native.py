@@ -154,6 +154,12 @@ lib.volume_matching_3d.restype = None
 lib.dtb_volume_matching.argtypes = [_SZ, _SZ, _SZ, _D, _D, _D, _P, _P, C.POINTER(Params), _P,
                                     C.POINTER(SolveStats)]
 lib.dtb_volume_matching.restype = _I
+lib.dtb_set_device_memory_limit.argtypes = [_SZ]
+lib.dtb_set_device_memory_limit.restype = _I
+lib.dtb_test_drop_tma_load.argtypes = [C.c_longlong, _I, C.c_uint]
+lib.dtb_test_drop_tma_load.restype = _I
+lib.dtb_set_verbose.argtypes = [_I]
+lib.dtb_set_verbose.restype = _I
 lib.dtb_set_autotune.argtypes = [_I]
 lib.dtb_set_autotune.restype = _I
 lib.dtb_get_tile_config.argtypes = [C.POINTER(C.c_int)]
@@ -181,7 +187,8 @@ EXPORTED = [
     "dtb_set_autotune", "dtb_get_tile_config", "dtb_smooth_device", "dtb_resample_device",
     "dtb_write_rvf", "dtb_read_rvf_header", "dtb_read_rvf", "dtb_write_vtk", "dtb_read_vtk_header",
     "dtb_read_vtk", "dtb_volume_change_device", "dtb_log_jacobian_accumulate_device",
-    "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching",
+    "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching", "dtb_set_verbose",
+    "dtb_set_device_memory_limit", "dtb_test_drop_tma_load",
 ]
 
 

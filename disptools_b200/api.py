@@ -146,6 +146,12 @@ def solve_batched(volumes: Iterable, algorithm: str = "gradient", precision: str
     return [(o, s.as_dict()) for o, s in zip(outs, stats)]
 
 
+def set_verbose(on: bool) -> bool:
+    """Print the reference's per-iteration lines on stdout after each solve;
+    returns the previous setting."""
+    return bool(N.lib.dtb_set_verbose(1 if on else 0))
+
+
 def set_autotune(on: bool) -> bool:
     """Turn the tile-shape autotuner of gradient solves on or off; returns
     the previous setting."""

@@ -160,18 +160,32 @@ std::mutex g_ws_mutex;
 // kept until dtb_release_device_memory() or the end of the process.
 std::vector<Workspace> g_ws, g_io;
 
+// Failure-path test hook (dtb_test_drop_tma_load).
+struct DropTest {
+    long long tile = -1;
+    int iteration = -1;
+    unsigned wait_limit = 0;
+} g_drop;
+
+// Cap on the device memory each of the two areas may hold (0: none).
+size_t g_mem_limit = 0;
+
 int grow(std::vector<Workspace> &pool, size_t bytes, char **out) {
     int dev = 0;
     DTB_CUDA(cudaGetDevice(&dev));
     if ((int) pool.size() <= dev) pool.resize(dev + 1);
     Workspace &w = pool[dev];
+    if (g_mem_limit && bytes > g_mem_limit)
+        DTB_FAIL(DTB_ERR_ALLOC, "the solve needs more device memory than the limit set by "
+                                "dtb_set_device_memory_limit");
     if (w.ptr && w.bytes < bytes) {
         cudaFree(w.ptr);
         w.ptr = nullptr;
         w.bytes = 0;
     }
     if (!w.ptr) {
-        const size_t want = bytes + bytes / 8;
+        size_t want = bytes + bytes / 8;
+        if (g_mem_limit && want > g_mem_limit) want = g_mem_limit;
         if (cudaMalloc(&w.ptr, want) != cudaSuccess) {
             cudaGetLastError();
             w.ptr = nullptr;
@@ -397,6 +411,17 @@ int ensure_profiling(Engine *e, size_t nk) {
     return DTB_OK;
 }
 
+// Verbose output of the solvers (the reference's verbose_printf lines);
+// -1: read DISPTOOLS_B200_VERBOSE on first use.
+int g_verbose = -1;
+bool verbose_enabled() {
+    if (g_verbose < 0) {
+        const char *v = std::getenv("DISPTOOLS_B200_VERBOSE");
+        g_verbose = (v && std::strcmp(v, "0") != 0 && v[0]) ? 1 : 0;
+    }
+    return g_verbose != 0;
+}
+
 // Tile and block shape of the TMA kernels (gradient method):
 //   tile_x    tile width in voxels (32, or 64 for FP32); tiles are TT_Y high
 //   trial_ty  thread rows of the trial kernel (16: one tile row and two
@@ -481,6 +506,9 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     const bool gradient = algorithm == DTB_ALGORITHM_GRADIENT;
     // ---- workspace layout: every buffer of the solve is the library's own,
     // in the pitched layout.
+    const long long log_cap = (verbose_enabled() && !tune_ms)
+                                  ? std::min<long long>(4 * (std::max<long long>(p.it_max, 0) + 16), 1ll << 20)
+                                  : 0;
     std::vector<int> tiles(count), tbegin(count);
     std::vector<Geom> geo(count);
     int total_tiles = 0;
@@ -501,6 +529,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         need += 2 * align(N * sizeof(T));            // e' (gradient) or error maps (greedy)
         need += align(t * sizeof(double2)) + align(t * sizeof(double));
         need += align(sizeof(SolverState)) + align(7 * sizeof(CUtensorMap));
+        need += align((size_t) log_cap * sizeof(IterLog));
     }
     need += align(count * sizeof(VolumeDesc<T>)) + align(total_tiles * sizeof(int)) + align(2 * sizeof(TileQueue));
 
@@ -538,6 +567,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         d.part_t = cv.take<double2>(tiles[i]);
         d.part_g = cv.take<double>(tiles[i]);
         d.st = cv.take<SolverState>(1);
+        IterLog *log = log_cap ? cv.take<IterLog>((size_t) log_cap) : nullptr;
         d_maps[i] = cv.take<CUtensorMap>(7);
         const int bz = bz_for(g.nz, cfg.bz);
         d.tiles_x = (g.nx + tile_x - 1) / tile_x;
@@ -546,6 +576,9 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         d.tile_begin = tbegin[i];
         d.ntiles = tiles[i];
         d.bz = bz;
+        d.drop_tile = (gradient && !tune_ms) ? (int) g_drop.tile : -1;
+        d.drop_it = g_drop.iteration;
+        d.wait_limit = g_drop.wait_limit;
         for (int t = 0; t < tiles[i]; ++t) tile_vol[tbegin[i] + t] = i;
 
         SolverState &s = hst[i];
@@ -567,6 +600,9 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         s.E_last = DBL_MAX;
         s.M_last = DBL_MAX;
         s.phase = PH_EVAL0;
+        s.log = log;
+        s.log_cap = log_cap;
+        s.log_n = 0;
 
         if (tune_ms) {
             // A step in the main loop: both kernels do all their work.
@@ -839,6 +875,35 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ev0, ev1) != cudaSuccess) ms = -1.f;
     cudaGetLastError();
+    if (log_cap) {
+        // The reference's verbose lines (src/displacement_field_gradient.c:377-410,
+        // src/displacement_field_greedy.c:184-228), printed after the solve.
+        for (int i = 0; i < count; ++i) {
+            const SolverState &s = h_states[i];
+            std::vector<IterLog> lines((size_t) std::min(s.log_n, log_cap));
+            if (!lines.empty())
+                DTB_CUDA(cudaMemcpy(lines.data(), s.log, lines.size() * sizeof(IterLog), cudaMemcpyDeviceToHost));
+            if (count > 1) std::printf("Volume %d\n", i);
+            for (const IterLog &l : lines) {
+                if (l.kind == 0)
+                    std::printf("Iteration %5lld:  total error %6e  max voxel error %6e  eta %6e\n", l.it, l.E, l.M,
+                                l.eta);
+                else
+                    std::printf("Error not decreasing, reducing step size to %.4e\n", l.eta);
+            }
+            switch (s.reason) {
+            case DTB_STOP_ERROR_EXPLODED: std::printf("Terminating: error exploded.\n"); break;
+            case DTB_STOP_ETA:
+            case DTB_STOP_THETA: std::printf("Error not decreasing, terminating.\n"); break;
+            case DTB_STOP_MAX_EXPLODED: std::printf("Terminating: voxel error exploded.\n"); break;
+            case DTB_STOP_EPSILON: std::printf("Terminating: reached desired tolerance.\n"); break;
+            default: break;
+            }
+            // Printed when the loop counter equals it_max on exit (:418).
+            if (s.it == p.it_max) std::printf("Terminating: reached maximum number of iterations.\n");
+        }
+        std::fflush(stdout);
+    }
     if (stats) {
         for (int i = 0; i < count; ++i) {
             const SolverState &s = h_states[i];
@@ -1252,6 +1317,30 @@ extern "C" int dtb_jacobian_adjoint_device(int precision, int order, size_t nx, 
         return adjoint_device_impl<float>(g, static_cast<const float *>(field), static_cast<const float *>(grad_J),
                                           static_cast<float *>(grad_field), s);
     DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
+extern "C" int dtb_set_device_memory_limit(size_t bytes) {
+    disptools_clear_error();
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    g_mem_limit = bytes;
+    return DTB_OK;
+}
+
+extern "C" int dtb_test_drop_tma_load(long long tile, int iteration, unsigned wait_limit) {
+    disptools_clear_error();
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    g_drop.tile = tile;
+    g_drop.iteration = iteration;
+    g_drop.wait_limit = tile >= 0 ? wait_limit : 0;
+    return DTB_OK;
+}
+
+extern "C" int dtb_set_verbose(int on) {
+    disptools_clear_error();
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    const int prev = verbose_enabled() ? 1 : 0;
+    g_verbose = on ? 1 : 0;
+    return prev;
 }
 
 extern "C" int dtb_set_autotune(int on) {

@@ -28,6 +28,17 @@ enum Phase {
 // Per-volume solver state, resident in device memory.  The last block of each
 // trial launch runs the step control on it (one thread, FP64), so no host
 // round trip is needed between trials.
+// One line of the verbose output: the reference prints "Iteration ..."
+// after every line search (kind 0) and the greedy method "reducing step
+// size" after a rejected step (kind 1), src/displacement_field_gradient.c:377-383,
+// src/displacement_field_greedy.c:184-212.
+struct IterLog {
+    long long it;
+    int kind;
+    int pad;
+    double E, M, eta;
+};
+
 struct SolverState {
     // parameters (reference signature order)
     double epsilon, tolerance, eta_max, alpha, beta, gamma, delta, zeta, theta, iota;
@@ -51,6 +62,8 @@ struct SolverState {
     unsigned int ticket_t;   // block counters of the trial / gradient launches
     unsigned int ticket_g;
     int fault;               // a bounded wait gave up (reported as an error)
+    IterLog *log;            // verbose output (null when off)
+    long long log_cap, log_n;
 };
 
 // Dynamic tile queue of one persistent launch: blocks take tiles with an
@@ -94,6 +107,12 @@ struct VolumeDesc {
     int tile_begin;          // first global tile index of this volume
     int ntiles;
     int bz;                  // planes per tile
+    // Failure-path test (dtb_test_drop_tma_load): the trial launch's tile
+    // `drop_tile` (global index, -1: none) does not issue the loads of its
+    // iteration `drop_it`; bounded waits poll at most `wait_limit` times
+    // (0: the default bound).
+    int drop_tile, drop_it;
+    unsigned wait_limit;
 };
 
 enum Mode { MODE_JAC = 0, MODE_GRAD = 1, MODE_GREEDY = 2 };

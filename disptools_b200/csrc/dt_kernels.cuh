@@ -150,6 +150,18 @@ __device__ __forceinline__ void finish(SolverState *st, int reason) {
     st->reason = reason;
 }
 
+__device__ __forceinline__ void log_line(SolverState *st, int kind, double E, double M) {
+    if (st->log && st->log_n < st->log_cap) {
+        IterLog &l = st->log[st->log_n++];
+        l.it = st->it;
+        l.kind = kind;
+        l.pad = 0;
+        l.E = E;
+        l.M = M;
+        l.eta = st->eta;
+    }
+}
+
 __device__ inline void control_after_trial(SolverState *st, double E, double M) {
     st->E = E;
     st->M = M;
@@ -160,6 +172,8 @@ __device__ inline void control_after_trial(SolverState *st, double E, double M) 
         st->E_last = E;
         st->ret_E = E;
         st->ret_M = M;
+        st->it = 0;
+        if (st->algorithm == DTB_ALGORITHM_GRADIENT) log_line(st, 0, E, M);  // :272-277
         st->it = 1;
         if (st->algorithm == DTB_ALGORITHM_GRADIENT) {
             st->phase = PH_SEARCH;
@@ -199,6 +213,7 @@ __device__ inline void control_after_trial(SolverState *st, double E, double M) 
             st->eta *= st->beta;
             break;
         }
+        log_line(st, 0, E, M);  // :377-383
         if (!is_normal(E)) finish(st, DTB_STOP_ERROR_EXPLODED);  // :387-410
         else if (st->eta < st->iota) finish(st, DTB_STOP_ETA);
         else if (1.0 - E / st->E_last < st->theta) finish(st, DTB_STOP_THETA);
@@ -224,10 +239,12 @@ __device__ inline void control_after_trial(SolverState *st, double E, double M) 
     case PH_GREEDY:
         st->trials++;
         st->v_cur ^= 1;  // the error map just written is the current one, accepted or not
+        log_line(st, 0, E, M);                                    // :184-189
         if (!is_normal(E)) finish(st, DTB_STOP_ERROR_EXPLODED);  // :193-196
         else if (E >= st->E_last) {                               // :198-213
             st->eta *= st->beta;
             if (st->eta < st->iota) finish(st, DTB_STOP_ETA);
+            else log_line(st, 1, E, M);
         } else if (1.0 - E / st->E_last < st->theta) finish(st, DTB_STOP_THETA);
         else if (!is_normal(M)) finish(st, DTB_STOP_MAX_EXPLODED);
         else if (M < st->epsilon) finish(st, DTB_STOP_EPSILON);

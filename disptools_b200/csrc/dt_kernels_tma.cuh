@@ -196,9 +196,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
 
         int issued_n = 0;  // iterations whose loads were issued (thread 0)
+        const unsigned wait_limit = V.wait_limit ? V.wait_limit : (1u << 22);
         // Issues the loads of iteration j (candidate plane z0-2+j) into its stage.
         auto issue = [&](int j) {
             issued_n = j + 1;
+            if (tile == V.drop_tile && j == V.drop_it) return;  // failure-path test only
             const uint32_t k = kbase + j;
             const int s = k % L::S;
             unsigned char *sb = smem + s * L::STAGE_BYTES;
@@ -257,7 +259,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             const uint32_t par = (k / L::S) & 1u;
             // Every thread waits for the stage itself (bounded); a timeout is
             // agreed on after the barrier below, so all threads leave together.
-            const bool ok = mbar_wait_bounded(&bars[s], par);
+            const bool ok = mbar_wait_bounded(&bars[s], par, wait_limit);
             if (!ok) s_fault = 1;
             const unsigned char *sb = smem + s * L::STAGE_BYTES;
             const int q = z0 - 2 + it, ze = q - 2;

@@ -366,6 +366,35 @@ int dtb_read_vtk_header(const char *filename, int *nd, size_t *nx, size_t *ny, s
  * rejected, as by the reference. */
 int dtb_read_vtk(const char *filename, double *data, size_t capacity);
 
+/* Upper bound, in bytes, on each of the two device-memory areas the library
+ * keeps (the solver workspace and the staging area of host-array calls);
+ * 0 removes the bound.  A solve that needs more fails with DTB_ERR_ALLOC and
+ * the error state set, before touching the device.  For hosts with a fixed
+ * memory budget; the tests use it to make an allocation fail. */
+int dtb_set_device_memory_limit(size_t bytes);
+
+/* Test hook of the failure path of the gradient method: in the following
+ * solves, the trial launch's tile `tile` (global tile index, -1 turns the
+ * hook off) does not issue the TMA loads of its plane iteration
+ * `iteration`, and every bounded wait of the trial kernel polls at most
+ * `wait_limit` times.  The block's wait for the missing plane then runs
+ * out: the volume is stopped with its fault flag, the block waits (bounded)
+ * for the loads it did issue, which complete normally, and the solve
+ * returns DTB_ERR_CUDA with the error state set; the device stays usable.
+ * No fault, trap or endless wait is involved. */
+int dtb_test_drop_tma_load(long long tile, int iteration, unsigned wait_limit);
+
+/* Verbose solver output on stdout, in the reference's format: one
+ * "Iteration %5ld:  total error %6e  max voxel error %6e  eta %6e" line per
+ * line search (per trial for the greedy method, with its "reducing step
+ * size" lines) and the termination message
+ * (src/displacement_field_gradient.c:377-410,
+ * src/displacement_field_greedy.c:184-228, printed there when built with
+ * DISPTOOLS_VERBOSE).  The lines are collected on the device and printed
+ * after each solve.  Off by default, or on when DISPTOOLS_B200_VERBOSE is
+ * set (and not "0") at first use.  Returns the previous setting. */
+int dtb_set_verbose(int on);
+
 /* Tile-shape autotuner of the gradient method.  When on (the default, or
  * DISPTOOLS_B200_AUTOTUNE=0 in the environment at first use for off), the
  * first solve of a problem shape on a device (shape = element type, volume
