@@ -8,6 +8,7 @@
 // is relaunched until every volume reports done; the host reads the small
 // state array once per graph launch, never per trial.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -144,6 +145,15 @@ extern "C" bool set_device(const int id) {
     }
     return true;
 }
+
+// NVTX range over a scope (shows the solver's phases in a timeline profiler;
+// header-only NVTX 3, inactive unless a tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // ---------------------------------------------------------------------------
 // Device workspace: one growing allocation reused across calls.
@@ -487,6 +497,7 @@ template <typename T>
 int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, const dtb_params &p,
                     dtb_solve_stats *stats, int precision, const TileConfig *cfg_in = nullptr,
                     float *tune_ms = nullptr) {
+    NvtxRange range(tune_ms ? "dtb tile-shape trial" : "dtb solve");
     cudaStream_t stream = e->stream;
     const int count = (int) vols.size();
     TileConfig cfg;
@@ -829,6 +840,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         *all_done = done;
         return cudaSuccess;
     };
+    NvtxRange loop_range("dtb step graphs");
     long long r = 0;
     if ((loop_err = enqueue(0)) != cudaSuccess) status = DTB_ERR_CUDA;
     while (status == DTB_OK) {
@@ -986,6 +998,7 @@ int choose_config(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, 
         *out = it->second;
         return DTB_OK;
     }
+    NvtxRange range("dtb autotune");
     TileConfig best = c;
     float best_ms = FLT_MAX;
     for (const TileConfig &cand : tile_candidates(sizeof(T))) {
@@ -1049,6 +1062,7 @@ template <typename T>
 int solve_host(int algorithm, int count, const dtb_volume *vols, const dtb_params &p, dtb_solve_stats *stats,
                int precision) {
     std::lock_guard<std::mutex> lock(g_ws_mutex);
+    NvtxRange range("dtb solve (host arrays)");
     Engine *e = nullptr;
     int rc = engine(&e);
     if (rc != DTB_OK) return rc;
