@@ -293,14 +293,15 @@ EncodeTiledFn encode_fn() {
 }
 
 // Tiled map over a pitched [comps][nz][ny][nx] array (comps = 1 gives rank 3).
+// The box is box_x x box_y x box_z voxels of every component.
 bool encode_map(CUtensorMap *out, CUtensorMapDataType type, size_t esize, const void *base, const Geom &g, int comps,
-                uint32_t box_x, uint32_t box_y) {
+                uint32_t box_x, uint32_t box_y, uint32_t box_z = 1) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
     const int rank = comps > 1 ? 4 : 3;
     cuuint64_t dims[4] = {(cuuint64_t) g.nx, (cuuint64_t) g.ny, (cuuint64_t) g.nz, (cuuint64_t) comps};
     cuuint64_t strides[3] = {(cuuint64_t) g.ys * esize, (cuuint64_t) g.zs * esize, (cuuint64_t) g.cs * esize};
-    cuuint32_t box[4] = {box_x, box_y, 1, (cuuint32_t) comps};
+    cuuint32_t box[4] = {box_x, box_y, box_z, (cuuint32_t) comps};
     cuuint32_t es[4] = {1, 1, 1, 1};
     return fn(out, type, rank, const_cast<void *>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -440,7 +441,7 @@ bool verbose_enabled() {
 //             columns per thread; 8: two rows)
 //   bz        planes of a tile along z (capped at nz)
 //   pf        L2 prefetch distance in planes beyond each TMA load (0: off)
-// The greedy method runs BX x BY tiles of bz planes.
+// The greedy method runs 32 x TT_Y tiles of bz planes.
 struct TileConfig {
     int tile_x = 32, trial_ty = 16, grad_ty = 16, bz = 32, pf = 0;
     bool operator==(const TileConfig &o) const {
@@ -511,7 +512,8 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     e->last_cfg[1] = cfg.trial_ty;
     e->last_cfg[2] = cfg.grad_ty;
     e->last_cfg[3] = cfg.bz;
-    const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? cfg.tile_x : BX;
+    // The greedy trial kernel exists for 32-wide tiles only.
+    const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? cfg.tile_x : 32;
     const int threads_y = cfg.grad_ty;
     const int trial_ty = cfg.trial_ty;
     const bool gradient = algorithm == DTB_ALGORITHM_GRADIENT;
@@ -525,7 +527,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     int total_tiles = 0;
     size_t need = 0;
     auto align = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const int tile_y = gradient ? TT_Y : BY;
+    const int tile_y = TT_Y;
     for (int i = 0; i < count; ++i) {
         const Geom g = pitched(vols[i].g);
         geo[i] = g;
@@ -644,17 +646,21 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
             DTB_CUDA(cudaMemsetAsync(aux1, 0, N * sizeof(T), stream));
         }
 
-        if (gradient) {
+        {
             CUtensorMap h_maps[7];
             const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
             // Boxes: the tile plus 4 voxels in x (16-byte aligned start) and 2
-            // rows in y for the stencil inputs; the bare tile for J_t and the mask.
+            // rows in y for the stencil inputs; the bare tile for J_t and the
+            // mask.  The greedy method's error maps are read as three planes
+            // with 3 rows of halo in y (slots 3 and 4).
             const uint32_t bx = (uint32_t) tile_x;
+            T *m3 = gradient ? d.ep[0] : d.v[0], *m4 = gradient ? d.ep[1] : d.v[1];
+            const uint32_t my = gradient ? TT_Y + 4 : TT_Y + 6, mz = gradient ? 1 : 3;
             bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, bx + 8, TT_Y + 4) &&
                       encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, bx + 8, TT_Y + 4) &&
                       encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, bx + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[3], ft, sizeof(T), d.ep[0], g, 1, bx + 8, TT_Y + 4) &&
-                      encode_map(&h_maps[4], ft, sizeof(T), d.ep[1], g, 1, bx + 8, TT_Y + 4) &&
+                      encode_map(&h_maps[3], ft, sizeof(T), m3, g, 1, bx + 8, my, mz) &&
+                      encode_map(&h_maps[4], ft, sizeof(T), m4, g, 1, bx + 8, my, mz) &&
                       encode_map(&h_maps[5], ft, sizeof(T), Jt, g, 1, bx, TT_Y) &&
                       encode_map(&h_maps[6], CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, g, 1, bx, TT_Y);
             if (!ok) DTB_FAIL(DTB_ERR_CUDA, "cannot encode the TMA descriptors (cuTensorMapEncodeTiled)");
@@ -663,8 +669,13 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
             d.tm_field[0] = d_maps[i] + 0;
             d.tm_field[1] = d_maps[i] + 1;
             d.tm_grad = d_maps[i] + 2;
-            d.tm_ep[0] = d_maps[i] + 3;
-            d.tm_ep[1] = d_maps[i] + 4;
+            if (gradient) {
+                d.tm_ep[0] = d_maps[i] + 3;
+                d.tm_ep[1] = d_maps[i] + 4;
+            } else {
+                d.tm_v[0] = d_maps[i] + 3;
+                d.tm_v[1] = d_maps[i] + 4;
+            }
             d.tm_Jt = d_maps[i] + 5;
             d.tm_mask = d_maps[i] + 6;
         }
@@ -684,13 +695,13 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
 
 
     // Persistent grids: as many blocks as fit on the device at once.
-    const int grid_t = gradient ? std::min(total_tiles, std::max(1, trial_tma_blocks_per_sm<T>(tile_x, trial_ty)) * num_sms())
-                                : total_tiles;
+    const int bps_t = gradient ? trial_tma_blocks_per_sm<T>(tile_x, trial_ty) : greedy_tma_blocks_per_sm<T>();
+    const int grid_t = std::min(total_tiles, std::max(1, bps_t) * num_sms());
     const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms());
     auto launch_t = [&](unsigned char *flag) -> cudaError_t {
         if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, trial_ty,
                                                     d_queues, cfg.pf);
-        return launch_trial<T>(MODE_GREEDY, d_desc, d_tile_vol, total_tiles, grid_t, stream, flag);
+        return launch_greedy_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, d_queues);
     };
     auto launch_g = [&](unsigned char *flag) -> cudaError_t {
         return launch_gradient_tma<T>(d_desc, d_tile_vol, total_tiles, grid_g, stream, flag, tile_x, threads_y,

@@ -94,10 +94,12 @@ struct VolumeDesc {
     T *v[2];                 // greedy: error maps
     T *jout;                 // jacobian-only launches: output map
     T *ep[2];                // gradient method: regularised error e' of field[i]
-    // TMA descriptors (device memory) of field[0..1], grad, ep[0..1], Jt, mask
+    // TMA descriptors (device memory) of field[0..1], grad, ep[0..1] or
+    // v[0..1] (three-plane boxes), Jt, mask
     const CUtensorMap *tm_field[2];
     const CUtensorMap *tm_grad;
     const CUtensorMap *tm_ep[2];
+    const CUtensorMap *tm_v[2];
     const CUtensorMap *tm_Jt;
     const CUtensorMap *tm_mask;
     SolverState *st;
@@ -149,6 +151,12 @@ template <typename T>
 int trial_tma_blocks_per_sm(int tile_x, int threads_y);
 template <typename T>
 int gradient_tma_blocks_per_sm(int tile_x, int threads_y);
+// TMA trial kernel of the greedy method (tiles 32 x TT_Y).
+template <typename T>
+cudaError_t launch_greedy_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                              cudaStream_t s, unsigned char *work_flag, TileQueue *queue);
+template <typename T>
+int greedy_tma_blocks_per_sm();
 template <typename T>
 cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s);
 template <typename T>

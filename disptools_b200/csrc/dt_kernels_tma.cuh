@@ -1,4 +1,4 @@
-// TMA-pipelined kernels of the gradient method (sm_100a).
+// TMA-pipelined kernels of the solvers (sm_100a).
 //
 // Both kernels march a TXW x TT_Y tile through its z range.  One elected thread streams one box per input per plane into a ring
 // of shared-memory stages with cp.async.bulk.tensor, completion tracked by an
@@ -13,7 +13,9 @@
 //                 in registers for the z differences, so shared memory holds
 //                 three candidate planes.  Jacobian, masked error, regularised
 //                 error e' per voxel; FP64 partials and the on-device step
-//                 control in the last tile.
+//                 control in the last tile.  Instantiated with GREEDY, it is
+//                 the greedy method's trial (error-map update, error map
+//                 stored instead of e').
 // k_gradient_tma  g = sum_k +-ih_k (P_ik(p - e_k) - P_ik(p + e_k)) with
 //                 P_ik = e' * minor_ik(I + grad u) (second-order central
 //                 differences, src/displacement_field_gradient.c:26-145),
@@ -36,7 +38,7 @@ struct Box {
     static constexpr int PLANE = TMA_PY * PX;  // elements of one component plane
 };
 
-template <typename T, int TXW>
+template <typename T, int TXW, bool GREEDY = false>
 struct TrialTmaLayout {
     static constexpr int TMA_PX = Box<TXW>::PX;
     static constexpr int TMA_PLANE = Box<TXW>::PLANE;
@@ -46,9 +48,18 @@ struct TrialTmaLayout {
     // against the current stencil reads.
     static constexpr int R = 4;
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
+    // Greedy method: the error map box of planes q-1, q, q+1, one row wider
+    // on each y side than the field box (the update reads v(p +- e_k)).
+    static constexpr int VPY = TMA_PY + 2;
+    static constexpr int V_PLANE = VPY * TMA_PX;
+    static constexpr int V3_BYTES = 3 * V_PLANE * (int) sizeof(T);
+    static constexpr int G_BYTES = GREEDY ? (V3_BYTES + 127) / 128 * 128 : U_BYTES;  // g or the v box
     static constexpr int JT_BYTES = TXW * TT_Y * (int) sizeof(T);
     static constexpr int MASK_BYTES = TXW * TT_Y;
-    static constexpr int STAGE_BYTES = 2 * U_BYTES + JT_BYTES + MASK_BYTES;  // u, g, Jt, mask
+    static constexpr int JT_OFF = U_BYTES + G_BYTES;
+    static constexpr int MASK_OFF = JT_OFF + JT_BYTES;
+    static constexpr int STAGE_BYTES = MASK_OFF + MASK_BYTES;  // u, g (or v), Jt, mask
+    static_assert(STAGE_BYTES % 128 == 0, "stages stay 128-byte aligned");
     static constexpr int RING_OFF = S * STAGE_BYTES;
     static constexpr int BAR_OFF = RING_OFF + R * U_BYTES;
     static constexpr int BYTES = BAR_OFF + S * 8;
@@ -139,6 +150,131 @@ __device__ __forceinline__ void st_pair(T *p, T a, T b) {
     *reinterpret_cast<typename PairOf<T>::type *>(p) = v;
 }
 
+// 16 bytes of consecutive elements.
+template <typename T>
+using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+
+// Greedy candidate of plane q over the field box `ub`, written to `out`
+// (both [3][TMA_PY][PX]):
+// * interior voxels: u + dd_k (v(p + e_k) - v(p - e_k))
+//   (src/displacement_field_greedy.c:30-63, same operation order);
+// * other voxels of the volume: the new field buffer's own content, which
+//   greedy_prefetch_stale has already copied into `out` (the caller waits
+//   for its own copies first);
+// * outside the volume: 0 (the field box arrives zero-filled there).
+// `vb` is the error map box: planes q-1, q, q+1 of rows y0-3 .. y0+TT_Y+2,
+// columns as in the field box.  A thread forms the three components of one
+// 16-byte run of x; a run whose voxels are all interior takes vector reads,
+// the others go voxel by voxel.  The box's first and last columns lack an x
+// neighbour; no stencil reads them, so they are formed from a clamped one.
+template <typename T, typename L>
+__device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, int tid, int nth, const Geom &g,
+                                            int x0, int y0, int q, double eta) {
+    using V4 = Vec16<T>;
+    constexpr int VEC = 16 / (int) sizeof(T);
+    constexpr int PX = L::TMA_PX, VP = L::V_PLANE, UP = L::TMA_PLANE;
+    constexpr int CPR = PX / VEC, NPOS = TMA_PY * CPR;  // runs per row, per plane
+    static_assert(PX % VEC == 0, "rows split in whole runs");
+    const bool q_in = q >= 1 && q <= g.nz - 2;
+    const bool q_vol = q >= 0 && q < g.nz;
+    auto ld = [](const T *p) { return *reinterpret_cast<const V4 *>(p); };
+    auto el = [](const V4 &v, int e) { return reinterpret_cast<const T *>(&v)[e]; };
+    for (int i = tid; i < NPOS; i += nth) {
+        const int ly = i / CPR;
+        const int lxc = (i - ly * CPR) * VEC;
+        const int gy = y0 - TMA_HY + ly, gx = x0 - TMA_HX + lxc;
+        const int o = ly * PX + lxc;                  // run offset in a field-box plane
+        const T *vp = vb + VP + (ly + 1) * PX + lxc;  // v at the run's voxels
+        // src/displacement_field_greedy.c:36-38
+        const T dd0 = (T) (eta * g.sp[0] * .5), dd1 = (T) (eta * g.sp[1] * .5), dd2 = (T) (eta * g.sp[2] * .5);
+        const bool row_in = q_in && gy >= 1 && gy <= g.ny - 2;
+        if (row_in && gx >= 1 && gx + VEC - 1 <= g.nx - 2) {
+            // One component at a time keeps few vectors live.
+#pragma unroll 1
+            for (int c = 0; c < 3; ++c) {
+                T hi[VEC], lo[VEC];
+                if (c == 0) {
+                    const V4 cur = ld(vp);
+                    const V4 prv = lxc >= VEC ? ld(vp - VEC) : cur;
+                    const V4 nxt = lxc + VEC < PX ? ld(vp + VEC) : cur;
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) {
+                        hi[e] = e + 1 < VEC ? el(cur, e + 1) : el(nxt, 0);
+                        lo[e] = e > 0 ? el(cur, e - 1) : el(prv, VEC - 1);
+                    }
+                } else {
+                    const int step = c == 1 ? PX : VP;
+                    const V4 h = ld(vp + step), l = ld(vp - step);
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) {
+                        hi[e] = el(h, e);
+                        lo[e] = el(l, e);
+                    }
+                }
+                const T ddc = c == 0 ? dd0 : (c == 1 ? dd1 : dd2);
+                V4 a = ld(ub + c * UP + o);
+                T *pa = reinterpret_cast<T *>(&a);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) pa[e] = pa[e] + ddc * (hi[e] - lo[e]);
+                *reinterpret_cast<V4 *>(out + c * UP + o) = a;
+            }
+        } else {
+            // Voxel by voxel, straight between the shared-memory boxes.
+            const bool yz_vol = q_vol && gy >= 0 && gy < g.ny;
+#pragma unroll 1
+            for (int c = 0; c < 3; ++c) {
+                const T ddc = c == 0 ? dd0 : (c == 1 ? dd1 : dd2);
+                const int step = c == 0 ? 1 : (c == 1 ? PX : VP);  // neighbour offset along e_c in the box
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) {
+                    const int x = gx + e;
+                    if (!(yz_vol && x >= 0 && x < g.nx)) {
+                        out[c * UP + o + e] = ub[c * UP + o + e];
+                    } else if (row_in && x >= 1 && x <= g.nx - 2) {
+                        const int lx = lxc + e;
+                        const int up = c == 0 ? (lx + 1 < PX ? 1 : 0) : step;
+                        const int dn = c == 0 ? (lx > 0 ? 1 : 0) : step;
+                        out[c * UP + o + e] = ub[c * UP + o + e] + ddc * (vp[e + up] - vp[e - dn]);
+                    }  // else: the prefetched stale value stays
+                }
+            }
+        }
+    }
+}
+
+// Copies, for the runs greedy_form gives this thread, the new field
+// buffer's content at the volume's boundary voxels of plane q into `out` (the
+// candidate plane q's ring slot), asynchronously: issued one plane ahead, the
+// loads overlap the current plane's work.  Boundary voxels are never written
+// by the greedy update, so `dst` holds constant values there.
+template <typename T, typename L>
+__device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, const Geom &g, int x0, int y0, int q,
+                                                      const T *dst) {
+    constexpr int VEC = 16 / (int) sizeof(T);
+    constexpr int PX = L::TMA_PX, UP = L::TMA_PLANE;
+    constexpr int CPR = PX / VEC, NPOS = TMA_PY * CPR;
+    if (q < 0 || q >= g.nz) return;
+    const bool q_in = q >= 1 && q <= g.nz - 2;
+    for (int i = tid; i < NPOS; i += nth) {
+        const int ly = i / CPR;
+        const int lxc = (i - ly * CPR) * VEC;
+        const int gy = y0 - TMA_HY + ly, gx = x0 - TMA_HX + lxc;
+        if (gy < 0 || gy >= g.ny) continue;
+        const bool row_in = q_in && gy >= 1 && gy <= g.ny - 2;
+        if (row_in && gx >= 1 && gx + VEC - 1 <= g.nx - 2) continue;  // all interior
+        const int o = ly * PX + lxc;
+        const T *drow = dst + (long long) q * g.zs + (long long) gy * g.ys + gx;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+            const int x = gx + e;
+            if (x < 0 || x >= g.nx || (row_in && x >= 1 && x <= g.nx - 2)) continue;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) cp_async_elem<(int) sizeof(T)>(out + c * UP + o + e, drow + c * g.cs + e);
+        }
+    }
+    cp_async_commit();
+}
+
 // Block of TXW / 2 x TYT threads; each thread owns two adjacent columns
 // (x, x + 1) of TT_Y / TYT rows of the tile, so every shared-memory read of
 // the stencil and every global store covers two voxels.  A warp spans the
@@ -146,11 +282,17 @@ __device__ __forceinline__ void st_pair(T *p, T a, T b) {
 // below uniform across a warp except on rows near the y ends.  Two resident
 // blocks per SM for FP32 (shared memory allows no more), one for FP64; the
 // bound caps the registers accordingly.
-template <typename T, int TXW, int TYT>
+//
+// GREEDY instantiates the greedy method's trial (src/displacement_field_greedy.c:
+// 23-67): the candidate is u + (eta d_k / 2) (v(p + e_k) - v(p - e_k)) on
+// interior voxels, v the error map of the accepted field, streamed as one box
+// of three planes per candidate plane; voxels on the volume boundary keep the
+// content of the new field buffer, and the stored map is the error itself.
+template <typename T, int TXW, int TYT, bool GREEDY = false>
 __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof(T) == 4) ? 2 : 1)
     k_trial_tma(const VolumeDesc<T> *__restrict__ vols, const int *__restrict__ tile_vol, int total_tiles,
                 unsigned char *__restrict__ work_flag, TileQueue *queue, int pf) {
-    using L = TrialTmaLayout<T, TXW>;
+    using L = TrialTmaLayout<T, TXW, GREEDY>;
     constexpr int TPX = TXW / 2, NTH = TPX * TYT, RYT = TT_Y / TYT;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
     static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
@@ -180,6 +322,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const Geom g = V.g;
         const int phase = ldcg_int(&st->phase);
         const int old_b = ldcg_int(&st->old_buf);
+        const int v_cur = GREEDY ? ldcg_int(&st->v_cur) : 0;
         const double eta = __ldcg(&st->eta);
         const bool trial = phase != PH_EVAL0;
         const int lt = tile - V.tile_begin;
@@ -188,9 +331,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const int z1 = min(z0 + V.bz, g.nz);
         const int n_it = z1 - z0 + 4;  // candidate planes z0-2 .. z1+1
         const CUtensorMap *tm_u = V.tm_field[old_b];
-        const CUtensorMap *tm_g = V.tm_grad;
+        const CUtensorMap *tm_g = GREEDY ? V.tm_v[v_cur] : V.tm_grad;
         T *dst = V.field[old_b ^ 1];
-        T *ep_out = V.ep[trial ? old_b ^ 1 : old_b];
+        // Gradient method: e' of the evaluated field; greedy: its error map.
+        T *ep_out = GREEDY ? V.v[trial ? v_cur ^ 1 : v_cur] : V.ep[trial ? old_b ^ 1 : old_b];
         const T eta_t = (T) eta;
         const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
         const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
@@ -206,14 +350,19 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             unsigned char *sb = smem + s * L::STAGE_BYTES;
             const int q = z0 - 2 + j, ze = q - 2;
             const bool with_target = ze >= z0 && ze < z1;
-            const uint32_t bytes =
-                L::U_BYTES + (trial ? L::U_BYTES : 0) + (with_target ? L::JT_BYTES + L::MASK_BYTES : 0);
+            const uint32_t bytes = L::U_BYTES + (trial ? (GREEDY ? L::V3_BYTES : L::U_BYTES) : 0) +
+                                   (with_target ? L::JT_BYTES + L::MASK_BYTES : 0);
             mbar_arrive_expect_tx(&bars[s], bytes);
             tma_load_4d(sb, tm_u, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
-            if (trial) tma_load_4d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
+            if (trial) {
+                if (GREEDY)
+                    tma_load_3d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY - 1, q - 1);
+                else
+                    tma_load_4d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
+            }
             if (with_target) {
-                tma_load_3d(sb + 2 * L::U_BYTES, V.tm_Jt, &bars[s], x0, y0, ze);
-                tma_load_3d(sb + 2 * L::U_BYTES + L::JT_BYTES, V.tm_mask, &bars[s], x0, y0, ze);
+                tma_load_3d(sb + L::JT_OFF, V.tm_Jt, &bars[s], x0, y0, ze);
+                tma_load_3d(sb + L::MASK_OFF, V.tm_mask, &bars[s], x0, y0, ze);
             }
             // Warm L2 with the boxes of iteration j + pf.
             if (pf > 0 && j + pf < n_it) {
@@ -253,6 +402,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         bool failed = false;
         int fail_it = 0;
         long long qoff = (long long) (z0 - 2) * g.zs;  // offset of plane q
+        // Greedy trial: stale boundary values of the first candidate plane
+        // (its ring slot is free: the tile queue's barrier has passed).
+        if (GREEDY && trial)
+            greedy_prefetch_stale<T, L>(ring + (size_t) ((z0 - 2) & (L::R - 1)) * 3 * TMA_PLANE, tid, NTH, g, x0, y0,
+                                        z0 - 2, dst);
         for (int it = 0; it < n_it; ++it, qoff += g.zs) {
             const uint32_t k = kbase + it;
             const int s = k % L::S;
@@ -271,6 +425,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 const V4 *u4 = reinterpret_cast<const V4 *>(sb);
                 const V4 *g4 = reinterpret_cast<const V4 *>(sb + L::U_BYTES);
                 V4 *c4 = reinterpret_cast<V4 *>(slot);
+                if (GREEDY && trial) {
+                    cp_async_wait_all();  // this thread's stale values of plane q
+                    greedy_form<T, L>(reinterpret_cast<const T *>(sb), reinterpret_cast<const T *>(sb + L::U_BYTES),
+                                      slot, tid, NTH, g, x0, y0, q, eta);
+                } else
                 for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NTH) {
                     V4 a = u4[i];
                     if (trial) {
@@ -292,9 +451,8 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 msk[r][0] = msk[r][1] = false;
                 if (eval && ok) {
                     const int o = (ty + r * TYT) * TXW + 2 * tx;
-                    const auto j2 = ld_pair(reinterpret_cast<const T *>(sb + 2 * L::U_BYTES) + o);
-                    const unsigned short m2 =
-                        *reinterpret_cast<const unsigned short *>(sb + 2 * L::U_BYTES + L::JT_BYTES + o);
+                    const auto j2 = ld_pair(reinterpret_cast<const T *>(sb + L::JT_OFF) + o);
+                    const unsigned short m2 = *reinterpret_cast<const unsigned short *>(sb + L::MASK_OFF + o);
                     jt[r][0] = j2.x;
                     jt[r][1] = j2.y;
                     msk[r][0] = (m2 & 0xffu) != 0;
@@ -308,6 +466,12 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 break;
             }
             if (tid == 0 && it + L::S < n_it) issue(it + L::S);
+            // Greedy trial: stale boundary values of plane q+1, into its ring
+            // slot, which held plane q-3: every warp has finished reading it
+            // (the stencil of the previous iteration) at the barrier above.
+            if (GREEDY && trial && it + 1 < n_it)
+                greedy_prefetch_stale<T, L>(ring + (size_t) ((q + 1) & (L::R - 1)) * 3 * TMA_PLANE, tid, NTH, g, x0,
+                                            y0, q + 1, dst);
             // Shift the own-column queues by plane q; store the candidate.
 #pragma unroll
             for (int r = 0; r < RYT; ++r) {
@@ -368,7 +532,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                         const T av = fabs(vv);  // the maximum is exact in the element type
                         if (msk[r][v] && av > acc_mt) acc_mt = av;
                         T ep = vv;
-                        if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
+                        if (!GREEDY && J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
                         epv[v] = ep;
                     };
                     if (row_in && tile_x_in) {
@@ -457,6 +621,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             }
         }
         if (failed) {
+            if (GREEDY) cp_async_wait_all();  // no element copy lands after the block has left
             if (tid == 0) tma_fault<L::S>(st, bars, kbase, fail_it + 1, issued_n);
             __syncthreads();
             return;
@@ -778,6 +943,19 @@ cudaError_t launch_trial_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, i
 }
 
 template <typename T, int TXW, int TYT>
+cudaError_t launch_greedy_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                                cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
+    constexpr int smem = TrialTmaLayout<T, TXW, true>::BYTES + 128;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr != cudaSuccess) return attr;
+    k_trial_tma<T, TXW, TYT, true><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag,
+                                                                           queue, 0);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, int TXW, int TYT>
 cudaError_t launch_gradient_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                   cudaStream_t s, unsigned char *work_flag, TileQueue *queue, int pf) {
     constexpr int smem = GradTmaLayout<T, TXW>::BYTES + 128;
@@ -798,6 +976,18 @@ int trial_blocks_v() {
                              TrialTmaLayout<T, TXW>::BYTES + 128);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T, TXW, TYT>, TXW / 2 * TYT,
                                                       TrialTmaLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return n;
+}
+template <typename T, int TXW, int TYT>
+int greedy_blocks_v() {
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TrialTmaLayout<T, TXW, true>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_tma<T, TXW, TYT, true>, TXW / 2 * TYT,
+                                                      TrialTmaLayout<T, TXW, true>::BYTES + 128);
         return v;
     }();
     return n;
@@ -848,6 +1038,17 @@ cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, 
     return launch_gradient_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
 }
 
+// Greedy trial: tile 32 x TT_Y, 16 x 16 threads.
+template <typename T>
+cudaError_t launch_greedy_tma(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                              cudaStream_t s, unsigned char *work_flag, TileQueue *q) {
+    return launch_greedy_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+}
+template <typename T>
+int greedy_tma_blocks_per_sm() {
+    return greedy_blocks_v<T, 32, 16>();
+}
+
 template <typename T>
 int trial_tma_blocks_per_sm(int tile_x, int threads_y) {
     if constexpr (sizeof(T) == 4)
@@ -867,6 +1068,9 @@ int gradient_tma_blocks_per_sm(int tile_x, int threads_y) {
     template cudaError_t launch_gradient_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t, \
                                                 unsigned char *, int, int, TileQueue *, int);               \
     template int trial_tma_blocks_per_sm<T>(int, int);                                                      \
+    template cudaError_t launch_greedy_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,   \
+                                              unsigned char *, TileQueue *);                                \
+    template int greedy_tma_blocks_per_sm<T>();                                                             \
     template int gradient_tma_blocks_per_sm<T>(int, int);
 
 }  // namespace dtb

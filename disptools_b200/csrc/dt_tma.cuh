@@ -80,6 +80,18 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// Per-thread asynchronous copy of one 4- or 8-byte element from global to
+// shared memory (cp.async, L1-allocating), grouped by commit and awaited by
+// the issuing thread only.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void *dst_smem, const void *src) {
+    static_assert(BYTES == 4 || BYTES == 8, "element copies of 4 or 8 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst_smem)), "l"(src), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // L2 prefetch of a tiled box (no shared memory, no completion to track):
 // warms L2 for a load issued later.  Same coordinate rules as the loads.
 __device__ __forceinline__ void tma_prefetch_3d(const CUtensorMap *map, int x, int y, int z) {

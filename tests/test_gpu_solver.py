@@ -113,6 +113,34 @@ def test_edge_cases_fp64_vs_oracle(oracle, name, algorithm):
     assert np.max(np.abs(out - ref)) <= 1e-10
 
 
+@pytest.mark.parametrize("shape", [(37, 45, 70), (70, 18, 33), (9, 40, 131)])
+def test_greedy_multi_tile_fp64_vs_oracle(oracle, shape):
+    """Greedy trials over several tiles along every axis, x extents that end
+    inside a 16-byte chunk, anisotropic spacing: bit-level agreement."""
+    rng = np.random.default_rng(sum(shape))
+    Jt = np.ascontiguousarray(1.0 + 0.08 * rng.standard_normal(shape))
+    mask = np.ascontiguousarray(rng.random(shape) < 0.5)
+    f0 = rng.normal(scale=0.02, size=(3,) + shape)
+    sp = (0.9, 1.1, 1.3)
+    ref, so = oracle.solve("greedy", Jt, mask, field=f0, spacing=sp, it_max=25)
+    out, st = dt.solve(Jt, mask, f0, spacing=sp, algorithm="greedy", precision="fp64", it_max=25)
+    assert st["reason"] == so.reason and st["iterations"] == so.iterations, (st, so)
+    assert st["trials"] == so.trials
+    assert np.max(np.abs(out - ref)) <= 1e-12
+
+
+def test_greedy_mixed_tracks_fp64():
+    shape = (37, 45, 70)
+    rng = np.random.default_rng(5)
+    Jt = np.ascontiguousarray(1.0 + 0.08 * rng.standard_normal(shape))
+    mask = np.ascontiguousarray(rng.random(shape) < 0.5)
+    f64, s64 = dt.solve(Jt, mask, algorithm="greedy", precision="fp64", it_max=25)
+    f32, s32 = dt.solve(Jt, mask, algorithm="greedy", precision="mixed", it_max=25)
+    assert s32["iterations"] == s64["iterations"]
+    assert np.max(np.abs(f32 - f64)) <= 1e-4
+    assert s32["error"] == pytest.approx(s64["error"], rel=1e-3)
+
+
 def test_device_tensor_solve_matches_host():
     import torch
     from disptools_b200 import torch_ops
