@@ -164,12 +164,13 @@ using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 // * outside the volume: 0 (the field box arrives zero-filled there).
 // `vb` is the error map box: planes q-1, q, q+1 of rows y0-3 .. y0+TT_Y+2,
 // columns as in the field box.  A thread forms the three components of one
-// 16-byte run of x; a run whose voxels are all interior takes vector reads,
-// the others go voxel by voxel.  The box's first and last columns lack an x
-// neighbour; no stencil reads them, so they are formed from a clamped one.
+// 16-byte run of x with vector reads; a run that is not all interior picks
+// each voxel's value by its class.  Values formed at non-interior voxels
+// (from zero-filled or clamped neighbours) are discarded.  The box's first
+// and last columns lack an x neighbour; no stencil reads them.
 template <typename T, typename L>
 __device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, int tid, int nth, const Geom &g,
-                                            int x0, int y0, int q, double eta) {
+                                            int x0, int y0, int q, const T *dd) {
     using V4 = Vec16<T>;
     constexpr int VEC = 16 / (int) sizeof(T);
     constexpr int PX = L::TMA_PX, VP = L::V_PLANE, UP = L::TMA_PLANE;
@@ -185,59 +186,58 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, in
         const int gy = y0 - TMA_HY + ly, gx = x0 - TMA_HX + lxc;
         const int o = ly * PX + lxc;                  // run offset in a field-box plane
         const T *vp = vb + VP + (ly + 1) * PX + lxc;  // v at the run's voxels
-        // src/displacement_field_greedy.c:36-38
-        const T dd0 = (T) (eta * g.sp[0] * .5), dd1 = (T) (eta * g.sp[1] * .5), dd2 = (T) (eta * g.sp[2] * .5);
         const bool row_in = q_in && gy >= 1 && gy <= g.ny - 2;
-        if (row_in && gx >= 1 && gx + VEC - 1 <= g.nx - 2) {
-            // One component at a time keeps few vectors live.
-#pragma unroll 1
-            for (int c = 0; c < 3; ++c) {
-                T hi[VEC], lo[VEC];
-                if (c == 0) {
-                    const V4 cur = ld(vp);
-                    const V4 prv = lxc >= VEC ? ld(vp - VEC) : cur;
-                    const V4 nxt = lxc + VEC < PX ? ld(vp + VEC) : cur;
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) {
-                        hi[e] = e + 1 < VEC ? el(cur, e + 1) : el(nxt, 0);
-                        lo[e] = e > 0 ? el(cur, e - 1) : el(prv, VEC - 1);
-                    }
-                } else {
-                    const int step = c == 1 ? PX : VP;
-                    const V4 h = ld(vp + step), l = ld(vp - step);
-#pragma unroll
-                    for (int e = 0; e < VEC; ++e) {
-                        hi[e] = el(h, e);
-                        lo[e] = el(l, e);
-                    }
-                }
-                const T ddc = c == 0 ? dd0 : (c == 1 ? dd1 : dd2);
-                V4 a = ld(ub + c * UP + o);
-                T *pa = reinterpret_cast<T *>(&a);
-#pragma unroll
-                for (int e = 0; e < VEC; ++e) pa[e] = pa[e] + ddc * (hi[e] - lo[e]);
-                *reinterpret_cast<V4 *>(out + c * UP + o) = a;
-            }
-        } else {
-            // Voxel by voxel, straight between the shared-memory boxes.
+        const bool all_in = row_in && gx >= 1 && gx + VEC - 1 <= g.nx - 2;
+        // Classes of the run's voxels: formed (interior) or kept (the
+        // prefetched stale value); the others keep the zero of the box.
+        unsigned formed_m = 0, keep_m = 0;
+        if (!all_in) {
             const bool yz_vol = q_vol && gy >= 0 && gy < g.ny;
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) {
+                const int x = gx + e;
+                const bool interior = row_in && x >= 1 && x <= g.nx - 2;
+                formed_m |= (unsigned) interior << e;
+                keep_m |= (unsigned) (yz_vol && x >= 0 && x < g.nx && !interior) << e;
+            }
+        }
+        // One component at a time keeps few vectors live.
 #pragma unroll 1
-            for (int c = 0; c < 3; ++c) {
-                const T ddc = c == 0 ? dd0 : (c == 1 ? dd1 : dd2);
-                const int step = c == 0 ? 1 : (c == 1 ? PX : VP);  // neighbour offset along e_c in the box
+        for (int c = 0; c < 3; ++c) {
+            T hi[VEC], lo[VEC];
+            if (c == 0) {
+                const V4 cur = ld(vp);
+                const V4 prv = lxc >= VEC ? ld(vp - VEC) : cur;
+                const V4 nxt = lxc + VEC < PX ? ld(vp + VEC) : cur;
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
-                    const int x = gx + e;
-                    if (!(yz_vol && x >= 0 && x < g.nx)) {
-                        out[c * UP + o + e] = ub[c * UP + o + e];
-                    } else if (row_in && x >= 1 && x <= g.nx - 2) {
-                        const int lx = lxc + e;
-                        const int up = c == 0 ? (lx + 1 < PX ? 1 : 0) : step;
-                        const int dn = c == 0 ? (lx > 0 ? 1 : 0) : step;
-                        out[c * UP + o + e] = ub[c * UP + o + e] + ddc * (vp[e + up] - vp[e - dn]);
-                    }  // else: the prefetched stale value stays
+                    hi[e] = e + 1 < VEC ? el(cur, e + 1) : el(nxt, 0);
+                    lo[e] = e > 0 ? el(cur, e - 1) : el(prv, VEC - 1);
+                }
+            } else {
+                const int step = c == 1 ? PX : VP;
+                const V4 h = ld(vp + step), l = ld(vp - step);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) {
+                    hi[e] = el(h, e);
+                    lo[e] = el(l, e);
                 }
             }
+            const T ddc = dd[c];
+            V4 a = ld(ub + c * UP + o);
+            T *pa = reinterpret_cast<T *>(&a);
+            if (all_in) {
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) pa[e] = pa[e] + ddc * (hi[e] - lo[e]);
+            } else {
+                const V4 old = ld(out + c * UP + o);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) {
+                    const T f = pa[e] + ddc * (hi[e] - lo[e]);
+                    pa[e] = (formed_m >> e) & 1u ? f : ((keep_m >> e) & 1u ? el(old, e) : pa[e]);
+                }
+            }
+            *reinterpret_cast<V4 *>(out + c * UP + o) = a;
         }
     }
 }
@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     T *ring = reinterpret_cast<T *>(smem + L::RING_OFF);
     __shared__ double red[2 * (NTH / 32)];
     __shared__ int s_flag, s_fault;
+    __shared__ T s_dd[3];  // greedy steps of the current tile
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
     if (tid == 0) {
@@ -336,6 +337,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         // Gradient method: e' of the evaluated field; greedy: its error map.
         T *ep_out = GREEDY ? V.v[trial ? v_cur ^ 1 : v_cur] : V.ep[trial ? old_b ^ 1 : old_b];
         const T eta_t = (T) eta;
+        if (GREEDY) {
+            // Greedy steps along x, y, z (src/displacement_field_greedy.c:36-38).
+            if (tid < 3) s_dd[tid] = (T) (eta * V.g.sp[tid] * .5);  // V.g: no local copy indexed
+            __syncthreads();
+        }
         const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
         const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
 
@@ -428,7 +434,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 if (GREEDY && trial) {
                     cp_async_wait_all();  // this thread's stale values of plane q
                     greedy_form<T, L>(reinterpret_cast<const T *>(sb), reinterpret_cast<const T *>(sb + L::U_BYTES),
-                                      slot, tid, NTH, g, x0, y0, q, eta);
+                                      slot, tid, NTH, g, x0, y0, q, s_dd);
                 } else
                 for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NTH) {
                     V4 a = u4[i];
