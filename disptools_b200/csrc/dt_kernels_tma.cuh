@@ -201,8 +201,7 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, in
                 keep_m |= (unsigned) (yz_vol && x >= 0 && x < g.nx && !interior) << e;
             }
         }
-        // One component at a time keeps few vectors live.
-#pragma unroll 1
+#pragma unroll
         for (int c = 0; c < 3; ++c) {
             T hi[VEC], lo[VEC];
             if (c == 0) {
