@@ -1291,7 +1291,7 @@ int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
     d.bz = bz;
     DTB_CUDA(cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s));
     DTB_CUDA(cudaMemsetAsync(d_tv, 0, (size_t) ntiles * sizeof(int), s));
-    DTB_CUDA(launch_trial<T>(MODE_JAC, d_desc, d_tv, ntiles, ntiles, s));
+    DTB_CUDA(launch_jacobian<T>(d_desc, d_tv, ntiles, ntiles, s));
     // The descriptor lives in the shared workspace: finish before releasing it.
     DTB_CUDA(cudaStreamSynchronize(s));
     return DTB_OK;

@@ -117,25 +117,18 @@ struct VolumeDesc {
     unsigned wait_limit;
 };
 
-enum Mode { MODE_JAC = 0, MODE_GRAD = 1, MODE_GREEDY = 2 };
-
-// Dynamic shared memory of the kernels (bytes).
-template <typename T> constexpr int trial_smem_bytes() {
+// Dynamic shared memory of the Jacobian map kernel (bytes): a five-plane ring.
+template <typename T> constexpr int jacobian_smem_bytes() {
     return 5 * 3 * (BY + 4) * (BX + 4) * (int) sizeof(T);
-}
-template <typename T> constexpr int gradient_smem_bytes() {
-    return 5 * 3 * (BY + 6) * (BX + 6) * (int) sizeof(T) + 3 * 9 * (BY + 2) * (BX + 2) * (int) sizeof(T);
 }
 
 // Launch wrappers, instantiated for float and double in dt_kernels_*.cu.
 // `work_flag` (may be null) is set to 1 by a launch that did work for at
 // least one volume (profiling separates real launches from no-op ones).
+// Jacobian map of field[0] of each volume into its jout (tiles BX x BY).
 template <typename T>
-cudaError_t launch_trial(int mode, const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
-                         int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
-template <typename T>
-cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles,
-                            int grid, cudaStream_t s, unsigned char *work_flag = nullptr);
+cudaError_t launch_jacobian(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                            cudaStream_t s);
 // TMA kernels of the gradient method; tiles are tile_x (64 or 32) by TT_Y
 // voxels; threads_y rows of threads (8 or 16).  `pf` > 0 prefetches into L2
 // the boxes of the plane pf iterations ahead of each load.

@@ -274,32 +274,8 @@ __device__ __forceinline__ double warp_max(double v) {
     return v;
 }
 
-// Returns (sum, max) of a block of NTH threads in thread 0; `red` holds
-// 2 * NTH / 32 doubles.
-template <int NTH = NT>
-__device__ __forceinline__ double2 block_reduce(double s, double m, double *red) {
-    static_assert(NTH <= 1024 && NTH % 32 == 0, "block size");
-    const int tid = threadIdx.y * BX + threadIdx.x;
-    s = warp_sum(s);
-    m = warp_max(m);
-    if ((tid & 31) == 0) {
-        red[tid >> 5] = s;
-        red[NTH / 32 + (tid >> 5)] = m;
-    }
-    __syncthreads();
-    double2 r = make_double2(0.0, 0.0);
-    if (tid < 32) {
-        s = tid < NTH / 32 ? red[tid] : 0.0;
-        m = tid < NTH / 32 ? red[NTH / 32 + tid] : 0.0;
-        s = warp_sum(s);
-        m = warp_max(m);
-        r = make_double2(s, m);
-    }
-    __syncthreads();
-    return r;
-}
-
-// block_reduce for blocks TXW threads wide.
+// Returns (sum, max) of a block of NTH threads, TXW threads wide, in thread
+// 0; `red` holds 2 * NTH / 32 doubles.
 template <int NTH, int TXW>
 __device__ __forceinline__ double2 block_reduce_n(double s, double m, double *red) {
     static_assert(NTH <= 1024 && NTH % 32 == 0, "block size");
@@ -323,24 +299,11 @@ __device__ __forceinline__ double2 block_reduce_n(double s, double m, double *re
     return r;
 }
 
+// Counts a finished tile of a volume and returns true in every thread of the
+// block that finished its last one (blocks TXW threads wide).
 template <int TXW>
 __device__ __forceinline__ bool publish_partial_n(unsigned int *ticket, int ntiles, int *s_flag) {
     const int tid = threadIdx.y * TXW + threadIdx.x;
-    if (tid == 0) {
-        __threadfence();
-        const unsigned int t = atomicAdd(ticket, 1u);
-        *s_flag = (t == (unsigned int) (ntiles - 1));
-    }
-    __syncthreads();
-    const bool last = *s_flag;
-    if (last) __threadfence();
-    return last;
-}
-
-// Publishes a tile partial and returns true in every thread of the block
-// that finished the volume's last tile.  Thread 0 holds `mine`.
-__device__ __forceinline__ bool publish_partial(unsigned int *ticket, int ntiles, int *s_flag) {
-    const int tid = threadIdx.y * BX + threadIdx.x;
     if (tid == 0) {
         __threadfence();
         const unsigned int t = atomicAdd(ticket, 1u);
@@ -359,94 +322,41 @@ __device__ __forceinline__ T ldcg(const T *p) {
 __device__ __forceinline__ int ldcg_int(const int *p) { return __ldcg(p); }
 
 // ------------------------------------------------------------------------
-// Trial / evaluation / Jacobian kernel.
-//
-// MODE_JAC:    J = det(I + grad f) of field[0] into jout.
-// MODE_GRAD:   phase EVAL0 evaluates field[old]; otherwise the candidate
-//              field[old] - eta * grad is formed on the fly, written to
-//              field[1-old] and evaluated (the move_field + jacobian +
-//              compute_error passes of the reference, fused).
-// MODE_GREEDY: phase EVAL0 evaluates field[old] and stores its error map;
-//              otherwise the candidate field[old] + (eta d / 2) (v(x+e) -
-//              v(x-e)) on interior voxels (src/displacement_field_greedy.c:23-67;
-//              the boundary keeps the stale content of the new buffer) is
-//              written, evaluated and its error map stored.
+// Jacobian map kernel: J = det(I + grad f) of field[0] into jout
+// (src/jacobian.c:113-241), for fields in any row layout.  A block owns a
+// BX x BY tile and marches bz planes with a five-plane shared ring (halo 2).
 // ------------------------------------------------------------------------
-template <typename T, int MODE>
-__global__ void __launch_bounds__(NT) k_trial(const VolumeDesc<T> *__restrict__ vols,
-                                              const int *__restrict__ tile_vol, int total_tiles,
-                                              unsigned char *__restrict__ work_flag) {
+template <typename T>
+__global__ void __launch_bounds__(NT) k_jacobian(const VolumeDesc<T> *__restrict__ vols,
+                                                 const int *__restrict__ tile_vol, int total_tiles) {
     constexpr int H = 2, PX = BX + 2 * H, PY = BY + 2 * H, NS = 5;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Ring<T, PX, PY> ring{reinterpret_cast<T *>(smem_raw)};
-    __shared__ double red[2 * (NT / 32)];
-    __shared__ int s_flag;
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
 
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const VolumeDesc<T> &V = vols[tile_vol[tile]];
         const Geom g = V.g;
-        SolverState *st = V.st;
-        int phase = PH_EVAL0, old_b = 0, v_cur = 0;
-        double eta = 0.0;
-        if (MODE != MODE_JAC) {
-            if (ldcg_int(&st->done)) continue;
-            phase = ldcg_int(&st->phase);
-            old_b = ldcg_int(&st->old_buf);
-            v_cur = ldcg_int(&st->v_cur);
-            eta = __ldcg(&st->eta);
-        }
-        const bool trial = MODE != MODE_JAC && phase != PH_EVAL0;
         const int lt = tile - V.tile_begin;
         const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
         const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
         const int z1 = min(z0 + V.bz, g.nz);
-
-        const T *src = MODE == MODE_JAC ? V.field[0] : V.field[old_b];
-        T *dst = V.field[old_b ^ 1];
-        const T *gp = V.grad;
-        const T *vlast = V.v[v_cur];
-        T *vout = MODE == MODE_GREEDY ? V.v[trial ? v_cur ^ 1 : v_cur] : nullptr;
-        const T eta_t = (T) eta;
-        // src/displacement_field_greedy.c:36-38
-        const T dd0 = (T) (eta * g.sp[0] * .5), dd1 = (T) (eta * g.sp[1] * .5), dd2 = (T) (eta * g.sp[2] * .5);
+        const T *src = V.field[0];
         const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
-        const T tol = (T) (MODE == MODE_JAC ? 0.0 : st->tolerance);
 
-        // Fill ring slot of plane zq (tile + halo 2), forming the candidate.
+        // Fill the ring slot of plane zq (tile + halo 2; 0 outside the volume).
         auto load_plane = [&](int zq) {
             const int slot = ring_slot(zq, NS);
             const bool zin = zq >= 0 && zq < g.nz;
-            const bool zcore = zq >= z0 && zq < z1;
             for (int i = tid; i < 3 * PY * PX; i += NT) {
                 const int c = i / (PY * PX);
                 const int r = i - c * (PY * PX);
                 const int ly = r / PX, lx = r - ly * PX;
                 const int gx = x0 - H + lx, gy = y0 - H + ly;
                 T val = T(0);
-                if (zin && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny) {
-                    const long long so = (long long) zq * g.zs + (long long) gy * g.ys + gx;
-                    const long long off = c * g.cs + so;
-                    const bool core = zcore && lx >= H && lx < H + BX && ly >= H && ly < H + BY;
-                    if (!trial) {
-                        val = src[off];
-                    } else if (MODE == MODE_GRAD) {
-                        val = src[off] - eta_t * gp[off];  // src/displacement_field_gradient.c:169-171
-                        if (core) dst[off] = val;
-                    } else {
-                        const bool interior = gx >= 1 && gx < g.nx - 1 && gy >= 1 && gy < g.ny - 1 &&
-                                              zq >= 1 && zq < g.nz - 1;
-                        if (interior) {
-                            const long long stc = c == 0 ? 1 : (c == 1 ? g.ys : g.zs);
-                            const T ddc = c == 0 ? dd0 : (c == 1 ? dd1 : dd2);
-                            val = src[off] + ddc * (vlast[so + stc] - vlast[so - stc]);
-                            if (core) dst[off] = val;
-                        } else {
-                            val = dst[off];
-                        }
-                    }
-                }
+                if (zin && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
+                    val = src[c * g.cs + (long long) zq * g.zs + (long long) gy * g.ys + gx];
                 ring.at(slot, c, ly, lx) = val;
             }
         };
@@ -455,7 +365,6 @@ __global__ void __launch_bounds__(NT) k_trial(const VolumeDesc<T> *__restrict__ 
 
         const int x = x0 + tx, y = y0 + ty;
         const bool in_xy = x < g.nx && y < g.ny;
-        double acc_s = 0.0, acc_m = 0.0;
         for (int z = z0; z < z1; ++z) {
             load_plane(z + 2);
             __syncthreads();
@@ -466,201 +375,10 @@ __global__ void __launch_bounds__(NT) k_trial(const VolumeDesc<T> *__restrict__ 
                                   ring_slot(z + 1, NS), ring_slot(z + 2, NS)};
                 T a[3][3];
                 ring_matrix<T, PX, PY>(ring, s, tx + H, ty + H, k, ih, a);
-                const T J = det_i_plus<T>(a);
-                const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
-                if (MODE == MODE_JAC) {
-                    V.jout[so] = J;
-                } else {
-                    const bool m = V.mask[so] != 0;
-                    const T vv = voxel_error<T>(J, V.Jt[so], m, tol);
-                    acc_s += (double) vv * (double) vv;
-                    const double av = fabs((double) vv);
-                    if (m && av > acc_m) acc_m = av;
-                    if (MODE == MODE_GREEDY) vout[so] = vv;
-                }
+                V.jout[(long long) z * g.zs + (long long) y * g.ys + x] = det_i_plus<T>(a);
             }
             __syncthreads();
         }
-
-        if (MODE != MODE_JAC) {
-            const double2 r = block_reduce(acc_s, acc_m, red);
-            if (tid == 0) V.part_t[lt] = r;
-            if (publish_partial(&st->ticket_t, V.ntiles, &s_flag)) {
-                double s = 0.0, m = 0.0;
-                for (int i = tid; i < V.ntiles; i += NT) {
-                    const double2 p = __ldcg(&V.part_t[i]);
-                    s += p.x;
-                    m = fmax(m, p.y);
-                }
-                const double2 tot = block_reduce(s, m, red);
-                if (tid == 0) {
-                    st->ticket_t = 0;
-                    control_after_trial(st, tot.x, tot.y);
-                    if (work_flag) *work_flag = 1;
-                    __threadfence();
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// ------------------------------------------------------------------------
-// Gradient kernel (src/displacement_field_gradient.c:26-145).
-//
-// J and the error map of the accepted field are recomputed in the tile
-// (halo 3) instead of being read back, so the launch streams only the field,
-// the target map and the mask and writes the gradient.  For each plane the
-// kernel forms P[i][k](q) = e'(q) * minor_ik(M(q)) on the tile plus a halo
-// of one (e' the regularised error, M = I + grad u by second-order central
-// differences), keeps three planes of P, and takes
-//   g_i(p) = sum_k (-1)^(i+k) ih_k (P[i][k](p - e_k) - P[i][k](p + e_k)).
-// Boundary voxels of the gradient are never written (they stay zero).
-// ------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(NT) k_gradient(const VolumeDesc<T> *__restrict__ vols,
-                                                 const int *__restrict__ tile_vol, int total_tiles,
-                                                 unsigned char *__restrict__ work_flag) {
-    constexpr int HU = 3, PXU = BX + 2 * HU, PYU = BY + 2 * HU, NSU = 5;
-    constexpr int PXP = BX + 2, PYP = BY + 2, NSP = 3;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Ring<T, PXU, PYU> ur{reinterpret_cast<T *>(smem_raw)};
-    T *pr = reinterpret_cast<T *>(smem_raw) + NSU * 3 * PYU * PXU;  // [NSP][9][PYP][PXP]
-    __shared__ double red[2 * (NT / 32)];
-    __shared__ int s_flag;
-    auto P = [&](int slot, int ik, int ly, int lx) -> T & {
-        return pr[((slot * 9 + ik) * PYP + ly) * PXP + lx];
-    };
-
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * BX + tx;
-
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-        const VolumeDesc<T> &V = vols[tile_vol[tile]];
-        const Geom g = V.g;
-        SolverState *st = V.st;
-        if (ldcg_int(&st->done) || !ldcg_int(&st->need_gradient)) continue;
-        const int old_b = ldcg_int(&st->old_buf);
-        const int lt = tile - V.tile_begin;
-        const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
-        const int x0 = txi * BX, y0 = tyi * BY, z0 = tzi * V.bz;
-        const int z1 = min(z0 + V.bz, g.nz);
-        const T *u = V.field[old_b];
-        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
-        const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
-
-        auto load_plane = [&](int zq) {
-            const int slot = ring_slot(zq, NSU);
-            const bool zin = zq >= 0 && zq < g.nz;
-            for (int i = tid; i < 3 * PYU * PXU; i += NT) {
-                const int c = i / (PYU * PXU);
-                const int r = i - c * (PYU * PXU);
-                const int ly = r / PXU, lx = r - ly * PXU;
-                const int gx = x0 - HU + lx, gy = y0 - HU + ly;
-                T val = T(0);
-                if (zin && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny)
-                    val = u[c * g.cs + (long long) zq * g.zs + (long long) gy * g.ys + gx];
-                ur.at(slot, c, ly, lx) = val;
-            }
-        };
-
-        // P on plane zp over the tile plus a halo of one.
-        auto compute_p = [&](int zp) {
-            const int ps = ring_slot(zp, NSP);
-            const int s[5] = {ring_slot(zp - 2, NSU), ring_slot(zp - 1, NSU), ring_slot(zp, NSU),
-                              ring_slot(zp + 1, NSU), ring_slot(zp + 2, NSU)};
-            for (int i = tid; i < PYP * PXP; i += NT) {
-                const int ly = i / PXP, lx = i - ly * PXP;
-                const int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-                if (zp >= 0 && zp < g.nz && gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny) {
-                    const int lxu = lx + 2, lyu = ly + 2;
-                    int k[3];
-                    schemes_at(gx, gy, zp, g, k);
-                    T a[3][3];
-                    ring_matrix<T, PXU, PYU>(ur, s, lxu, lyu, k, ih, a);
-                    const T J = det_i_plus<T>(a);
-                    const long long so = (long long) zp * g.zs + (long long) gy * g.ys + gx;
-                    const T v = voxel_error<T>(J, V.Jt[so], V.mask[so] != 0, tol);
-                    T ep = v;
-                    if (J < delta) ep += zeta * (J - delta);  // :71-88
-                    // M = I + grad u, second-order central (:13-21)
-                    T m[3][3];
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        m[c][0] = fd_c2<T>(ur.at(s[2], c, lyu, lxu + 1), ur.at(s[2], c, lyu, lxu - 1), ih[0]);
-                        m[c][1] = fd_c2<T>(ur.at(s[2], c, lyu + 1, lxu), ur.at(s[2], c, lyu - 1, lxu), ih[1]);
-                        m[c][2] = fd_c2<T>(ur.at(s[3], c, lyu, lxu), ur.at(s[1], c, lyu, lxu), ih[2]);
-                        m[c][c] += T(1.0);
-                    }
-#pragma unroll
-                    for (int ii = 0; ii < 3; ++ii) {
-                        const int r0 = ii == 0 ? 1 : 0, r1 = ii == 2 ? 1 : 2;
-#pragma unroll
-                        for (int kk = 0; kk < 3; ++kk) {
-                            const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
-                            P(ps, ii * 3 + kk, ly, lx) = ep * (m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0]);
-                        }
-                    }
-                } else {
-#pragma unroll
-                    for (int ik = 0; ik < 9; ++ik) P(ps, ik, ly, lx) = T(0);
-                }
-            }
-        };
-
-        for (int zq = z0 - 3; zq < z0 + 2; ++zq) load_plane(zq);
-        __syncthreads();
-        compute_p(z0 - 1);
-        __syncthreads();
-        load_plane(z0 + 2);
-        __syncthreads();
-        compute_p(z0);
-        __syncthreads();  // the first load of the loop reuses the slot of z0 - 2
-
-        const int x = x0 + tx, y = y0 + ty;
-        const bool interior_xy = x >= 1 && x < g.nx - 1 && y >= 1 && y < g.ny - 1;
-        double acc = 0.0;
-        for (int z = z0; z < z1; ++z) {
-            load_plane(z + 3);
-            __syncthreads();
-            compute_p(z + 1);
-            __syncthreads();
-            if (interior_xy && z >= 1 && z < g.nz - 1) {
-                const int lx = tx + 1, ly = ty + 1;
-                const int sm = ring_slot(z - 1, NSP), s0 = ring_slot(z, NSP), sp = ring_slot(z + 1, NSP);
-                T t[3][3];
-#pragma unroll
-                for (int ii = 0; ii < 3; ++ii) {
-                    t[ii][0] = ih[0] * (P(s0, ii * 3 + 0, ly, lx - 1) - P(s0, ii * 3 + 0, ly, lx + 1));
-                    t[ii][1] = ih[1] * (P(s0, ii * 3 + 1, ly - 1, lx) - P(s0, ii * 3 + 1, ly + 1, lx));
-                    t[ii][2] = ih[2] * (P(sm, ii * 3 + 2, ly, lx) - P(sp, ii * 3 + 2, ly, lx));
-                }
-                const T gx = t[0][0] - t[0][1] + t[0][2];
-                const T gy = -t[1][0] + t[1][1] - t[1][2];
-                const T gz = t[2][0] - t[2][1] + t[2][2];
-                const long long so = (long long) z * g.zs + (long long) y * g.ys + x;
-                V.grad[so] = gx;
-                V.grad[g.cs + so] = gy;
-                V.grad[2 * g.cs + so] = gz;
-                acc += (double) (gx * gx + gy * gy + gz * gz);
-            }
-        }
-
-        const double2 r = block_reduce(acc, 0.0, red);
-        if (tid == 0) V.part_g[lt] = r.x;
-        if (publish_partial(&st->ticket_g, V.ntiles, &s_flag)) {
-            double s = 0.0;
-            for (int i = tid; i < V.ntiles; i += NT) s += __ldcg(&V.part_g[i]);
-            const double2 tot = block_reduce(s, 0.0, red);
-            if (tid == 0) {
-                st->ticket_g = 0;
-                st->gn2 = tot.x;
-                st->need_gradient = 0;
-                st->gradients++;
-                if (work_flag) *work_flag = 1;
-                __threadfence();
-            }
-        }
-        __syncthreads();
     }
 }
 
@@ -787,38 +505,14 @@ inline int elementwise_grid(long long n) {
 }
 
 template <typename T>
-cudaError_t launch_trial(int mode, const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                         cudaStream_t s, unsigned char *work_flag) {
-    constexpr int smem = trial_smem_bytes<T>();
-    const dim3 block(BX, BY);
-    // Opt in to the dynamic shared memory once per process (outside any
-    // stream capture: the first call of each kernel happens before capture).
-    static const cudaError_t attr = [] {
-        cudaError_t e = cudaFuncSetAttribute(k_trial<T, MODE_JAC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_trial<T, MODE_GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_trial<T, MODE_GREEDY>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        return e;
-    }();
-    if (attr != cudaSuccess) return attr;
-    switch (mode) {
-    case MODE_JAC: k_trial<T, MODE_JAC><<<grid, block, smem, s>>>(vols, tile_vol, total_tiles, work_flag); break;
-    case MODE_GRAD: k_trial<T, MODE_GRAD><<<grid, block, smem, s>>>(vols, tile_vol, total_tiles, work_flag); break;
-    default: k_trial<T, MODE_GREEDY><<<grid, block, smem, s>>>(vols, tile_vol, total_tiles, work_flag); break;
-    }
-    count_launch();
-    return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_gradient(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
-                            cudaStream_t s, unsigned char *work_flag) {
-    constexpr int smem = gradient_smem_bytes<T>();
+cudaError_t launch_jacobian(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                            cudaStream_t s) {
+    constexpr int smem = jacobian_smem_bytes<T>();
+    // Opt in to the dynamic shared memory once per process.
     static const cudaError_t attr =
-        cudaFuncSetAttribute(k_gradient<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_jacobian<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
-    k_gradient<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles, work_flag);
+    k_jacobian<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles);
     count_launch();
     return cudaGetLastError();
 }
@@ -854,10 +548,7 @@ cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s) {
 }
 
 #define DTB_INSTANTIATE(T)                                                                                   \
-    template cudaError_t launch_trial<T>(int, const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
-                                         unsigned char *);                                                   \
-    template cudaError_t launch_gradient<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,      \
-                                            unsigned char *);                                                \
+    template cudaError_t launch_jacobian<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t);     \
     template cudaError_t launch_adjoint<T>(const Geom &, const T *, const T *, T *, T *, cudaStream_t);      \
     template cudaError_t launch_convert<T>(const void *, int, T *, long long, cudaStream_t);                 \
     template cudaError_t launch_to_double<T>(const T *, double *, long long, cudaStream_t);                  \

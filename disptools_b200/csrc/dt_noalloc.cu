@@ -131,7 +131,7 @@ int jacobian_noalloc(size_t nx, size_t ny, size_t nz, double dx, double dy, doub
     // Every tile belongs to volume 0: the table must be zero, whatever the
     // previous call left there.
     if (e == cudaSuccess) e = cudaMemsetAsync(d_tile_vol, 0, (size_t) tiles * sizeof(int), s);
-    if (e == cudaSuccess) e = launch_trial<T>(MODE_JAC, d_desc, d_tile_vol, (int) tiles, (int) tiles, s, nullptr);
+    if (e == cudaSuccess) e = launch_jacobian<T>(d_desc, d_tile_vol, (int) tiles, (int) tiles, s);
     if (e != cudaSuccess) {
         cudaGetLastError();
         report(__LINE__, __func__, cudaGetErrorString(e));
