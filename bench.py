@@ -34,6 +34,10 @@ UNIT = "voxel-iters/s"
 # the gradient.
 BYTES_PER_VOXEL = {"trial": 12 + 12 + 4 + 1 + 12, "gradient": 12 + 4 + 1 + 12}
 BYTES_PER_VOXEL_FP64 = {"trial": 24 + 24 + 8 + 1 + 24, "gradient": 24 + 8 + 1 + 24}
+# Greedy method: each trial reads the field, the error map, the target map and
+# the mask and writes the candidate and its error map.
+BYTES_PER_VOXEL_GREEDY = {"trial": 12 + 4 + 4 + 1 + 12 + 4}
+METRIC_GREEDY = "greedy-method voxel-iters/s at 256³, FP32-mixed; % HBM peak"
 
 
 def parse():
@@ -47,10 +51,11 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="c2", choices=["c2", "c4", "c5"],
+    p.add_argument("--workload", default="c2", choices=["c2", "c4", "c5", "greedy"],
                    help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
                         "axes U{48..192} split over the ranks; c5: one 512x512x384 volume per "
-                        "rank through a 3-level pyramid, plus greedy on the coarsest level")
+                        "rank through a 3-level pyramid, plus greedy on the coarsest level; "
+                        "greedy: the config-2 volume solved by the greedy method")
     return p.parse_args()
 
 
@@ -162,7 +167,7 @@ def iterations_done(st) -> int:
     return int(st["iterations"] - 1 if st["reason"] == "it_max" else st["iterations"])
 
 
-def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6):
+def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6, algorithm="gradient"):
     """The reference C library (FP64, OpenMP, all host cores) on the same
     volume: per-iteration rate from two solves (it_max it_lo and it_hi), so
     set-up work cancels out."""
@@ -174,10 +179,16 @@ def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6):
     times = {}
     for it in (it_lo, it_hi):
         t0 = time.perf_counter()
-        impl.solve("gradient", Jt, mask, it_max=it)
+        impl.solve(algorithm, Jt, mask, it_max=it)
         times[it] = time.perf_counter() - t0
     n = Jt.size
-    rate = n * (it_hi - it_lo) / max(times[it_hi] - times[it_lo], 1e-9)
+    d = times[it_hi] - times[it_lo]
+    if d > 0.05 * times[it_hi]:
+        rate = n * (it_hi - it_lo) / d
+    else:
+        # The solve stopped before it_hi iterations (a small volume): the
+        # difference holds no iterations, so take the whole it_hi solve.
+        rate = n * it_hi / times[it_hi]
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     return rate, kind, cores, times
 
@@ -187,11 +198,12 @@ def run_reference_arm(args, world, rank):
         return
     from disptools_b200.synthetic import blob_problem
     n = args.size
+    algorithm = "greedy" if args.workload == "greedy" else "gradient"
     Jt, mask = blob_problem((n, n, n), blobs=16, seed=0)
     rates = []
     samples = []
     for s in range(args.warmup + args.steps):
-        rate, kind, cores, times = reference_cpu_rate(Jt, mask)
+        rate, kind, cores, times = reference_cpu_rate(Jt, mask, algorithm=algorithm)
         if s >= args.warmup:
             rates.append(rate)
             samples.append(times)
@@ -199,12 +211,12 @@ def run_reference_arm(args, world, rank):
     sample = (f"per step: reference C library (FLOAT_SIZE=64, ORDER_PD=4, OpenMP) solving the "
               f"{n}^3 volume with it_max=1 and it_max=6; rate = voxels x 5 / time difference")
     out = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC_GREEDY if algorithm == "greedy" else METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * statistics.mean(t[6] + t[1] for t in samples),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"config 2: gradient method on {n}^3, 16 Gaussian blobs",
+        "config": {"workload": f"config 2: {algorithm} method on {n}^3, 16 Gaussian blobs",
                    "size": [n, n, n]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
@@ -417,6 +429,8 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.size
+    algorithm = "greedy" if args.workload == "greedy" else "gradient"
+    bytes_per_voxel = BYTES_PER_VOXEL_GREEDY if algorithm == "greedy" else BYTES_PER_VOXEL
     Jt_np, mask_np = blob_problem((n, n, n), blobs=16, seed=rank)
     nvox = Jt_np.size
     IT = args.it_max
@@ -428,7 +442,7 @@ def main():
 
     def step():
         field.zero_()
-        return torch_ops.solve(Jt, mask, field, it_max=IT)
+        return torch_ops.solve(Jt, mask, field, algorithm=algorithm, it_max=IT)
 
     # Profiling adds event nodes to the step graphs: switch it on before the
     # warm-up so the profiled graphs are built there, not in the timed steps.
@@ -470,22 +484,25 @@ def main():
     dom = max(prof, key=lambda k: prof[k][1]) if prof else "trial"
     nl, tot_ms = prof.get(dom, (0, 0.0))
     avg_ms = tot_ms / max(nl, 1)
-    bytes_launch = BYTES_PER_VOXEL[dom] * nvox
+    bytes_launch = bytes_per_voxel[dom] * nvox
     achieved = bytes_launch / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             t = json.load(open(tpath))
-            traffic = t.get(dom, {}).get("bytes_per_launch_256")
+            traffic = t.get("greedy_trial" if algorithm == "greedy" else dom, {}).get("bytes_per_launch_256")
         except Exception:
             traffic = None
     kernels = {k: {"launches": v[0], "avg_ms": v[1] / max(v[0], 1),
-                   "achieved_gbs": BYTES_PER_VOXEL[k] * nvox / (v[1] / max(v[0], 1) / 1000.0) / 1e9
+                   "achieved_gbs": bytes_per_voxel.get(k, 0) * nvox / (v[1] / max(v[0], 1) / 1000.0) / 1e9
                    if v[0] else None,
                    "share": v[1] / max(sum(x[1] for x in prof.values()), 1e-12)}
                for k, v in prof.items()}
-    path_achieved = (29 + 41 * tbar) * value / 1e9 / world
+    # Algorithmic bytes per voxel-iteration of the whole path: a gradient pass
+    # and T trials (gradient method), or T trials (greedy method).
+    path_bpv = 37 * tbar if algorithm == "greedy" else 29 + 41 * tbar
+    path_achieved = path_bpv * value / 1e9 / world
 
     # ---- plain FP64 path (same workload, fewer steps)
     fp64 = None
@@ -493,14 +510,14 @@ def main():
         Jt64 = torch.from_numpy(Jt_np).to(dev)
         f64 = torch.zeros((3, n, n, n), dtype=torch.float64, device=dev)
         f64.zero_()
-        torch_ops.solve(Jt64, mask, f64, it_max=IT)
+        torch_ops.solve(Jt64, mask, f64, algorithm=algorithm, it_max=IT)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         it64 = 0
         k64 = max(1, min(args.steps, 2))
         for _ in range(k64):
             f64.zero_()
-            s64 = torch_ops.solve(Jt64, mask, f64, it_max=IT)
+            s64 = torch_ops.solve(Jt64, mask, f64, algorithm=algorithm, it_max=IT)
             it64 += iterations_done(s64)
         torch.cuda.synchronize()
         t64 = time.perf_counter() - t0
@@ -525,7 +542,8 @@ def main():
             zero initial guess is written before the timed call."""
             fh[...] = 0.0
             t0 = time.perf_counter()
-            rc = N.lib.dtb_generate_displacement(0, 0, n, n, n, 1.0, 1.0, 1.0, Jh.ctypes.data,
+            rc = N.lib.dtb_generate_displacement(N.algorithm_code(algorithm), 0, n, n, n, 1.0, 1.0, 1.0,
+                                                 Jh.ctypes.data,
                                                  mh.ctypes.data, C.byref(p), fh.ctypes.data,
                                                  C.byref(stt))
             dt_s = time.perf_counter() - t0
@@ -550,22 +568,26 @@ def main():
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, kind, cores, times = reference_cpu_rate(Jt_np, mask_np)
+        rate, kind, cores, times = reference_cpu_rate(Jt_np, mask_np, algorithm=algorithm)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": f"{n}^3 volume, reference C library FP64 OpenMP: solves with it_max=1 "
+               "sample": f"{n}^3 volume, reference C library FP64 OpenMP, {algorithm} method: "
+                         f"solves with it_max=1 "
                          f"({times[1]:.2f} s) and it_max=6 ({times[6]:.2f} s); "
                          f"rate = voxels x 5 / time difference"}
 
     if rank == 0:
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "metric": METRIC_GREEDY if algorithm == "greedy" else METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"config 2: gradient method on {n}^3 (16 Gaussian blobs), "
+            "config": {"workload": f"config 2: {algorithm} method on {n}^3 (16 Gaussian blobs), "
                                    f"FP32 field, FP64 reductions, zero initial field, "
                                    f"it_max={IT} per step",
                        "size": [n, n, n], "it_max_per_step": IT,
-                       "l2": "inputs larger than L2 (FP32 field 201 MB + gradient 201 MB)",
+                       "l2": "inputs larger than L2 (FP32 field 201 MB + "
+                             + ("error map 67 MB + candidate 201 MB)" if algorithm == "greedy"
+                                else "gradient 201 MB)"),
                        "iterations_per_step": iters / args.steps,
                        "trials_per_iteration": tbar, "parallelism": f"{world} independent volumes",
                        "tiles": tiles, "tiles_from": "autotuner (first solve of the shape, in warm-up)",
