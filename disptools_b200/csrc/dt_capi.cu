@@ -589,7 +589,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
         d.tile_begin = tbegin[i];
         d.ntiles = tiles[i];
         d.bz = bz;
-        d.drop_tile = (gradient && !tune_ms) ? (int) g_drop.tile : -1;
+        d.drop_tile = !tune_ms ? (int) g_drop.tile : -1;
         d.drop_it = g_drop.iteration;
         d.wait_limit = g_drop.wait_limit;
         for (int t = 0; t < tiles[i]; ++t) tile_vol[tbegin[i] + t] = i;

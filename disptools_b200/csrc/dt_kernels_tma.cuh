@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         // Issues the loads of iteration j (candidate plane z0-2+j) into its stage.
         auto issue = [&](int j) {
             issued_n = j + 1;
-            if (tile == V.drop_tile && j == V.drop_it) return;  // failure-path test only
+            if (trial && tile == V.drop_tile && j == V.drop_it) return;  // failure-path test only
             const uint32_t k = kbase + j;
             const int s = k % L::S;
             unsigned char *sb = smem + s * L::STAGE_BYTES;

@@ -373,9 +373,10 @@ int dtb_read_vtk(const char *filename, double *data, size_t capacity);
  * memory budget; the tests use it to make an allocation fail. */
 int dtb_set_device_memory_limit(size_t bytes);
 
-/* Test hook of the failure path of the gradient method: in the following
- * solves, the trial launch's tile `tile` (global tile index, -1 turns the
- * hook off) does not issue the TMA loads of its plane iteration
+/* Test hook of the failure path of both solvers' trial kernel: in the
+ * following solves, tile `tile` (global tile index, -1 turns the hook off)
+ * of every launch that evaluates a candidate (not the evaluation of the
+ * initial field) does not issue the TMA loads of its plane iteration
  * `iteration`, and every bounded wait of the trial kernel polls at most
  * `wait_limit` times.  The block's wait for the missing plane then runs
  * out: the volume is stopped with its fault flag, the block waits (bounded)
