@@ -1269,6 +1269,20 @@ namespace {
 
 template <typename T>
 int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
+    // TMA kernel: fourth order, rows a multiple of 16 bytes long, a 16-byte
+    // aligned field and pair-aligned J.  It takes its tensor map as a kernel
+    // parameter and needs no device memory of its own: no lock, no wait.
+    if (g.order == 4 && (g.ys * (long long) sizeof(T)) % 16 == 0 && reinterpret_cast<uintptr_t>(field) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(J) % (2 * sizeof(T)) == 0) {
+        CUtensorMap tm;
+        const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        if (encode_map(&tm, ft, sizeof(T), field, g, 3, 32 + 2 * 4, TT_Y + 2 * 2)) {
+            DTB_CUDA(launch_jacobian_tma<T>(tm, g, J, g.ys, g.zs, num_sms(), s));
+            return DTB_OK;
+        }
+    }
+    // Other layouts and order 2: the plain-load kernel, with its descriptor
+    // in the shared workspace.
     std::lock_guard<std::mutex> lock(g_ws_mutex);
     const int bz = bz_for(g.nz, 32);
     const int ntiles = ((g.nx + BX - 1) / BX) * ((g.ny + BY - 1) / BY) * ((g.nz + bz - 1) / bz);

@@ -150,6 +150,11 @@ cudaError_t launch_greedy_tma(const VolumeDesc<T> *vols, const int *tile_vol, in
                               cudaStream_t s, unsigned char *work_flag, TileQueue *queue);
 template <typename T>
 int greedy_tma_blocks_per_sm();
+// TMA Jacobian map of one field of order 4 (the map `tm_u` over the field
+// with box 40 x 20 x 1 x 3) into jout with element strides jys, jzs.
+template <typename T>
+cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
+                                int num_sms, cudaStream_t s);
 template <typename T>
 cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s);
 template <typename T>

@@ -22,6 +22,9 @@
 //                 from field[old] and the stored e' of that field.
 #pragma once
 
+#include <algorithm>
+#include <cmath>
+
 #include "dt_kernels.cuh"
 #include "dt_tma.cuh"
 
@@ -272,6 +275,109 @@ __device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, 
         }
     }
     cp_async_commit();
+}
+
+// The Jacobian matrices minus I of the two voxels (x, x + 1) of row y of
+// plane ze, each handed to finish(v, a) when the voxel lies in the volume.
+// `jp` is the plane's field box in shared memory ([3][TMA_PY][PX], column lx
+// holds x, row ly holds y); zq holds the two columns' values of planes
+// ze-2 .. ze+2 per component.  FP32 folds the spacing into the fourth-order
+// weights; the FP64 path keeps the reference's operation order.  Three
+// evaluators:
+// * rows and planes inside [2, n-3] of a tile whose columns all lie inside
+//   [2, nx-3] use the fourth-order stencil only;
+// * interior rows of a tile that reaches an x end select the scheme per
+//   voxel without branching;
+// * rows or planes on the two outer layers take the general path.
+// The trial kernel keeps the same evaluator inline: calling this function
+// there changes its register allocation (it then spills).
+template <typename T, int TMA_PX, int TMA_PLANE, typename F>
+__device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5], int lx, int ly, int x, int y,
+                                             int ze, const Geom &g, const T (&ih)[3], bool row_in,
+                                             bool tile_x_in, F &&finish) {
+    const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
+    const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1], FD<T>::one_twelfth * ih[2]};
+    auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
+        if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+        return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
+    };
+    if (row_in && tile_x_in) {
+        T a0[3][3], a1[3][3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+            const auto xm = ld_pair(p - 2), xc = ld_pair(p), xp = ld_pair(p + 2);
+            a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
+            a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
+            const auto ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
+            const auto ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
+            a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
+            a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+            const T *z0q = zq[0][c], *z1q = zq[1][c];
+            a0[c][2] = c4(z0q[3], z0q[1], z0q[4], z0q[0], 2);
+            a1[c][2] = c4(z1q[3], z1q[1], z1q[4], z1q[0], 2);
+        }
+        finish(0, a0);
+        finish(1, a1);
+    } else if (row_in) {
+        // Interior row: the scheme depends on x only
+        // (src/jacobian.c:113-241): outer column -> one-sided
+        // in x and second-order central in y, z; penultimate
+        // column -> second-order central; else fourth order.
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            const int xv = x + v;
+            if (xv >= g.nx) continue;
+            const bool xo_lo = xv == 0, xo_hi = xv == g.nx - 1;
+            const bool second = xo_lo || xo_hi || xv == 1 || xv == g.nx - 2;
+            T a[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx + v;
+                const T fx = xo_lo ? fd_fwd<T>(p[0], p[1], p[2], ih[0])
+                                   : (xo_hi ? fd_bwd<T>(p[0], p[-1], p[-2], ih[0])
+                                            : fd_c2<T>(p[1], p[-1], ih[0]));
+                const T cx4 = c4(p[1], p[-1], p[2], p[-2], 0);
+                a[c][0] = second ? fx : cx4;
+                const T cy4 = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
+                const T cy2 = fd_c2<T>(p[TMA_PX], p[-TMA_PX], ih[1]);
+                a[c][1] = second ? cy2 : cy4;
+                const T *zv = zq[v][c];
+                const T cz4 = c4(zv[3], zv[1], zv[4], zv[0], 2);
+                const T cz2 = fd_c2<T>(zv[3], zv[1], ih[2]);
+                a[c][2] = second ? cz2 : cz4;
+            }
+            finish(v, a);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            const int xv = x + v;
+            if (xv >= g.nx) continue;
+            int kk[3];
+            schemes_at(xv, y, ze, g, kk);
+            T a[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx + v;
+                const T vx[5] = {p[-2], p[-1], p[0], p[1], p[2]};
+                const T vy[5] = {p[-2 * TMA_PX], p[-TMA_PX], p[0], p[TMA_PX], p[2 * TMA_PX]};
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) {
+                    const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[v][c]);
+                    T d;
+                    switch (kk[ax]) {
+                    case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
+                    case S_BWD: d = fd_bwd<T>(w[2], w[1], w[0], ih[ax]); break;
+                    case S_C2: d = fd_c2<T>(w[3], w[1], ih[ax]); break;
+                    default: d = c4(w[3], w[1], w[4], w[0], ax); break;
+                    }
+                    a[c][ax] = d;
+                }
+            }
+            finish(v, a);
+        }
+    }
 }
 
 // Block of TXW / 2 x TYT threads; each thread owns two adjacent columns
@@ -1067,6 +1173,213 @@ int gradient_tma_blocks_per_sm(int tile_x, int threads_y) {
     return threads_y == 16 ? gradient_blocks_v<T, 32, 16>() : gradient_blocks_v<T, 32, 8>();
 }
 
+// ------------------------------------------------------------------------
+// Jacobian map of one field with the TMA pipeline (src/jacobian.c:70-242,
+// fourth-order interior): J = det(I + grad u) into jout.
+//
+// A block of TXW / 2 x TYT threads marches a TXW x TT_Y tile through bz
+// planes.  Field boxes (tile + 4 voxels in x, 2 rows in y, three components)
+// go straight into S shared-memory stages and stay there until their plane
+// has been the stencil's centre plane, so no candidate plane is formed.
+// Threads wait for each stage's mbarrier themselves; the block barrier only
+// guards stage reuse and is taken every B planes.  At the barrier of
+// iteration it every warp has finished iteration it-1, so the loads of
+// iterations it+LA .. it+LA+B-1 (LA + B = S - 2) go into stages whose planes
+// were last read, as a stencil's centre plane, by iteration it-1.  Each
+// thread keeps its two columns of planes ze-2 .. ze+2 in registers for the
+// z differences.  The tensor map is a kernel parameter and tiles are dealt
+// round-robin (one volume, uniform tiles), so a launch needs no device
+// memory of its own.  A load that does not arrive within the bound leaves
+// NaN in the rest of the block's tile (no endless wait).
+// ------------------------------------------------------------------------
+template <typename T, int TXW>
+struct JacTmaLayout {
+    static constexpr int TMA_PX = Box<TXW>::PX;
+    static constexpr int TMA_PLANE = Box<TXW>::PLANE;
+    static constexpr int S = 10;   // stages: 96 KB (FP32, two blocks per SM), 192 KB (FP64, one)
+    static constexpr int B = 4;    // planes between block barriers
+    static constexpr int LA = S - 2 - B;  // first load distance: loads of it+LA .. it+LA+B-1 at a barrier
+    static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
+    static constexpr int BAR_OFF = S * U_BYTES;
+    static constexpr int BYTES = BAR_OFF + S * 8;
+    static_assert(U_BYTES % 128 == 0, "stages stay 128-byte aligned");
+};
+
+template <typename T, int TXW, int TYT>
+__global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
+    k_jacobian_tma(const __grid_constant__ CUtensorMap tm_u, const Geom g, T *__restrict__ jout, long long jys,
+                   long long jzs, int tiles_x, int tiles_y, int ntiles, int bz) {
+    using L = JacTmaLayout<T, TXW>;
+    constexpr int TPX = TXW / 2, RYT = TT_Y / TYT;
+    constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE, S = L::S, LA = L::LA;
+    static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem = align_smem_128(smem_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    __shared__ int s_fault;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
+    if (tid == 0) {
+        for (int k = 0; k < S; ++k) mbar_init(&bars[k], 1);
+        fence_mbar_init();
+        tmap_prefetch(&tm_u);
+        s_fault = 0;
+    }
+    __syncthreads();
+    const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+    uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int txi = tile % tiles_x, tyi = (tile / tiles_x) % tiles_y, tzi = tile / (tiles_x * tiles_y);
+        const int x0 = txi * TXW, y0 = tyi * TT_Y, z0 = tzi * bz;
+        const int z1 = min(z0 + bz, g.nz);
+        const int n_it = z1 - z0 + 4;  // planes z0-2 .. z1+1
+        // Every warp has finished the previous tile, whose stages the first
+        // loads below overwrite.
+        __syncthreads();
+        int issued_n = 0;
+        auto issue = [&](int j) {
+            issued_n = j + 1;
+            const uint32_t k = kbase + j;
+            uint64_t *bar = &bars[k % S];
+            mbar_arrive_expect_tx(bar, L::U_BYTES);
+            tma_load_4d(smem + (k % S) * L::U_BYTES, &tm_u, bar, x0 - TMA_HX, y0 - TMA_HY, z0 - 2 + j, 0);
+        };
+        if (tid == 0)
+            for (int j = 0; j < min(LA, n_it); ++j) issue(j);
+
+        const int x = x0 + 2 * tx;       // this thread's columns: x, x + 1
+        const int lx = 2 * tx + TMA_HX;  // their box column
+        const bool pair_in = x + 1 < g.nx;
+        T zq[RYT][2][3][5];
+#pragma unroll
+        for (int r = 0; r < RYT; ++r)
+#pragma unroll
+            for (int v = 0; v < 2; ++v)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
+        const bool tile_x_in = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3;
+        bool failed = false;
+        int fail_it = 0;
+        for (int it = 0; it < n_it; ++it) {
+            const uint32_t k = kbase + it;
+            if (it % L::B == 0) {
+                __syncthreads();
+                if (s_fault) {
+                    failed = true;
+                    fail_it = it;
+                    break;
+                }
+                if (tid == 0)
+                    for (int j = it + LA; j < min(it + LA + L::B, n_it); ++j) issue(j);
+            }
+            // A load that does not arrive stops the block at the next barrier
+            // (this plane's values are not used then).
+            if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u)) s_fault = 1;
+            const T *sb = reinterpret_cast<const T *>(smem + (k % S) * L::U_BYTES);
+            const int q = z0 - 2 + it, ze = q - 2;
+#pragma unroll
+            for (int r = 0; r < RYT; ++r) {
+                const int ly = ty + r * TYT + TMA_HY;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const auto nv = ld_pair(sb + c * TMA_PLANE + ly * TMA_PX + lx);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        zq[r][0][c][kk] = zq[r][0][c][kk + 1];
+                        zq[r][1][c][kk] = zq[r][1][c][kk + 1];
+                    }
+                    zq[r][0][c][4] = nv.x;
+                    zq[r][1][c][4] = nv.y;
+                }
+            }
+            if (ze < z0 || ze >= z1) continue;
+            const T *jp = reinterpret_cast<const T *>(smem + ((k - 2) % S) * L::U_BYTES);  // plane ze
+            const bool plane_in = ze >= 2 && ze <= g.nz - 3;
+#pragma unroll
+            for (int r = 0; r < RYT; ++r) {
+                const int y = y0 + ty + r * TYT;
+                if (x >= g.nx || y >= g.ny) continue;
+                const bool row_in = plane_in && y >= 2 && y <= g.ny - 3;
+                T jv[2];
+                stencil_pair<T, TMA_PX, TMA_PLANE>(jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
+                                                   tile_x_in,
+                                                   [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); });
+                T *o = jout + ze * jzs + y * jys + x;
+                if (pair_in)
+                    st_pair(o, jv[0], jv[1]);
+                else
+                    o[0] = jv[0];
+            }
+        }
+        if (failed) {
+            // Wait (bounded) for the loads still in flight, mark the tile's
+            // planes NaN and leave.
+            if (tid == 0)
+                for (int j = max(0, fail_it - L::B); j < issued_n; ++j) {
+                    const uint32_t kk = kbase + j;
+                    mbar_wait_bounded(&bars[kk % S], (kk / S) & 1u, 1u << 16);
+                }
+            const T nan = T(NAN);
+            for (int ze = z0; ze < z1; ++ze)
+#pragma unroll
+                for (int r = 0; r < RYT; ++r) {
+                    const int y = y0 + ty + r * TYT;
+                    if (y >= g.ny) continue;
+                    for (int v = 0; v < 2; ++v)
+                        if (x + v < g.nx) jout[ze * jzs + y * jys + x + v] = nan;
+                }
+            __syncthreads();
+            return;
+        }
+        kbase += n_it;
+    }
+}
+
+template <typename T, int TXW, int TYT>
+int jacobian_blocks_v() {
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             JacTmaLayout<T, TXW>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_jacobian_tma<T, TXW, TYT>, TXW / 2 * TYT,
+                                                      JacTmaLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return n;
+}
+
+// Jacobian map of the field `tm_u` describes (geometry g, order 4) into jout
+// (strides jys, jzs): tiles of 32 x TT_Y voxels, 16 x 16 threads, as many
+// blocks as fit on the device.  Tiles are dealt round-robin, so the z split
+// is chosen to fill whole waves of the grid: about 32 planes a tile, then as
+// many z tiles per column as fit in that many waves (at least 8 planes a
+// tile, since each tile also loads 4 halo planes).
+template <typename T>
+cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
+                                int num_sms, cudaStream_t s) {
+    constexpr int TXW = 32, TYT = 16, BZ = 32;
+    constexpr int smem = JacTmaLayout<T, TXW>::BYTES + 128;
+    static const cudaError_t attr =
+        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (attr != cudaSuccess) return attr;
+    const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
+    const int cols = tiles_x * tiles_y;
+    const int slots = std::max(1, jacobian_blocks_v<T, TXW, TYT>()) * num_sms;  // resident blocks
+    int nzt = (g.nz + BZ - 1) / BZ;                                             // z tiles per column
+    const int waves = (cols * nzt + slots - 1) / slots;
+    nzt = std::min((g.nz + 7) / 8, std::max(nzt, waves * slots / cols));  // at least 8 planes a tile
+    const int bz = (g.nz + nzt - 1) / nzt;
+    const int ntiles = cols * ((g.nz + bz - 1) / bz);
+    const int grid = std::min(ntiles, slots);
+    k_jacobian_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_u, g, jout, jys, jzs, tiles_x, tiles_y,
+                                                                      ntiles, bz);
+    count_launch();
+    return cudaGetLastError();
+}
+
 #define DTB_INSTANTIATE_TMA(T)                                                                              \
     template cudaError_t launch_trial_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
                                              unsigned char *, int, int, TileQueue *, int);                  \
@@ -1076,6 +1389,8 @@ int gradient_tma_blocks_per_sm(int tile_x, int threads_y) {
     template cudaError_t launch_greedy_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,   \
                                               unsigned char *, TileQueue *);                                \
     template int greedy_tma_blocks_per_sm<T>();                                                             \
+    template cudaError_t launch_jacobian_tma<T>(const CUtensorMap &, const Geom &, T *, long long, long long, int, \
+                                                cudaStream_t);                                              \
     template int gradient_tma_blocks_per_sm<T>(int, int);
 
 }  // namespace dtb

@@ -37,13 +37,20 @@ def _stream(t: torch.Tensor) -> int:
 
 
 def jacobian_raw(field: torch.Tensor, spacing: Sequence[float] = (1.0, 1.0, 1.0),
-                 order: int = 4) -> torch.Tensor:
-    """Jacobian map of one ``[3, nz, ny, nx]`` device field (no autograd)."""
+                 order: int = 4, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Jacobian map of one ``[3, nz, ny, nx]`` device field (no autograd),
+    into ``out`` (contiguous, ``[nz, ny, nx]``) when given."""
     _check(field, "field")
     if field.dim() != 4 or field.shape[0] != 3:
         raise ValueError("field must have shape (3, nz, ny, nx)")
     _, nz, ny, nx = field.shape
-    J = torch.empty((nz, ny, nx), dtype=field.dtype, device=field.device)
+    if out is None:
+        J = torch.empty((nz, ny, nx), dtype=field.dtype, device=field.device)
+    else:
+        _check(out, "out")
+        if out.shape != (nz, ny, nx) or out.dtype != field.dtype or out.device != field.device:
+            raise ValueError("out must match the field's spatial shape, dtype and device")
+        J = out
     with torch.cuda.device(field.device):
         N.check(N.lib.dtb_jacobian_device(_precision(field), order, nx, ny, nz,
                                           *map(float, spacing), field.data_ptr(), J.data_ptr(),
@@ -52,15 +59,22 @@ def jacobian_raw(field: torch.Tensor, spacing: Sequence[float] = (1.0, 1.0, 1.0)
 
 
 def jacobian_adjoint_raw(field: torch.Tensor, grad_J: torch.Tensor,
-                         spacing: Sequence[float] = (1.0, 1.0, 1.0), order: int = 4) -> torch.Tensor:
-    """(dJ/dfield)^T grad_J for one device field."""
+                         spacing: Sequence[float] = (1.0, 1.0, 1.0), order: int = 4,
+                         out: torch.Tensor | None = None) -> torch.Tensor:
+    """(dJ/dfield)^T grad_J for one device field, into ``out`` (contiguous,
+    the field's shape) when given."""
     _check(field, "field")
     grad_J = grad_J.contiguous()
     _check(grad_J, "grad_J")
     if grad_J.dtype != field.dtype or grad_J.shape != field.shape[1:]:
         raise ValueError("grad_J must match the field's dtype and spatial shape")
     _, nz, ny, nx = field.shape
-    out = torch.empty_like(field)
+    if out is None:
+        out = torch.empty_like(field)
+    else:
+        _check(out, "out")
+        if out.shape != field.shape or out.dtype != field.dtype or out.device != field.device:
+            raise ValueError("out must match the field's shape, dtype and device")
     with torch.cuda.device(field.device):
         N.check(N.lib.dtb_jacobian_adjoint_device(_precision(field), order, nx, ny, nz,
                                                   *map(float, spacing), field.data_ptr(),
@@ -79,15 +93,20 @@ class JacobianFunction(torch.autograd.Function):
         ctx.spacing = tuple(float(s) for s in spacing)
         ctx.order = order
         if field.dim() == 5:
-            return torch.stack([jacobian_raw(f, spacing, order) for f in field])
+            J = torch.empty((field.shape[0],) + tuple(field.shape[2:]), dtype=field.dtype,
+                            device=field.device)
+            for f, j in zip(field, J):
+                jacobian_raw(f, spacing, order, out=j)
+            return J
         return jacobian_raw(field, spacing, order)
 
     @staticmethod
     def backward(ctx, grad_J):
         (field,) = ctx.saved_tensors
         if field.dim() == 5:
-            g = torch.stack([jacobian_adjoint_raw(f, gj, ctx.spacing, ctx.order)
-                             for f, gj in zip(field, grad_J)])
+            g = torch.empty_like(field)
+            for f, gj, gf in zip(field, grad_J, g):
+                jacobian_adjoint_raw(f, gj, ctx.spacing, ctx.order, out=gf)
         else:
             g = jacobian_adjoint_raw(field, grad_J, ctx.spacing, ctx.order)
         return g, None, None

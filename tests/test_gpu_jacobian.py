@@ -51,6 +51,41 @@ def test_device_entry_fp32_and_fp64(oracle, oracle_pd2, order):
     assert rel_err(J32.astype(np.float64), ref) <= 2e-5
 
 
+@pytest.mark.parametrize("shape", [(37, 45, 68), (70, 18, 36), (3, 3, 4), (33, 17, 132), (5, 40, 8)])
+def test_device_entry_tma_layouts(oracle, shape):
+    """Rows a multiple of 16 bytes long take the TMA kernel: several tiles
+    along every axis, partial tiles, thin volumes; FP64 to the last bits."""
+    torch = _torch()
+    from disptools_b200 import torch_ops
+    rng = np.random.default_rng(sum(shape))
+    f = rng.normal(scale=0.2, size=(3,) + shape)
+    sp = tuple(rng.uniform(0.5, 2.0, 3))
+    ref = oracle.jacobian(f, sp)
+    J64 = torch_ops.jacobian_raw(torch.from_numpy(f).cuda(), sp).cpu().numpy()
+    assert rel_err(J64, ref) <= 1e-12
+    J32 = torch_ops.jacobian_raw(torch.from_numpy(f).float().cuda(), sp).cpu().numpy()
+    assert rel_err(J32.astype(np.float64), ref) <= 2e-5
+
+
+def test_device_entry_unaligned_field_takes_plain_kernel(oracle):
+    """A field that starts off a 16-byte boundary goes to the plain-load
+    kernel and gives the same map."""
+    torch = _torch()
+    from disptools_b200 import torch_ops
+    shape = (9, 20, 24)
+    rng = np.random.default_rng(7)
+    f = rng.normal(scale=0.2, size=(3,) + shape)
+    ref = oracle.jacobian(f)
+    n = f.size
+    buf = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.from_numpy(f.ravel()).cuda()
+    view = buf[1:].view((3,) + shape)  # 8 bytes past the allocation's start
+    assert view.data_ptr() % 16 == 8
+    J = torch_ops.jacobian_raw(view).cpu().numpy()
+    assert rel_err(J, ref) <= 1e-12
+    np.testing.assert_array_equal(J, torch_ops.jacobian_raw(view.clone()).cpu().numpy())
+
+
 def test_full_size_256_vs_oracle(oracle):
     torch = _torch()
     from disptools_b200 import torch_ops
