@@ -1314,11 +1314,26 @@ int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
 template <typename T>
 int adjoint_device_impl(const Geom &g, const T *field, const T *gJ, T *gout, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(g_ws_mutex);
+    // Weights W[9][wn] in the workspace, each component 256-byte aligned.
+    const long long wn = ((long long) g.cs + 63) / 64 * 64;
     char *base = nullptr;
-    int rc = workspace(9 * (size_t) g.cs * sizeof(T) + 256, &base);
+    int rc = workspace(9 * (size_t) wn * sizeof(T) + 256, &base);
     if (rc != DTB_OK) return rc;
     T *W = reinterpret_cast<T *>(base);
-    DTB_CUDA(launch_adjoint<T>(g, field, gJ, W, gout, s));
+    // The weight pass on the TMA stencil kernel when the layout allows it
+    // (as for the Jacobian map), else on the plain-load kernel.
+    bool w_done = false;
+    if (g.order == 4 && (g.ys * (long long) sizeof(T)) % 16 == 0 && reinterpret_cast<uintptr_t>(field) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(gJ) % (2 * sizeof(T)) == 0) {
+        CUtensorMap tm;
+        const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        if (encode_map(&tm, ft, sizeof(T), field, g, 3, 32 + 2 * 4, TT_Y + 2 * 2)) {
+            DTB_CUDA(launch_jacobian_tma<T>(tm, g, nullptr, g.ys, g.zs, num_sms(), s, gJ, W, wn));
+            w_done = true;
+        }
+    }
+    DTB_CUDA(launch_adjoint<T>(g, field, gJ, W, wn, gout, w_done, s));
+    // W lives in the shared workspace: finish before releasing it.
     DTB_CUDA(cudaStreamSynchronize(s));
     return DTB_OK;
 }

@@ -150,13 +150,19 @@ cudaError_t launch_greedy_tma(const VolumeDesc<T> *vols, const int *tile_vol, in
                               cudaStream_t s, unsigned char *work_flag, TileQueue *queue);
 template <typename T>
 int greedy_tma_blocks_per_sm();
-// TMA Jacobian map of one field of order 4 (the map `tm_u` over the field
-// with box 40 x 20 x 1 x 3) into jout with element strides jys, jzs.
+// TMA stencil of one field of order 4 (the map `tm_u` over the field with
+// box 40 x 20 x 1 x 3), with element strides jys, jzs for the scalar maps:
+// the Jacobian map into jout, or (adjoint weights) W[c][a] = gJ * cof_ca(I +
+// grad u) * ih_a into W with component stride wn.
 template <typename T>
 cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
-                                int num_sms, cudaStream_t s);
+                                int num_sms, cudaStream_t s, const T *gJ = nullptr, T *W = nullptr,
+                                long long wn = 0);
+// Adjoint of the Jacobian stencil: the weight pass (unless w_done: W already
+// holds the weights) and the gather pass; W is [9][N] with component stride wn.
 template <typename T>
-cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s);
+cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, long long wn, T *gout, bool w_done,
+                           cudaStream_t s);
 template <typename T>
 cudaError_t launch_convert(const void *src, int src_is_double, T *dst, long long n, cudaStream_t s);
 template <typename T>

@@ -386,6 +386,7 @@ __global__ void __launch_bounds__(NT) k_jacobian(const VolumeDesc<T> *__restrict
 // Exact adjoint of the Jacobian stencil (for autograd).
 // Pass 1: W[c][a](p) = w(p) * cof_ca(I + A(p)) * ih_a, A the stencil matrix.
 // Pass 2: grad_c(q) = sum_a sum_t W[c][a](q - t e_a) * kappa(k_a(q - t e_a), t).
+// W is dense, [9][nz][ny][nx] with component stride wn.
 // ------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T gload_deriv(const T *f, long long o, long long s, int k, T ih) {
@@ -398,7 +399,8 @@ __device__ __forceinline__ T gload_deriv(const T *f, long long o, long long s, i
 }
 
 template <typename T>
-__global__ void k_adjoint_w(Geom g, const T *__restrict__ f, const T *__restrict__ gJ, T *__restrict__ W) {
+__global__ void k_adjoint_w(Geom g, const T *__restrict__ f, const T *__restrict__ gJ, T *__restrict__ W,
+                            long long wn) {
     const long long N = (long long) g.nx * g.ny * g.nz;
     for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < N;
          i += (long long) gridDim.x * blockDim.x) {
@@ -423,7 +425,7 @@ __global__ void k_adjoint_w(Geom g, const T *__restrict__ f, const T *__restrict
                 const int c0 = a == 0 ? 1 : 0, c1 = a == 2 ? 1 : 2;
                 const T minor = m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
                 const T cof = ((c + a) & 1) ? -minor : minor;
-                W[(c * 3 + a) * N + i] = w * cof * (T) g.ih[a];
+                W[(c * 3 + a) * wn + i] = w * cof * (T) g.ih[a];
             }
         }
     }
@@ -441,15 +443,53 @@ __device__ __forceinline__ T kappa(int k, int t) {
     }
 }
 
+// Voxel coordinates of a dense index; 32-bit division when the volume has
+// fewer than 2^32 voxels (64-bit division costs several times as much).
+__device__ __forceinline__ void voxel_of(long long i, const Geom &g, bool small, int q[3]) {
+    if (small) {
+        const unsigned u = (unsigned) i, r = u / (unsigned) g.nx;
+        q[0] = (int) (u - r * (unsigned) g.nx);
+        q[1] = (int) (r % (unsigned) g.ny);
+        q[2] = (int) (r / (unsigned) g.ny);
+    } else {
+        q[0] = (int) (i % g.nx);
+        q[1] = (int) ((i / g.nx) % g.ny);
+        q[2] = (int) (i / ((long long) g.nx * g.ny));
+    }
+}
+
 template <typename T>
-__global__ void k_adjoint_gather(Geom g, const T *__restrict__ W, T *__restrict__ out) {
+__global__ void k_adjoint_gather(Geom g, const T *__restrict__ W, long long wn, T *__restrict__ out) {
     const long long N = (long long) g.nx * g.ny * g.nz;
+    const bool small = N < (1ll << 32);
     for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < N;
          i += (long long) gridDim.x * blockDim.x) {
-        const int q[3] = {(int) (i % g.nx), (int) ((i / g.nx) % g.ny), (int) (i / ((long long) g.nx * g.ny))};
+        int q[3];
+        voxel_of(i, g, small, q);
         const int n[3] = {g.nx, g.ny, g.nz};
         const long long dstr[3] = {1, g.nx, (long long) g.nx * g.ny};  // W is dense
         T acc[3] = {T(0), T(0), T(0)};
+        // At least four voxels from every face (order 4): each tap's voxel
+        // uses the fourth-order central scheme on its axis, so the weights
+        // are constants.  Same taps and summation order as the general path.
+        const bool deep = g.order == 4 && q[0] >= 4 && q[0] <= g.nx - 5 && q[1] >= 4 && q[1] <= g.ny - 5 &&
+                          q[2] >= 4 && q[2] <= g.nz - 5;
+        if (deep) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int t = -2; t <= 2; ++t) {
+                    if (t == 0) continue;
+                    const T kp = kappa<T>(S_C4, t);
+                    const long long pi = i - t * dstr[a];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) acc[c] += W[(c * 3 + a) * wn + pi] * kp;
+                }
+            const long long o = (long long) q[2] * g.zs + (long long) q[1] * g.ys + q[0];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) out[c * g.cs + o] = acc[c];
+            continue;
+        }
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             for (int t = -2; t <= 2; ++t) {
@@ -462,7 +502,7 @@ __global__ void k_adjoint_gather(Geom g, const T *__restrict__ W, T *__restrict_
                 if (kp == T(0)) continue;
                 const long long pi = i - t * dstr[a];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) acc[c] += W[(c * 3 + a) * N + pi] * kp;
+                for (int c = 0; c < 3; ++c) acc[c] += W[(c * 3 + a) * wn + pi] * kp;
             }
         }
         const long long o = (long long) q[2] * g.zs + (long long) q[1] * g.ys + q[0];
@@ -518,11 +558,15 @@ cudaError_t launch_jacobian(const VolumeDesc<T> *vols, const int *tile_vol, int 
 }
 
 template <typename T>
-cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, T *gout, cudaStream_t s) {
+cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, long long wn, T *gout, bool w_done,
+                           cudaStream_t s) {
     const long long N = (long long) g.nx * g.ny * g.nz;
-    k_adjoint_w<T><<<elementwise_grid(N), 256, 0, s>>>(g, field, gJ, W);
-    k_adjoint_gather<T><<<elementwise_grid(N), 256, 0, s>>>(g, W, gout);
-    count_launch(2);
+    if (!w_done) {
+        k_adjoint_w<T><<<elementwise_grid(N), 256, 0, s>>>(g, field, gJ, W, wn);
+        count_launch();
+    }
+    k_adjoint_gather<T><<<elementwise_grid(N), 256, 0, s>>>(g, W, wn, gout);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -549,7 +593,8 @@ cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s) {
 
 #define DTB_INSTANTIATE(T)                                                                                   \
     template cudaError_t launch_jacobian<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t);     \
-    template cudaError_t launch_adjoint<T>(const Geom &, const T *, const T *, T *, T *, cudaStream_t);      \
+    template cudaError_t launch_adjoint<T>(const Geom &, const T *, const T *, T *, long long, T *, bool,    \
+                                           cudaStream_t);                                                    \
     template cudaError_t launch_convert<T>(const void *, int, T *, long long, cudaStream_t);                 \
     template cudaError_t launch_to_double<T>(const T *, double *, long long, cudaStream_t);                  \
     template cudaError_t launch_regularise<T>(T *, long long, double, cudaStream_t);

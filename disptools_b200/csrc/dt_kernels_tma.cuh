@@ -1205,10 +1205,15 @@ struct JacTmaLayout {
     static_assert(U_BYTES % 128 == 0, "stages stay 128-byte aligned");
 };
 
-template <typename T, int TXW, int TYT>
+//
+// ADJ instantiates the weight pass of the Jacobian's adjoint instead: with
+// w = gJ(p), W[c][a](p) = w * cof_ca(I + A(p)) * ih_a for the stencil matrix
+// A(p), W dense with component stride wn (the gather pass follows).
+template <typename T, int TXW, int TYT, bool ADJ = false>
 __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     k_jacobian_tma(const __grid_constant__ CUtensorMap tm_u, const Geom g, T *__restrict__ jout, long long jys,
-                   long long jzs, int tiles_x, int tiles_y, int ntiles, int bz) {
+                   long long jzs, int tiles_x, int tiles_y, int ntiles, int bz, const T *__restrict__ gJ,
+                   T *__restrict__ W, long long wn) {
     using L = JacTmaLayout<T, TXW>;
     constexpr int TPX = TXW / 2, RYT = TT_Y / TYT;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE, S = L::S, LA = L::LA;
@@ -1303,15 +1308,55 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                 const int y = y0 + ty + r * TYT;
                 if (x >= g.nx || y >= g.ny) continue;
                 const bool row_in = plane_in && y >= 2 && y <= g.ny - 3;
-                T jv[2];
-                stencil_pair<T, TMA_PX, TMA_PLANE>(jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
-                                                   tile_x_in,
-                                                   [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); });
-                T *o = jout + ze * jzs + y * jys + x;
-                if (pair_in)
-                    st_pair(o, jv[0], jv[1]);
-                else
-                    o[0] = jv[0];
+                const long long off = ze * jzs + y * jys + x;
+                if (ADJ) {
+                    T w[2];
+                    if (pair_in) {
+                        const auto w2 = ld_pair(gJ + off);
+                        w[0] = w2.x;
+                        w[1] = w2.y;
+                    } else {
+                        w[0] = gJ[off];
+                        w[1] = T(0);
+                    }
+                    T wv[9][2];
+                    stencil_pair<T, TMA_PX, TMA_PLANE>(
+                        jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in, tile_x_in,
+                        [&](int v, const T (&a)[3][3]) {
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+#pragma unroll
+                                for (int b = 0; b < 3; ++b) {
+                                    const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+                                    const T m00 = a[r0][c0] + (r0 == c0 ? T(1) : T(0));
+                                    const T m11 = a[r1][c1] + (r1 == c1 ? T(1) : T(0));
+                                    const T m01 = a[r0][c1] + (r0 == c1 ? T(1) : T(0));
+                                    const T m10 = a[r1][c0] + (r1 == c0 ? T(1) : T(0));
+                                    const T minor = m00 * m11 - m01 * m10;
+                                    const T cof = ((c + b) & 1) ? -minor : minor;
+                                    wv[c * 3 + b][v] = w[v] * cof * ih[b];
+                                }
+                            }
+                        });
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {
+                        if (pair_in)
+                            st_pair(W + k * wn + off, wv[k][0], wv[k][1]);
+                        else
+                            W[k * wn + off] = wv[k][0];
+                    }
+                } else {
+                    T jv[2];
+                    stencil_pair<T, TMA_PX, TMA_PLANE>(jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
+                                                       tile_x_in,
+                                                       [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); });
+                    T *o = jout + off;
+                    if (pair_in)
+                        st_pair(o, jv[0], jv[1]);
+                    else
+                        o[0] = jv[0];
+                }
             }
         }
         if (failed) {
@@ -1328,8 +1373,14 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                 for (int r = 0; r < RYT; ++r) {
                     const int y = y0 + ty + r * TYT;
                     if (y >= g.ny) continue;
-                    for (int v = 0; v < 2; ++v)
-                        if (x + v < g.nx) jout[ze * jzs + y * jys + x + v] = nan;
+                    for (int v = 0; v < 2; ++v) {
+                        if (x + v >= g.nx) continue;
+                        const long long off = ze * jzs + y * jys + x + v;
+                        if (ADJ)
+                            for (int k = 0; k < 9; ++k) W[k * wn + off] = nan;
+                        else
+                            jout[off] = nan;
+                    }
                 }
             __syncthreads();
             return;
@@ -1338,46 +1389,53 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     }
 }
 
-template <typename T, int TXW, int TYT>
+template <typename T, int TXW, int TYT, bool ADJ>
 int jacobian_blocks_v() {
     static const int n = [] {
         int v = 0;
-        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT, ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              JacTmaLayout<T, TXW>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_jacobian_tma<T, TXW, TYT>, TXW / 2 * TYT,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_jacobian_tma<T, TXW, TYT, ADJ>, TXW / 2 * TYT,
                                                       JacTmaLayout<T, TXW>::BYTES + 128);
         return v;
     }();
     return n;
 }
 
-// Jacobian map of the field `tm_u` describes (geometry g, order 4) into jout
-// (strides jys, jzs): tiles of 32 x TT_Y voxels, 16 x 16 threads, as many
+// Jacobian map (or adjoint weights) of the field `tm_u` describes (geometry
+// g, order 4) into jout (strides jys, jzs): tiles of 32 x TT_Y voxels, 16 x 16 threads, as many
 // blocks as fit on the device.  Tiles are dealt round-robin, so the z split
 // is chosen to fill whole waves of the grid: about 32 planes a tile, then as
 // many z tiles per column as fit in that many waves (at least 8 planes a
 // tile, since each tile also loads 4 halo planes).
-template <typename T>
-cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
-                                int num_sms, cudaStream_t s) {
+template <typename T, bool ADJ>
+cudaError_t launch_jacobian_tma_v(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
+                                  int num_sms, cudaStream_t s, const T *gJ, T *W, long long wn) {
     constexpr int TXW = 32, TYT = 16, BZ = 32;
     constexpr int smem = JacTmaLayout<T, TXW>::BYTES + 128;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static const cudaError_t attr = cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT, ADJ>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (attr != cudaSuccess) return attr;
     const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
     const int cols = tiles_x * tiles_y;
-    const int slots = std::max(1, jacobian_blocks_v<T, TXW, TYT>()) * num_sms;  // resident blocks
+    const int slots = std::max(1, jacobian_blocks_v<T, TXW, TYT, ADJ>()) * num_sms;  // resident blocks
     int nzt = (g.nz + BZ - 1) / BZ;                                             // z tiles per column
     const int waves = (cols * nzt + slots - 1) / slots;
     nzt = std::min((g.nz + 7) / 8, std::max(nzt, waves * slots / cols));  // at least 8 planes a tile
     const int bz = (g.nz + nzt - 1) / nzt;
     const int ntiles = cols * ((g.nz + bz - 1) / bz);
     const int grid = std::min(ntiles, slots);
-    k_jacobian_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_u, g, jout, jys, jzs, tiles_x, tiles_y,
-                                                                      ntiles, bz);
+    k_jacobian_tma<T, TXW, TYT, ADJ><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_u, g, jout, jys, jzs, tiles_x,
+                                                                           tiles_y, ntiles, bz, gJ, W, wn);
     count_launch();
     return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
+                                int num_sms, cudaStream_t s, const T *gJ, T *W, long long wn) {
+    if (W) return launch_jacobian_tma_v<T, true>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
+    return launch_jacobian_tma_v<T, false>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
 }
 
 #define DTB_INSTANTIATE_TMA(T)                                                                              \
@@ -1390,7 +1448,7 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
                                               unsigned char *, TileQueue *);                                \
     template int greedy_tma_blocks_per_sm<T>();                                                             \
     template cudaError_t launch_jacobian_tma<T>(const CUtensorMap &, const Geom &, T *, long long, long long, int, \
-                                                cudaStream_t);                                              \
+                                                cudaStream_t, const T *, T *, long long);                   \
     template int gradient_tma_blocks_per_sm<T>(int, int);
 
 }  // namespace dtb
