@@ -165,10 +165,13 @@ struct Workspace {
     size_t bytes = 0;
 };
 std::mutex g_ws_mutex;
-// Per device: the solver's scratch (pitched buffers, descriptors, partials)
-// and the staging area of host-array calls.  Both grow on demand and are
-// kept until dtb_release_device_memory() or the end of the process.
-std::vector<Workspace> g_ws, g_io;
+// Per device: the solver's scratch (pitched buffers, descriptors, partials),
+// the staging area of host-array calls and the adjoint's weights.  They grow
+// on demand and are kept until dtb_release_device_memory() or the end of the
+// process.
+std::vector<Workspace> g_ws, g_io, g_adj;
+// Per device: recorded after the last adjoint's gather pass, on its stream.
+std::vector<cudaEvent_t> g_adj_done;
 
 // Failure-path test hook (dtb_test_drop_tma_load).
 struct DropTest {
@@ -1314,11 +1317,20 @@ int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
 template <typename T>
 int adjoint_device_impl(const Geom &g, const T *field, const T *gJ, T *gout, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(g_ws_mutex);
-    // Weights W[9][wn] in the workspace, each component 256-byte aligned.
+    // Weights W[9][wn] in the adjoint's own buffer, each component 256-byte
+    // aligned.  Calls are ordered on the device, not on the host: this
+    // call's stream waits for the previous call's gather (any stream) before
+    // it overwrites W.  Growing the buffer frees the old one, which waits
+    // for the device.
     const long long wn = ((long long) g.cs + 63) / 64 * 64;
     char *base = nullptr;
-    int rc = workspace(9 * (size_t) wn * sizeof(T) + 256, &base);
+    int rc = grow(g_adj, 9 * (size_t) wn * sizeof(T) + 256, &base);
     if (rc != DTB_OK) return rc;
+    int dev = 0;
+    DTB_CUDA(cudaGetDevice(&dev));
+    if ((int) g_adj_done.size() <= dev) g_adj_done.resize(dev + 1, nullptr);
+    if (!g_adj_done[dev]) DTB_CUDA(cudaEventCreateWithFlags(&g_adj_done[dev], cudaEventDisableTiming));
+    DTB_CUDA(cudaStreamWaitEvent(s, g_adj_done[dev], 0));
     T *W = reinterpret_cast<T *>(base);
     // The weight pass on the TMA stencil kernel when the layout allows it
     // (as for the Jacobian map), else on the plain-load kernel.
@@ -1333,8 +1345,7 @@ int adjoint_device_impl(const Geom &g, const T *field, const T *gJ, T *gout, cud
         }
     }
     DTB_CUDA(launch_adjoint<T>(g, field, gJ, W, wn, gout, w_done, s));
-    // W lives in the shared workspace: finish before releasing it.
-    DTB_CUDA(cudaStreamSynchronize(s));
+    DTB_CUDA(cudaEventRecord(g_adj_done[dev], s));
     return DTB_OK;
 }
 
@@ -1422,7 +1433,7 @@ extern "C" int dtb_release_device_memory(void) {
     std::lock_guard<std::mutex> lock(g_ws_mutex);
     int dev = 0;
     DTB_CUDA(cudaGetDevice(&dev));
-    for (std::vector<Workspace> *pool : {&g_ws, &g_io}) {
+    for (std::vector<Workspace> *pool : {&g_ws, &g_io, &g_adj}) {
         if ((int) pool->size() > dev && (*pool)[dev].ptr) {
             cudaFree((*pool)[dev].ptr);
             (*pool)[dev] = Workspace{};
