@@ -53,11 +53,12 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="c2", choices=["c2", "c4", "c5", "greedy"],
+    p.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "greedy"],
                    help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
                         "axes U{48..192} split over the ranks; c5: one 512x512x384 volume per "
                         "rank through a 3-level pyramid, plus greedy on the coarsest level; "
-                        "greedy: the config-2 volume solved by the greedy method")
+                        "greedy: the config-2 volume solved by the greedy method; "
+                        "c3: the differentiable Jacobian, forward + backward, on 4 192x224x192 fields")
     return p.parse_args()
 
 
@@ -198,6 +199,9 @@ def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6, algorithm="gradient"):
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
+    if args.workload == "c3":
+        run_reference_c3(args)
+        return
     from disptools_b200.synthetic import blob_problem
     n = args.size
     algorithm = "greedy" if args.workload == "greedy" else "gradient"
@@ -225,6 +229,40 @@ def run_reference_arm(args, world, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
+
+
+def run_reference_c3(args):
+    """The reference C library's jacobian_dynamic (FP64, OpenMP) on the
+    config-3 fields.  The reference has no adjoint of its Jacobian, so a step
+    is the forward map of the batch only; the line says so."""
+    import numpy as np
+
+    from disptools_b200.synthetic import smooth_field
+    from oracle.oracle import Oracle, Reference
+    shape, B = (192, 224, 192), 4
+    fields = [smooth_field(shape, seed=b) for b in range(B)]
+    impl, kind = (Reference("ref64"), "reference") if Reference.available("ref64") else (Oracle(4), "port")
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for f in fields:
+            impl.jacobian(f)
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = statistics.mean(times)
+    value = B * float(np.prod(shape)) / t
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "differentiable jacobian() forward + backward voxels/s, 4 x 192x224x192 FP32 (config 3)",
+        "value": value, "unit": "voxels/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "config 3 fields, forward map only (the reference has no adjoint)"},
+        "cpu_baseline": {"value": value, "unit": "voxels/s", "cores": cores, "kind": kind,
+                         "sample": f"per step: jacobian_dynamic on 4 fields of {shape}"},
+        "e2e": {"value": value, "unit": "voxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
 
 
 def run_c4(args, world, rank, local):
@@ -398,11 +436,116 @@ def run_c5(args, world, rank, local):
         }))
 
 
+def run_c3(args, world, rank, local):
+    """Config 3: the differentiable Jacobian on a batch of 4 FP32 fields of
+    192x224x192 per rank (smooth random fields, max |u| = 3).  One step = the
+    forward map and the backward adjoint of torch_ops.jacobian for the batch.
+    Metric: field voxels through forward + backward per second.  The roofline
+    is the Jacobian kernel's, timed alone: 16 algorithmic bytes per voxel
+    (field 12 in, J 4 out)."""
+    import numpy as np
+    import torch
+
+    import disptools_b200 as dt
+    from disptools_b200 import torch_ops
+    from disptools_b200.synthetic import smooth_field
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    shape, B = (192, 224, 192), 4
+    f0 = torch.stack([torch.from_numpy(smooth_field(shape, seed=4 * rank + b)).float()
+                      for b in range(B)]).to(dev)
+    rng = np.random.default_rng(rank)
+    w = torch.from_numpy(rng.standard_normal((B,) + shape)).float().to(dev)
+    f = f0.clone().requires_grad_(True)
+    nvox = B * int(np.prod(shape))
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        f.grad = None
+        torch_ops.jacobian(f).backward(w)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = dt.kernel_launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    launches = dt.kernel_launch_count() - launches0
+    value = sum_over_ranks(world, float(nvox) * args.steps) / (ms / 1000.0)
+
+    # Jacobian kernel alone (one launch per field), then the backward alone.
+    def timed(fn, reps=10):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    fd = f.detach()
+    J = torch.empty((B,) + shape, dtype=torch.float32, device=dev)
+    G = torch.empty_like(fd)
+    fwd_ms = timed(lambda: [torch_ops.jacobian_raw(fd[b], out=J[b]) for b in range(B)])
+    bwd_ms = timed(lambda: [torch_ops.jacobian_adjoint_raw(fd[b], w[b], out=G[b]) for b in range(B)])
+    hbm, peak_kind = peaks()
+    achieved = 16.0 * nvox / (fwd_ms / 1000.0) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.oracle import Oracle, Reference
+        impl, kind = (Reference("ref64"), "reference") if Reference.available("ref64") else (Oracle(4), "port")
+        f64 = fd[0].double().cpu().numpy()
+        impl.jacobian(f64)
+        t0 = time.perf_counter()
+        impl.jacobian(f64)
+        t = time.perf_counter() - t0
+        cpu = {"value": np.prod(shape) / t, "unit": "voxels/s (forward map only)",
+               "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": kind,
+               "sample": f"one {shape} field, reference jacobian_dynamic (FP64, OpenMP): {t:.3f} s"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "differentiable jacobian() forward + backward voxels/s, 4 x 192x224x192 FP32 (config 3)",
+            "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config 3: torch_ops.jacobian forward + backward on 4 FP32 fields of "
+                                   "192x224x192 (Gaussian-filtered noise, sigma 6, max |u| = 3)",
+                       "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                       "l2": "inputs larger than L2 (fields 397 MB)",
+                       "parallelism": f"{world} independent batches"},
+            "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                         "peak_source": peak_kind, "bytes_per_voxel": 16},
+            "cpu_baseline": cpu,
+            "e2e": None,
+            "gpu_launches": launches, "clocks": clk.summary(),
+        }))
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.workload == "c5" and args.impl == "b200":
         run_c5(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.workload == "c3" and args.impl == "b200":
+        run_c3(args, world, rank, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
