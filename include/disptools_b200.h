@@ -241,7 +241,10 @@ int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, double dy, d
  * `J` [nz][ny][nx], both device pointers of the element type of
  * `precision` (float for MIXED, double for FP64); `order` is the interior
  * finite-difference order, 4 (the reference default ORDER_PD) or 2;
- * `stream` is a cudaStream_t or NULL. */
+ * `stream` is a cudaStream_t or NULL.  The work is enqueued on `stream`:
+ * with order 4, rows a multiple of 16 bytes long, `field` 16-byte aligned
+ * and `J` aligned to two elements, the call returns without waiting for the
+ * device; otherwise it returns once the map is complete. */
 int dtb_jacobian_device(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, void *J, void *stream);
@@ -249,7 +252,9 @@ int dtb_jacobian_device(
 /* Adjoint of dtb_jacobian_device: grad_field = (dJ/dfield)^T grad_J, the
  * exact transpose of the position-dependent stencil (fourth order inside,
  * second order on the penultimate and outer layers).  Device pointers as
- * above; grad_field is overwritten. */
+ * above; grad_field is overwritten.  The work is enqueued on `stream` and
+ * the call returns without waiting for the device; calls on different
+ * streams are ordered on the device (they share one weight buffer). */
 int dtb_jacobian_adjoint_device(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, const void *grad_J, void *grad_field, void *stream);
