@@ -164,6 +164,18 @@ def test_full_size_256_fp64_first_iterations(oracle):
     assert np.max(np.abs(out - ref)) <= 1e-10
 
 
+def test_full_size_256_fp64_greedy_first_iterations(oracle):
+    """Config-2 inputs at full size, greedy method: a few FP64 iterations
+    against the oracle (every tile, both field buffers, the error maps)."""
+    from disptools_b200.synthetic import blob_problem
+    Jt, mask = blob_problem((256, 256, 256), blobs=16, seed=0)
+    ref, so = oracle.solve("greedy", Jt, mask, it_max=4)
+    out, st = dt.solve(Jt, mask, algorithm="greedy", precision="fp64", it_max=4)
+    assert st["iterations"] == so.iterations and st["trials"] == so.trials and st["reason"] == so.reason
+    assert st["error"] == pytest.approx(so.error, rel=1e-12)
+    assert np.max(np.abs(out - ref)) <= 1e-12
+
+
 def test_full_size_256_mixed_properties(oracle):
     """Config-2 inputs at full size, mixed precision: the reported error of the
     returned field matches an FP64 recomputation, and it decreased."""
