@@ -490,19 +490,39 @@ __global__ void k_adjoint_gather(Geom g, const T *__restrict__ W, long long wn, 
             for (int c = 0; c < 3; ++c) out[c * g.cs + o] = acc[c];
             continue;
         }
+        // The scheme of tap voxel p = q - t e_a along a (schemes_at(p)[a]):
+        // p differs from q only along a, so the outer / penultimate flags of
+        // the other two axes come from q once.
+        bool ob[3], pb[3];
 #pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            ob[b] = q[b] == 0 || q[b] == n[b] - 1;
+            pb[b] = q[b] == 1 || q[b] == n[b] - 2;
+        }
+        // One axis at a time (a rolled loop keeps few loads in flight and
+        // few registers); per-axis values by selects, not array indexing.
+#pragma unroll 1
         for (int a = 0; a < 3; ++a) {
-            for (int t = -2; t <= 2; ++t) {
-                int p[3] = {q[0], q[1], q[2]};
-                p[a] -= t;
-                if (p[a] < 0 || p[a] >= n[a]) continue;
-                int k[3];
-                schemes_at(p[0], p[1], p[2], g, k);
-                const T kp = kappa<T>(k[a], t);
-                if (kp == T(0)) continue;
-                const long long pi = i - t * dstr[a];
+            const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
+            const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
+            const int qa = a == 0 ? q[0] : (a == 1 ? q[1] : q[2]);
+            const int na = a == 0 ? n[0] : (a == 1 ? n[1] : n[2]);
+            const long long da = a == 0 ? dstr[0] : (a == 1 ? dstr[1] : dstr[2]);
+            const T *w0 = W + a * wn, *w1 = W + (3 + a) * wn, *w2 = W + (6 + a) * wn;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) acc[c] += W[(c * 3 + a) * wn + pi] * kp;
+            for (int t = -2; t <= 2; ++t) {
+                const int pa = qa - t;
+                if (pa < 0 || pa >= na) continue;
+                const bool outer = o_other || pa == 0 || pa == na - 1;
+                const bool pen = p_other || pa == 1 || pa == na - 2;
+                const int k = outer ? (pa == 0 ? S_FWD : (pa == na - 1 ? S_BWD : S_C2))
+                                    : ((g.order == 2 || pen) ? S_C2 : S_C4);
+                const T kp = kappa<T>(k, t);
+                if (kp == T(0)) continue;
+                const long long pi = i - t * da;
+                acc[0] += w0[pi] * kp;
+                acc[1] += w1[pi] * kp;
+                acc[2] += w2[pi] * kp;
             }
         }
         const long long o = (long long) q[2] * g.zs + (long long) q[1] * g.ys + q[0];
