@@ -39,20 +39,23 @@ def fd_check(field64, w, grad, probes, spacing=(1.0, 1.0, 1.0), h=1e-6, order=4)
     return got, np.array(fd)
 
 
-def test_adjoint_fp64_vs_finite_differences():
+@pytest.mark.parametrize("shape", [(14, 12, 10), (13, 11, 19)])
+def test_adjoint_fp64_vs_finite_differences(shape):
+    """The second shape has odd extents and a deep interior along x, where
+    the gather uses its constant weights."""
     import torch
     from disptools_b200 import torch_ops
     from disptools_b200.synthetic import smooth_field
-    f = torch.from_numpy(smooth_field((14, 12, 10), sigma=2.0, max_disp=0.8, seed=1)).cuda()
+    f = torch.from_numpy(smooth_field(shape, sigma=2.0, max_disp=0.8, seed=1)).cuda()
     f.requires_grad_(True)
     rng = np.random.default_rng(2)
-    w = torch.from_numpy(rng.standard_normal((14, 12, 10))).cuda()
+    w = torch.from_numpy(rng.standard_normal(shape)).cuda()
     sp = (0.9, 1.1, 1.3)
     J = torch_ops.jacobian(f, sp)
     (J * w).sum().backward()
     probes = [(int(c), int(z), int(y), int(x)) for c, z, y, x in
-              zip(rng.integers(0, 3, 300), rng.integers(0, 14, 300), rng.integers(0, 12, 300),
-                  rng.integers(0, 10, 300))]
+              zip(rng.integers(0, 3, 300), rng.integers(0, shape[0], 300), rng.integers(0, shape[1], 300),
+                  rng.integers(0, shape[2], 300))]
     got, fd = fd_check(f.detach(), w, f.grad, probes, sp)
     np.testing.assert_allclose(got, fd, rtol=1e-6, atol=1e-7)
 
