@@ -170,13 +170,13 @@ def iterations_done(st) -> int:
     return int(st["iterations"] - 1 if st["reason"] == "it_max" else st["iterations"])
 
 
-def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6, algorithm="gradient"):
-    """The reference C library (FP64, OpenMP, all host cores) on the same
-    volume: per-iteration rate from two solves (it_max it_lo and it_hi), so
-    set-up work cancels out."""
+def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6, algorithm="gradient", flavour="ref64"):
+    """The reference C library (FP64 build by default, OpenMP, all host
+    cores) on the same volume: per-iteration rate from two solves (it_max
+    it_lo and it_hi), so set-up work cancels out."""
     from oracle.oracle import Oracle, Reference
-    if Reference.available("ref64"):
-        impl, kind = Reference("ref64"), "reference"
+    if Reference.available(flavour):
+        impl, kind = Reference(flavour), "reference"
     else:
         impl, kind = Oracle(4), "port"
     times = {}
@@ -714,7 +714,13 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, kind, cores, times = reference_cpu_rate(Jt_np, mask_np, algorithm=algorithm)
-        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
+        from oracle.oracle import Reference
+        fp32 = None
+        if Reference.available("ref32"):
+            r32, _, _, t32 = reference_cpu_rate(Jt_np, mask_np, algorithm=algorithm, flavour="ref32")
+            fp32 = {"value": r32, "sample": f"the reference's default FP32 build, same solves "
+                                            f"({t32[1]:.2f} s, {t32[6]:.2f} s)"}
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "fp32_build": fp32,
                "sample": f"{n}^3 volume, reference C library FP64 OpenMP, {algorithm} method: "
                          f"solves with it_max=1 "
                          f"({times[1]:.2f} s) and it_max=6 ({times[6]:.2f} s); "
