@@ -502,6 +502,12 @@ def run_c3(args, world, rank, local):
     bwd_ms = timed(lambda: [torch_ops.jacobian_adjoint_raw(fd[b], w[b], out=G[b]) for b in range(B)])
     hbm, peak_kind = peaks()
     achieved = 16.0 * nvox / (fwd_ms / 1000.0) / 1e9
+    traffic = None  # DRAM bytes of one launch (one field), from the committed ncu capture
+    try:
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["jacobian_c3_field"][
+            "bytes_per_launch"]
+    except Exception:
+        traffic = None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -527,8 +533,9 @@ def run_c3(args, world, rank, local):
                        "l2": "inputs larger than L2 (fields 397 MB)",
                        "parallelism": f"{world} independent batches"},
             "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                         "peak_source": peak_kind, "bytes_per_voxel": 16},
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": peak_kind, "bytes_per_voxel": 16,
+                         "bytes_per_launch": 16 * nvox // B, "avg_launch_ms": fwd_ms / B},
             "cpu_baseline": cpu,
             "e2e": None,
             "gpu_launches": launches, "clocks": clk.summary(),
