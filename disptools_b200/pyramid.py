@@ -133,6 +133,13 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
     else:
         its = [int(it_max)] * levels
     p = pad + 1 if pad > 0 else 1
+    if len(tuple(jacobian.shape)) == 3:
+        # Every level must keep 3 voxels per axis (the solver's minimum):
+        # checked before any work on the device.
+        sizes0, _ = level_geometry(tuple(int(s) + 2 * p for s in jacobian.shape), spacing, levels)
+        if min(sizes0[-1]) < 3:
+            raise ValueError(f"level {levels - 1} would be {sizes0[-1]} voxels, below 3 along an axis: "
+                             "use fewer levels")
     on_device = isinstance(jacobian, torch.Tensor)
     if on_device:
         # Device tensors stay on their device: padding and redistribution in

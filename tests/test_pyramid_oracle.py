@@ -80,3 +80,24 @@ def test_blob_problem_device_matches_numpy_on_cpu():
     Jd, md = blob_problem_device((23, 19, 27), blobs=5, seed=4, sigma=(2.0, 5.0), device="cpu")
     np.testing.assert_allclose(Jd.numpy(), J, rtol=1e-14)
     np.testing.assert_array_equal(md.numpy(), m)
+
+
+def test_level_geometry_follows_the_reference_rule():
+    """disptools/displacements.py:459-466: each level halves the previous
+    size (integer division); spacings keep the finest level's extent."""
+    from disptools_b200.pyramid import level_geometry
+    sizes, spacings = level_geometry((386, 514, 514), (1.0, 1.0, 1.0), 3)
+    assert sizes == [(386, 514, 514), (193, 257, 257), (96, 128, 128)]
+    assert spacings[1] == (2.0, 2.0, 2.0)
+    assert spacings[2] == (514 / 128, 514 / 128, 386 / 96)
+    sizes, spacings = level_geometry((7, 9, 11), (0.5, 1.5, 2.0), 2)
+    assert sizes == [(7, 9, 11), (3, 4, 5)]
+    assert spacings[1] == (0.5 * 11 / 5, 1.5 * 9 / 4, 2.0 * 7 / 3)
+
+
+def test_pyramid_rejects_levels_below_three_voxels_before_device_work():
+    import numpy as np
+    import pytest
+    from disptools_b200 import pyramid
+    with pytest.raises(ValueError, match="below 3"):
+        pyramid.displacement(np.ones((5, 5, 5)), levels=3)
