@@ -447,9 +447,6 @@ bool verbose_enabled() {
 // The greedy method runs 32 x TT_Y tiles of bz planes.
 struct TileConfig {
     int tile_x = 32, trial_ty = 16, grad_ty = 16, bz = 32, pf = 0;
-    bool operator==(const TileConfig &o) const {
-        return tile_x == o.tile_x && trial_ty == o.trial_ty && grad_ty == o.grad_ty && bz == o.bz && pf == o.pf;
-    }
 };
 
 // Explicit shapes from the environment (DISPTOOLS_B200_TILE_X = 32 | 64,
