@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-greedy", action="store_true")
     p.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "greedy"],
                    help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
                         "axes U{48..192} split over the ranks; c5: one 512x512x384 volume per "
@@ -170,30 +171,59 @@ def iterations_done(st) -> int:
     return int(st["iterations"] - 1 if st["reason"] == "it_max" else st["iterations"])
 
 
-def reference_cpu_rate(Jt, mask, it_lo=1, it_hi=6, algorithm="gradient", flavour="ref64"):
-    """The reference C library (FP64 build by default, OpenMP, all host
-    cores) on the same volume: per-iteration rate from two solves (it_max
-    it_lo and it_hi), so set-up work cancels out."""
+def workload_c2(algorithm: str, n: int, it_max: int) -> str:
+    """The workload string of the config-2 lines (both arms)."""
+    return (f"config 2: {algorithm} method on {n}^3 (16 Gaussian blobs), zero initial field, "
+            f"the reference's default parameters, it_max={it_max} per step")
+
+
+def reference_impl():
+    """The reference C library's FP64 build with its stock verbose output
+    (what its Python package builds, setup.py: DISPTOOLS_VERBOSE=ON), which
+    reports the iterations each solve completed; the restatement when the
+    reference was not built."""
     from oracle.oracle import Oracle, Reference
-    if Reference.available(flavour):
-        impl, kind = Reference(flavour), "reference"
+    if Reference.available("ref64_verbose"):
+        return Reference("ref64_verbose"), "reference"
+    return Oracle(4), "port"
+
+
+def reference_solve(impl, kind, algorithm, Jt, mask, it_max):
+    """One solve from the zero field: (seconds, iterations completed, field)."""
+    t0 = time.perf_counter()
+    if kind == "reference":
+        field, _, its = impl.solve_logged(algorithm, Jt, mask, it_max=it_max)
     else:
-        impl, kind = Oracle(4), "port"
-    times = {}
-    for it in (it_lo, it_hi):
-        t0 = time.perf_counter()
-        impl.solve(algorithm, Jt, mask, it_max=it)
-        times[it] = time.perf_counter() - t0
-    n = Jt.size
-    d = times[it_hi] - times[it_lo]
-    if d > 0.05 * times[it_hi]:
-        rate = n * (it_hi - it_lo) / d
-    else:
-        # The solve stopped before it_hi iterations (a small volume): the
-        # difference holds no iterations, so take the whole it_hi solve.
-        rate = n * it_hi / times[it_hi]
+        field, st = impl.solve(algorithm, Jt, mask, it_max=it_max)
+        its = st.iterations - 1 if st.reason == "it_max" else st.iterations
+    return time.perf_counter() - t0, int(its), field
+
+
+def reference_cpu_rate(Jt, mask, it_max, samples=3, warmup=1, algorithm="gradient"):
+    """The reference C library (FP64, OpenMP, all host cores) solving the
+    same volume with the same it_max: `warmup` short solves (it_max 2), then
+    `samples` full ones.  Rate = voxels x iterations completed / time, summed
+    over the samples; the last sample's field is returned for the accuracy
+    comparison."""
+    impl, kind = reference_impl()
+    for _ in range(warmup):
+        reference_solve(impl, kind, algorithm, Jt, mask, min(2, it_max))
+    times, its, field = [], [], None
+    for _ in range(samples):
+        t, k, field = reference_solve(impl, kind, algorithm, Jt, mask, it_max)
+        times.append(t)
+        its.append(k)
+    rate = Jt.size * sum(its) / sum(times)
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return rate, kind, cores, times
+    return rate, kind, cores, times, its, field
+
+
+def masked_residual(J, Jt, mask) -> float:
+    """Final masked max |J - J_t| (the reference's max voxel error inside the
+    mask, src/headers/error.h:87-172, without the tolerance band outside)."""
+    import numpy as np
+    d = np.abs(J - Jt)[mask]
+    return float(d.max()) if d.size else 0.0
 
 
 def run_reference_arm(args, world, rank):
@@ -202,28 +232,36 @@ def run_reference_arm(args, world, rank):
     if args.workload == "c3":
         run_reference_c3(args)
         return
+    # the seeded generator only: this arm loads no library of this package
     from disptools_b200.synthetic import blob_problem
     n = args.size
+    IT = args.it_max
     algorithm = "greedy" if args.workload == "greedy" else "gradient"
     Jt, mask = blob_problem((n, n, n), blobs=16, seed=0)
-    rates = []
-    samples = []
-    for s in range(args.warmup + args.steps):
-        rate, kind, cores, times = reference_cpu_rate(Jt, mask, algorithm=algorithm)
-        if s >= args.warmup:
-            rates.append(rate)
-            samples.append(times)
-    value = statistics.mean(rates)
-    sample = (f"per step: reference C library (FLOAT_SIZE=64, ORDER_PD=4, OpenMP) solving the "
-              f"{n}^3 volume with it_max=1 and it_max=6; rate = voxels x 5 / time difference")
+    impl, kind = reference_impl()
+    # warm-up steps: short solves (threads and pages brought up)
+    for _ in range(args.warmup):
+        reference_solve(impl, kind, algorithm, Jt, mask, min(2, IT))
+    times, its = [], []
+    for _ in range(args.steps):
+        t, k, _ = reference_solve(impl, kind, algorithm, Jt, mask, IT)
+        times.append(t)
+        its.append(k)
+    value = Jt.size * sum(its) / sum(times)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"per step: one {algorithm} solve of the {n}^3 volume from the zero field, it_max={IT}, "
+              f"reference C library (FLOAT_SIZE=64, ORDER_PD=4, OpenMP, verbose output as its "
+              f"Python package builds it) through its C ABI; iterations per step {sorted(set(its))}")
     out = {
-        "impl": "reference", "metric": METRIC_GREEDY if algorithm == "greedy" else METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC_GREEDY if algorithm == "greedy" else METRIC, "value": value,
+        "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * statistics.mean(t[6] + t[1] for t in samples),
+        "ms_per_step": 1000.0 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"config 2: {algorithm} method on {n}^3, 16 Gaussian blobs",
-                   "size": [n, n, n]},
+        "config": {"workload": workload_c2(algorithm, n, IT), "size": [n, n, n], "it_max_per_step": IT,
+                   "iterations_per_step": statistics.mean(its),
+                   "warmup_steps": "it_max=2 solves"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -542,6 +580,50 @@ def run_c3(args, world, rank, local):
         }))
 
 
+def greedy_leg(dt, torch_ops, torch, Jt, mask, field, stream, IT, nvox, world):
+    """The greedy method on the headline volume (same target, mask and
+    it_max): device-timed solves, and its trial kernel's roofline at the 29
+    algorithmic bytes per voxel of a greedy trial (field 12 + target 4 + mask
+    1 in, candidate 12 out)."""
+    def step():
+        field.zero_()
+        return torch_ops.solve(Jt, mask, field, algorithm="greedy", it_max=IT)
+
+    dt.set_profiling(True)
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    dt.set_profiling(True)  # counters cleared
+    k, iters = 3, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        iters += iterations_done(step())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = dt.kernel_profile()
+    dt.set_profiling(False)
+    hbm, peak_kind = peaks()
+    nl, tot = prof.get("trial", (0, 0.0))
+    avg = tot / max(nl, 1)
+    bpl = BYTES_PER_VOXEL_GREEDY["trial"] * nvox
+    achieved = bpl / (avg / 1000.0) / 1e9 if avg > 0 else 0.0
+    traffic = None
+    try:
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["greedy_trial"][
+            "bytes_per_launch_256"]
+    except Exception:
+        traffic = None
+    value = nvox * iters / (ms / 1000.0)
+    return {"metric": METRIC_GREEDY, "value": value, "unit": UNIT, "steps": k,
+            "ms_per_step": ms / k, "iterations_per_step": iters / k,
+            "roofline": {"bound": "hbm", "kernel": "greedy trial", "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": peak_kind, "bytes_per_launch": bpl, "avg_launch_ms": avg,
+                         "launches": nl}}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -626,6 +708,7 @@ def main():
     prof = dt.kernel_profile()
     tiles = dt.tile_config()
     dt.set_profiling(False)
+    field_mixed = field.double().cpu().numpy()  # the last timed solve's result
     ms_max = max_over_ranks(world, ms)
     total_vi = sum_over_ranks(world, float(nvox) * iters)
     value = total_vi / (ms_max / 1000.0)
@@ -676,7 +759,14 @@ def main():
         v64 = nvox * it64 / t64
         fp64 = {"value": v64, "unit": UNIT, "ratio_mixed_over_fp64": (value / world) / v64,
                 "steps": k64}
+        field_fp64 = f64.cpu().numpy()
         del Jt64, f64
+
+    # ---- greedy method on the same volume (gradient workload only): its
+    # trial kernel's roofline at 29 algorithmic bytes per voxel
+    greedy = None
+    if algorithm == "gradient" and not args.no_greedy:
+        greedy = greedy_leg(dt, torch_ops, torch, Jt, mask, field, stream, IT, nvox, world)
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
@@ -717,21 +807,38 @@ def main():
                "d2h_bytes_per_step": int(fh.nbytes), "steps": ke,
                "path": "dtb_generate_displacement (C ABI, host float64 arrays in pinned memory)"}
 
-    # ---- CPU baseline (rank 0, N = 1 only)
+    # ---- CPU baseline (rank 0, N = 1 only): the reference solving the same
+    # volume to the same it_max; its result is the FP64 oracle of `accuracy`
     cpu = None
+    accuracy = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, kind, cores, times = reference_cpu_rate(Jt_np, mask_np, algorithm=algorithm)
-        from oracle.oracle import Reference
+        rate, kind, cores, times, its, field_ref = reference_cpu_rate(Jt_np, mask_np, IT, algorithm=algorithm)
+        from oracle.oracle import Oracle, Reference
         fp32 = None
-        if Reference.available("ref32"):
-            r32, _, _, t32 = reference_cpu_rate(Jt_np, mask_np, algorithm=algorithm, flavour="ref32")
-            fp32 = {"value": r32, "sample": f"the reference's default FP32 build, same solves "
-                                            f"({t32[1]:.2f} s, {t32[6]:.2f} s)"}
+        if Reference.available("ref32_verbose"):
+            r32 = Reference("ref32_verbose")
+            reference_solve(r32, "reference", algorithm, Jt_np, mask_np, min(2, IT))
+            t32, k32, _ = reference_solve(r32, "reference", algorithm, Jt_np, mask_np, IT)
+            fp32 = {"value": nvox * k32 / t32,
+                    "sample": f"the reference's default FP32 build (its Python package's), one solve with "
+                              f"it_max={IT}: {k32} iterations in {t32:.2f} s"}
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "fp32_build": fp32,
-               "sample": f"{n}^3 volume, reference C library FP64 OpenMP, {algorithm} method: "
-                         f"solves with it_max=1 "
-                         f"({times[1]:.2f} s) and it_max=6 ({times[6]:.2f} s); "
-                         f"rate = voxels x 5 / time difference"}
+               "sample": f"{n}^3 volume, {algorithm} method from the zero field, it_max={IT}: reference C "
+                         f"library FP64 (OpenMP) through its C ABI, one warm-up solve (it_max=2), then "
+                         f"{len(times)} solves of {its} iterations in "
+                         f"{', '.join(f'{t:.2f}' for t in times)} s"}
+        # Accuracy against the FP64 oracle: the final masked max |J - J_t| of
+        # each result, its Jacobian recomputed in FP64 by the reference.
+        ref = Reference("ref64") if Reference.available("ref64") else Oracle(4)
+        r_ref = masked_residual(ref.jacobian(field_ref), Jt_np, mask_np)
+        r_mix = masked_residual(ref.jacobian(field_mixed), Jt_np, mask_np)
+        accuracy = {"residual_mixed": r_mix, "residual_oracle": r_ref, "difference": abs(r_mix - r_ref),
+                    "tolerance": 1e-4, "within_tolerance": abs(r_mix - r_ref) <= 1e-4,
+                    "iterations_mixed": iters // max(args.steps, 1), "iterations_oracle": its[-1],
+                    "oracle": f"reference C library FP64 ({kind}), same volume and it_max"}
+        if fp64 is not None:
+            accuracy["fp64_field_max_abs_diff"] = float(np.max(np.abs(field_fp64 - field_ref)))
+            accuracy["residual_fp64"] = masked_residual(ref.jacobian(field_fp64), Jt_np, mask_np)
 
     if rank == 0:
         out = {
@@ -739,9 +846,8 @@ def main():
             "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"config 2: {algorithm} method on {n}^3 (16 Gaussian blobs), "
-                                   f"FP32 field, FP64 reductions, zero initial field, "
-                                   f"it_max={IT} per step",
+            "config": {"workload": workload_c2(algorithm, n, IT),
+                       "precision": "FP32 field and stencils, FP64 reductions and step control",
                        "size": [n, n, n], "it_max_per_step": IT,
                        "l2": "inputs larger than L2 (FP32 field 201 MB + "
                              + ("error map 67 MB + candidate 201 MB)" if algorithm == "greedy"
@@ -762,6 +868,8 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "fp64_plain": fp64,
+            "accuracy": accuracy,
+            "greedy": greedy,
         }
         print(json.dumps(out))
     if world > 1:

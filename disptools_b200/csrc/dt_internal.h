@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "disptools_b200.h"
 
 namespace dtb {
@@ -174,5 +176,21 @@ cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s);
 // captured are not counted; each replay of a graph counts its kernels.
 void count_launch(unsigned n = 1);
 void set_capturing(bool on);
+
+// Opts kernel `fn` in to `bytes` of dynamic shared memory on the current
+// device.  The attribute belongs to one device, so it is set once per device
+// ordinal (bit d of `devs`, one word per kernel at the call site); ordinals
+// from 64 up set it on every call.
+template <typename K>
+inline cudaError_t opt_in_smem(K *fn, int bytes, std::atomic<unsigned long long> &devs) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev >= 0 && dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (devs.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && bit) devs.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 }  // namespace dtb

@@ -568,9 +568,8 @@ template <typename T>
 cudaError_t launch_jacobian(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                             cudaStream_t s) {
     constexpr int smem = jacobian_smem_bytes<T>();
-    // Opt in to the dynamic shared memory once per process.
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_jacobian<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_jacobian<T>, smem, devs);
     if (attr != cudaSuccess) return attr;
     k_jacobian<T><<<grid, dim3(BX, BY), smem, s>>>(vols, tile_vol, total_tiles);
     count_launch();

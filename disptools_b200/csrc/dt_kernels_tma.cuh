@@ -1044,8 +1044,8 @@ template <typename T, int TXW, int TYT>
 cudaError_t launch_trial_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                cudaStream_t s, unsigned char *work_flag, TileQueue *queue, int pf) {
     constexpr int smem = TrialTmaLayout<T, TXW>::BYTES + 128;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_trial_tma<T, TXW, TYT>, smem, devs);
     if (attr != cudaSuccess) return attr;
     k_trial_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue,
                                                                      pf);
@@ -1057,8 +1057,8 @@ template <typename T, int TXW, int TYT>
 cudaError_t launch_greedy_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                 cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
     constexpr int smem = TrialTmaLayout<T, TXW, true>::BYTES + 128;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_trial_tma<T, TXW, TYT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_trial_tma<T, TXW, TYT, true>, smem, devs);
     if (attr != cudaSuccess) return attr;
     k_trial_tma<T, TXW, TYT, true><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag,
                                                                            queue, 0);
@@ -1070,8 +1070,8 @@ template <typename T, int TXW, int TYT>
 cudaError_t launch_gradient_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                   cudaStream_t s, unsigned char *work_flag, TileQueue *queue, int pf) {
     constexpr int smem = GradTmaLayout<T, TXW>::BYTES + 128;
-    static const cudaError_t attr =
-        cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_gradient_tma<T, TXW, TYT>, smem, devs);
     if (attr != cudaSuccess) return attr;
     k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag,
                                                                        queue, pf);
@@ -1413,8 +1413,8 @@ cudaError_t launch_jacobian_tma_v(const CUtensorMap &tm_u, const Geom &g, T *jou
                                   int num_sms, cudaStream_t s, const T *gJ, T *W, long long wn) {
     constexpr int TXW = 32, TYT = 16, BZ = 32;
     constexpr int smem = JacTmaLayout<T, TXW>::BYTES + 128;
-    static const cudaError_t attr = cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT, ADJ>,
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_jacobian_tma<T, TXW, TYT, ADJ>, smem, devs);
     if (attr != cudaSuccess) return attr;
     const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
     const int cols = tiles_x * tiles_y;

@@ -1,20 +1,29 @@
 // Jacobian determinant on device pointers without any allocation.
 //
-// Some callers cannot allocate device memory at the point where they need a
-// Jacobian map: code running while a CUDA stream is being captured into a
-// graph (an allocation there would be recorded or fail), real-time or
-// embedded hosts whose memory budget is fixed when they start, and
-// allocator-less runtimes that hand the library pointers into memory they
-// manage themselves.  dtb_jacobian_device() draws its launch descriptor and
-// tile table from the library's growing device workspace and may call
-// cudaMalloc; this entry point keeps them in a fixed array in device memory
-// that is part of the library image instead.
+// Some callers cannot let a library allocate device memory when they need a
+// Jacobian map:
+// * hosts that fix their device-memory budget at start-up (real-time and
+//   embedded systems), where a later cudaMalloc may fail or, because
+//   cudaMalloc and cudaFree can synchronise the device, stall a loop that
+//   has a deadline;
+// * processes whose device memory is already handed out by another
+//   allocator (a framework's caching allocator that reserved it), so an
+//   allocation of the library's own fails;
+// * runtimes without an allocator of their own, which pass the library
+//   pointers into memory they manage.
+// dtb_jacobian_device() draws its launch descriptor and tile table from the
+// library's growing device workspace and may call cudaMalloc; this entry
+// point keeps them in a fixed array in device memory that is part of the
+// library image instead.
 //
 // The array is `g_noalloc_scratch` below: NOALLOC_SCRATCH_BYTES (65 KiB)
 // that every GPU which loads this library holds until the process exits.  It
 // is shared by every call on a device and keeps the contents of the last
 // call, so two calls whose work overlaps on the GPU (for instance on two
-// streams without ordering between them) race on it.
+// streams without ordering between them) race on it.  The descriptor is
+// written into the array by a one-thread kernel that receives it as a
+// launch argument, and the tile table is cleared by a memset, so nothing is
+// copied from host memory.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -82,6 +91,12 @@ int scratch_address(unsigned char **out) {
     return DTB_OK;
 }
 
+// Writes the launch descriptor into the fixed array.
+template <typename T>
+__global__ void k_store_desc(const VolumeDesc<T> d, VolumeDesc<T> *out) {
+    *out = d;
+}
+
 template <typename T>
 int jacobian_noalloc(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz, int order, const T *field,
                      T *J, cudaStream_t s) {
@@ -125,9 +140,11 @@ int jacobian_noalloc(size_t nx, size_t ny, size_t nz, double dx, double dy, doub
     d.bz = bz;
     VolumeDesc<T> *d_desc = reinterpret_cast<VolumeDesc<T> *>(scratch);
     int *d_tile_vol = reinterpret_cast<int *>(scratch + NOALLOC_DESC_BYTES);
-    // The descriptor comes from pageable host memory: the runtime stages it
-    // before the call returns, so the local `d` may go out of scope.
-    cudaError_t e = cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s);
+    // The descriptor travels as a kernel argument (the launch keeps its own
+    // copy), so `d` may go out of scope as soon as the launch is enqueued.
+    k_store_desc<T><<<1, 1, 0, s>>>(d, d_desc);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
     // Every tile belongs to volume 0: the table must be zero, whatever the
     // previous call left there.
     if (e == cudaSuccess) e = cudaMemsetAsync(d_tile_vol, 0, (size_t) tiles * sizeof(int), s);

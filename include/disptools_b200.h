@@ -260,15 +260,21 @@ int dtb_jacobian_adjoint_device(
     const void *field, const void *grad_J, void *grad_field, void *stream);
 
 /* Jacobian determinant of a device-resident field, like dtb_jacobian_device,
- * but without allocating any memory.  No counterpart in the reference: it is
- * for callers that cannot allocate device memory when they need the map
- * (during stream capture, or on hosts with a fixed memory budget).  Its
- * launch descriptor and tile table live in a 65 KiB array in device memory
- * that belongs to the library and is held by every GPU that loads it; the
- * first call on a device looks up that array's address, so make it before
- * any stream capture.  Volumes up to 16384 tiles of 32 x 8 x 32 voxels
- * (512^3) are accepted; larger ones return DTB_ERR_ARGUMENT.  All calls on
- * a device share the array: calls whose work overlaps on the GPU race. */
+ * but without allocating any memory.  No counterpart in the reference.  It
+ * is for callers that cannot let the library allocate device memory: hosts
+ * that fix their memory budget at start-up (a later cudaMalloc may fail, and
+ * cudaMalloc / cudaFree can synchronise the device and stall a loop with a
+ * deadline), processes whose device memory another allocator has already
+ * reserved, and runtimes that hand the library pointers into memory they
+ * manage.  Its launch descriptor and tile table live in a 65 KiB array in
+ * device memory that belongs to the library and is held by every GPU that
+ * loads it until the process exits.  The first call on a device looks up
+ * that array's address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  Volumes up to 16384 tiles of 32 x 8 x 32 voxels (512^3) are
+ * accepted; larger ones return DTB_ERR_ARGUMENT before any device work.
+ * All calls on a device share the array and it keeps the last call's
+ * contents: calls whose work overlaps on the GPU race, so consecutive calls
+ * on one device must use one stream or be ordered by an event. */
 int dtb_jacobian_device_noalloc(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, void *J, void *stream);

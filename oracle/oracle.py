@@ -61,10 +61,17 @@ class SolveStats:
     eta: float
 
 
+def reference_dir() -> str:
+    """Where the reference checkout lies: $DISPTOOLS_REFERENCE, else the
+    default location of this build environment.  The only place that names
+    it; the GPU-side runs use the libraries already built into _ref/."""
+    return os.environ.get("DISPTOOLS_REFERENCE", "/root/reference")
+
+
 def build(ref: bool | None = None) -> None:
     """Build the oracle (and the reference libraries when the reference
     sources are reachable)."""
-    ref_src = os.environ.get("DISPTOOLS_REFERENCE", "/root/reference")
+    ref_src = reference_dir()
     targets = ["oracle"]
     if ref is None:
         ref = os.path.isdir(os.path.join(ref_src, "src"))
@@ -232,6 +239,34 @@ class Reference:
         nz, ny, nx = J.shape
         self.lib.regularise(nx, ny, nz, _ptr(J), float(epsilon))
         return J
+
+    def solve_logged(self, algorithm, Jt, mask, field=None, spacing=(1.0, 1.0, 1.0), **params):
+        """``solve`` with the library's standard output captured at the file
+        descriptor (the verbose build, ``ref64_verbose``, prints one
+        ``Iteration`` line per pass of its loop, src/displacement_field_gradient.c:378,
+        src/displacement_field_greedy.c:184).  Returns the field, the output
+        lines and the iterations completed: the largest number printed on an
+        ``Iteration`` line (the loop counter; iteration 0 is the initial
+        field, src/displacement_field_gradient.c:272, and the greedy method
+        prints a rejected step again under the same number,
+        src/displacement_field_greedy.c:209-212)."""
+        import sys
+        import tempfile
+        libc = C.CDLL(None)
+        sys.stdout.flush()
+        saved = os.dup(1)
+        with tempfile.TemporaryFile(mode="w+b") as tmp:
+            os.dup2(tmp.fileno(), 1)
+            try:
+                out = self.solve(algorithm, Jt, mask, field, spacing, **params)
+            finally:
+                libc.fflush(None)
+                os.dup2(saved, 1)
+                os.close(saved)
+            tmp.seek(0)
+            lines = tmp.read().decode(errors="replace").splitlines()
+        its = max([int(ln.split()[1].rstrip(":")) for ln in lines if ln.startswith("Iteration ")] or [0])
+        return out, lines, its
 
     def solve(self, algorithm, Jt, mask, field=None, spacing=(1.0, 1.0, 1.0), **params):
         Jt = np.ascontiguousarray(Jt, dtype=self.dtype)

@@ -1,7 +1,9 @@
 """dtb_jacobian_device_noalloc: the Jacobian entry point for callers that
-cannot allocate device memory (during stream capture, or with a fixed memory
-budget).  Its results must equal those of dtb_jacobian_device, call after
-call, although every call reuses the same fixed scratch array.
+cannot let the library allocate device memory — hosts whose memory budget is
+fixed at start-up, processes whose device memory another allocator has
+reserved, runtimes that hand the library pointers into memory they manage.
+Its results must equal those of dtb_jacobian_device and of the FP64 oracle,
+call after call, although every call reuses the same fixed scratch array.
 
 This file is collected last so that a failure here does not stop the rest of
 the suite early."""
@@ -27,7 +29,7 @@ def _jacobians(torch, N, field, spacing, order):
     return ref.cpu().numpy(), new.cpu().numpy()
 
 
-def test_noalloc_matches_allocating_entry_point_on_consecutive_calls():
+def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(oracle, oracle_pd2):
     import torch
     from disptools_b200 import _native as N
     rng = np.random.default_rng(12)
@@ -38,11 +40,18 @@ def test_noalloc_matches_allocating_entry_point_on_consecutive_calls():
              ((3, 9, 5), torch.float64, (2.0, 3.0, 4.0), 2),
              ((21, 34, 45), torch.float64, (0.9, 1.2, 1.05), 4)]
     for shape, dtype, spacing, order in cases:
-        f = torch.from_numpy(rng.normal(scale=0.2, size=(3,) + shape)).to(dtype).cuda()
+        f64 = rng.normal(scale=0.2, size=(3,) + shape)
+        f = torch.from_numpy(f64).to(dtype).cuda()
         ref, new = _jacobians(torch, N, f, spacing, order)
         # same kernel and arithmetic: identical up to the FP64 tolerance of the suite
         rel = np.max(np.abs(new - ref) / np.maximum(np.abs(ref), 1.0))
         assert rel <= 1e-12, (shape, dtype, rel)
+        # and against the oracle on the field the device saw: 1e-12 relative
+        # in FP64, the suite's FP32 bound (1e-4) in FP32
+        o = (oracle if order == 4 else oracle_pd2).jacobian(f.double().cpu().numpy(), spacing)
+        tol = 1e-12 if dtype == torch.float64 else 1e-4
+        rel_o = np.max(np.abs(new - o) / np.maximum(np.abs(o), 1.0))
+        assert rel_o <= tol, (shape, dtype, rel_o)
 
 
 def test_noalloc_rejects_volumes_beyond_its_scratch():
