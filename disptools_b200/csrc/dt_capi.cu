@@ -977,11 +977,43 @@ bool autotune_enabled() {
     return g_autotune != 0;
 }
 
-// Candidate shapes, the fixed default first.
-std::vector<TileConfig> tile_candidates(size_t tsize) {
+// Planes per z tile that fill the waves of a persistent grid of `slots`
+// resident blocks.  The launch is modelled as ceil(tiles / slots) waves of
+// bz + 6 plane-times (a tile forms bz + 4 planes, plus its fixed cost), with
+// tiles(bz) = sum over volumes of (x-y tiles) x ceil(nz / bz); the cheapest
+// bz in [12, 64] wins, the larger one on ties.  At 256^3 with 32 x 16 tiles
+// and 296 slots this gives 29 planes (1152 tiles, 3.9 waves) where 32
+// planes leave the fourth wave less than half full (1024 tiles, 3.5 waves).
+int wave_filled_bz(const std::vector<Geom> &geo, int tile_x, int slots) {
+    int mz = 0;
+    for (const Geom &g : geo) mz = std::max(mz, g.nz);
+    int best = std::min(mz, 32);
+    double best_t = DBL_MAX;
+    for (int bz = std::min(64, mz); bz >= 12; --bz) {
+        long long tiles = 0;
+        for (const Geom &g : geo) {
+            const int b = std::min(bz, g.nz);
+            tiles += (long long) ((g.nx + tile_x - 1) / tile_x) * ((g.ny + TT_Y - 1) / TT_Y) * ((g.nz + b - 1) / b);
+        }
+        const double t = (double) ((tiles + slots - 1) / slots) * (bz + 6);
+        if (t < best_t) {
+            best_t = t;
+            best = bz;
+        }
+    }
+    return best;
+}
+
+// Candidate shapes, the fixed default first; `bzw` (the wave-filled depth of
+// the solve, 0: none) adds the default x-y shapes at that depth.
+std::vector<TileConfig> tile_candidates(size_t tsize, int bzw) {
     std::vector<TileConfig> c = {{32, 16, 16, 32}, {32, 16, 8, 32}, {32, 16, 16, 16}, {32, 16, 16, 64},
                                  {32, 8, 16, 32}};
     if (tsize == 4) c.push_back({64, 16, 8, 32});
+    if (bzw > 0 && bzw != 16 && bzw != 32 && bzw != 64) {
+        c.push_back({32, 16, 16, bzw});
+        c.push_back({32, 16, 8, bzw});
+    }
     return c;
 }
 
@@ -1012,7 +1044,10 @@ int choose_config(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols, 
     NvtxRange range("dtb autotune");
     TileConfig best = c;
     float best_ms = FLT_MAX;
-    for (const TileConfig &cand : tile_candidates(sizeof(T))) {
+    std::vector<Geom> geo;
+    for (const DevVol<T> &v : vols) geo.push_back(v.g);
+    const int slots = std::max(1, trial_tma_blocks_per_sm<T>(32, 16)) * num_sms();
+    for (const TileConfig &cand : tile_candidates(sizeof(T), wave_filled_bz(geo, 32, slots))) {
         float ms = FLT_MAX;
         const int rc = solve_device_on<T>(e, algorithm, vols, p, nullptr, precision, &cand, &ms);
         if (rc != DTB_OK) return rc;

@@ -183,7 +183,7 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, in
     const bool q_vol = q >= 0 && q < g.nz;
     auto ld = [](const T *p) { return *reinterpret_cast<const V4 *>(p); };
     auto el = [](const V4 &v, int e) { return reinterpret_cast<const T *>(&v)[e]; };
-    for (int i = tid; i < NPOS; i += nth) {
+    for (int i = nth - 1 - tid; i < NPOS; i += nth) {  // as greedy_prefetch_stale
         const int ly = i / CPR;
         const int lxc = (i - ly * CPR) * VEC;
         const int gy = y0 - TMA_HY + ly, gx = x0 - TMA_HX + lxc;
@@ -257,7 +257,9 @@ __device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, 
     constexpr int CPR = PX / VEC, NPOS = TMA_PY * CPR;
     if (q < 0 || q >= g.nz) return;
     const bool q_in = q >= 1 && q <= g.nz - 2;
-    for (int i = tid; i < NPOS; i += nth) {
+    // Runs counted from the last thread (the first threads' warp issues the
+    // loads), the same mapping as greedy_form.
+    for (int i = nth - 1 - tid; i < NPOS; i += nth) {
         const int ly = i / CPR;
         const int lxc = (i - ly * CPR) * VEC;
         const int gy = y0 - TMA_HY + ly, gx = x0 - TMA_HX + lxc;
@@ -541,7 +543,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                     greedy_form<T, L>(reinterpret_cast<const T *>(sb), reinterpret_cast<const T *>(sb + L::U_BYTES),
                                       slot, tid, NTH, g, x0, y0, q, s_dd);
                 } else
-                for (int i = tid; i < 3 * TMA_PLANE / VEC; i += NTH) {
+                // Counted from the last thread: the runs left over after
+                // whole sweeps go to the last warps, not to warp 0, whose
+                // thread 0 also issues the loads.
+                for (int i = NTH - 1 - tid; i < 3 * TMA_PLANE / VEC; i += NTH) {
                     V4 a = u4[i];
                     if (trial) {
                         const V4 b = g4[i];

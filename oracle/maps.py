@@ -3,7 +3,8 @@ infrastructure: the checker of disptools_b200.maps).
 
 Follows disptools/displacements.py line by line on NumPy arrays; the
 Jacobians of fields come from the C oracle (dt_oracle.c), which is pinned
-to the reference build.  The reference's NaN handling differs in one
+to the reference build.  Pinned to the reference's own map functions by the
+golden vectors of tests/golden/maps.npz (tests/test_maps_oracle.py).  The reference's NaN handling differs in one
 place: its volume-change map leaves NaN voxels uninitialised (np.empty,
 :658), which this restatement and the device code both return as NaN.
 """

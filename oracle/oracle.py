@@ -76,7 +76,7 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(os.path.join(ref_src, "src"))
     if ref:
-        targets.append("ref")
+        targets += ["ref", "refext"]
     subprocess.check_call(["make", "-s", "-C", HERE, f"REF={ref_src}", *targets])
 
 
@@ -197,6 +197,22 @@ def solver_params(**params):
         else:
             out.append(float(p[k]))
     return out
+
+
+def reference_extension():
+    """The reference's own ``_disptools`` extension module compiled against
+    the drop-in library (``make refext``), or None when it was not built."""
+    import glob
+    import importlib.machinery
+    import importlib.util
+    paths = glob.glob(os.path.join(REF_DIR, "refext", "_disptools*.so"))
+    if not paths:
+        return None
+    loader = importlib.machinery.ExtensionFileLoader("_disptools", paths[0])
+    spec = importlib.util.spec_from_file_location("_disptools", paths[0], loader=loader)
+    mod = importlib.util.module_from_spec(spec)
+    loader.exec_module(mod)
+    return mod
 
 
 class Reference:

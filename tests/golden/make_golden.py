@@ -8,7 +8,13 @@ generate_displacement_greedy, and volume_matching_3d from
 libdisptools_ref64_match) on seeded inputs and stores inputs and outputs
 as small .npz files.  Run it where the reference sources are available:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py --maps   # maps.npz only
+
+maps.npz comes from the reference's own Python map functions
+(disptools/displacements.py), executed from its source with the SimpleITK
+calls answered by a small stand-in (the package needs SimpleITK, which is not
+installed) and its _disptools calls by the reference C library.
 
 Inputs are seeded synthetic data; the shapes mirror the reference's own tests
 (test/test_displacements.py:43-55 uses sin_vector_field(10);
@@ -66,7 +72,123 @@ def small_problem(seed: int, shape):
     return np.ascontiguousarray(Jt), np.ascontiguousarray(mask)
 
 
+class _Image:
+    """The part of a SimpleITK image that the reference's map functions use:
+    the pixel array ([z, y, x] or [z, y, x, 3]), spacing, CopyInformation."""
+
+    def __init__(self, arr, spacing=(1.0, 1.0, 1.0)):
+        self.arr = np.asarray(arr)
+        self.spacing = tuple(spacing)
+
+    def GetSize(self):
+        return tuple(reversed(self.arr.shape[:3]))
+
+    def GetSpacing(self):
+        return self.spacing
+
+    def CopyInformation(self, other):
+        self.spacing = other.spacing
+
+
+def _sitk_stub(files):
+    """SimpleITK calls of disptools/displacements.py:23-95 and :486-668 on
+    _Image objects; `files` maps file names to images (ReadImage).
+    Threshold follows ITK's ThresholdImageFilter with ThresholdOutside:
+    values outside [lower, upper] (NaN included) become outsideValue."""
+    import types
+    st = types.SimpleNamespace()
+    st.Cast = lambda img, t: _Image(np.asarray(img.arr, dtype=np.float64), img.spacing)
+    st.GetArrayViewFromImage = lambda img: img.arr
+    st.GetArrayFromImage = lambda img: np.array(img.arr, copy=True)
+    st.GetImageFromArray = lambda a, isVector=False: _Image(np.array(a, copy=True))
+    st.Image = lambda img: _Image(np.array(img.arr, copy=True), img.spacing)
+    st.ReadImage = lambda f: files[f]
+    st.Threshold = lambda img, lower, upper, outsideValue: _Image(
+        np.where((img.arr >= lower) & (img.arr <= upper), img.arr, outsideValue), img.spacing)
+    return st
+
+
+def reference_map_functions(ref, files):
+    """regularise, jacobian, jacobian_to_volume_change, average_jacobian and
+    average_jacobian_from_displacements, executed from the reference's own
+    source (disptools/displacements.py; extracted with ast, since the package
+    imports SimpleITK, which is not installed).  Their SimpleITK calls go to
+    _sitk_stub, their _disptools calls to the reference C library `ref`."""
+    import ast
+    import fnmatch
+    import logging
+    import re
+    import types
+    from oracle.oracle import reference_dir
+    path = os.path.join(reference_dir(), "disptools", "displacements.py")
+    tree = ast.parse(open(path).read(), path)
+    names = {"regularise", "jacobian", "jacobian_to_volume_change", "average_jacobian",
+             "average_jacobian_from_displacements"}
+    body = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in names]
+    assert {n.name for n in body} == names, "reference functions not found"
+    for n in body:  # annotations name sitk types; not evaluated
+        n.returns = None
+        for a in n.args.args:
+            a.annotation = None
+
+    def c_jacobian(spacing, field, out):
+        out[...] = ref.jacobian(field, spacing)
+
+    def c_regularise(arr, eps):
+        arr[...] = ref.regularise(arr, eps)
+
+    ns = {
+        "np": np, "sitk": _sitk_stub(files), "logging": logging, "re": re,
+        "glob": lambda pat: sorted(f for f in files if fnmatch.fnmatch(f, pat)),
+        "_disptools": types.SimpleNamespace(jacobian=c_jacobian, regularise=c_regularise),
+        "io": types.SimpleNamespace(read_rvf=lambda f: files[f]),
+        "np_float_type": np.float64, "sitk_float_type": None, "sitk_vector_float_type": None,
+    }
+    exec(compile(ast.Module(body=body, type_ignores=[]), path, "exec"), ns)
+    return ns
+
+
+def map_fixtures(ref) -> dict:
+    """Golden vectors of the Jacobian-map utilities (disptools/displacements.py:
+    486-668) and of regularise (src/jacobian.c:29-55), from the reference's
+    own code on seeded maps and fields."""
+    rng = np.random.default_rng(7)
+    out = {}
+    shape = (9, 11, 13)
+    maps = []
+    for k in range(4):
+        J = rng.uniform(-0.2, 2.5, shape)
+        J.flat[:5] = [0.0, 1e-6, 1.0, 2e9, 1e-5]
+        maps.append(J)
+        out[f"map{k}"] = J
+    fields = [rng.normal(scale=0.3, size=(3, 8, 9, 10)) for _ in range(3)]
+    spacing = (0.9, 1.1, 1.3)
+    files = {f"j{k}.vtk": _Image(m) for k, m in enumerate(maps)}
+    # vector images: pixel arrays [z, y, x, 3]
+    files.update({f"u{k}.rvf": _Image(np.moveaxis(f, 0, -1).copy(), spacing) for k, f in enumerate(fields)})
+    for k, f in enumerate(fields):
+        out[f"field{k}"] = f
+    out["spacing"] = np.array(spacing)
+    R = reference_map_functions(ref, files)
+    for eps in (1e-5, 0.3):
+        tag = str(eps).replace(".", "p").replace("-", "m")
+        out[f"volume_change_{tag}"] = R["jacobian_to_volume_change"](_Image(maps[0].copy()), eps).arr
+        out[f"average_jacobian_{tag}"] = R["average_jacobian"]("j*.vtk", eps).arr
+        out[f"average_from_fields_{tag}"] = R["average_jacobian_from_displacements"]("u*.rvf", eps).arr
+    # regularise with NaN and infinities (src/jacobian.c:29-55: J < eps -> eps)
+    Jr = maps[1].copy()
+    Jr.flat[5:9] = [np.nan, -np.inf, np.inf, -0.0]
+    out["regularise_in"] = Jr
+    out["regularise_out_0p05"] = R["regularise"](_Image(Jr.copy()), 0.05).arr
+    return out
+
+
 def main() -> None:
+    if "--maps" in sys.argv:
+        build(ref=True)
+        np.savez_compressed(os.path.join(HERE, "maps.npz"), **map_fixtures(Reference("ref64")))
+        print("map fixtures written to", HERE)
+        return
     if os.environ.get("MALLOC_PERTURB_") != "255":
         # zero-filled mallocs for the reference matching solver (see below)
         os.execve(sys.executable, [sys.executable, os.path.abspath(__file__)],
@@ -161,6 +283,7 @@ def main() -> None:
         mat[f"m{k}_it_max"] = np.array(it_max)
         mat[f"m{k}_out"] = out
     np.savez_compressed(os.path.join(HERE, "matching.npz"), **mat)
+    np.savez_compressed(os.path.join(HERE, "maps.npz"), **map_fixtures(ref))
     print("golden fixtures written to", HERE)
 
 

@@ -1,5 +1,6 @@
 """Jacobian-map utilities on the device against their CPU restatement
-(oracle/maps.py)."""
+(oracle/maps.py), and against golden vectors made by the reference's own map
+functions and regularise (tests/golden/maps.npz)."""
 from __future__ import annotations
 
 import numpy as np
@@ -67,3 +68,36 @@ def test_map_argument_errors():
         M.average_jacobian([], 1e-5)
     with pytest.raises(ValueError):
         M.average_jacobian([np.ones((3, 3, 3)), np.ones((3, 3, 4))])
+
+
+def _golden_maps():
+    import os
+    return dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "maps.npz")))
+
+
+def test_maps_match_reference_functions():
+    """Device results against the reference's own functions
+    (disptools/displacements.py:486-668) on the same inputs."""
+    g = _golden_maps()
+    maps = [g[f"map{k}"] for k in range(4)]
+    fields = [g[f"field{k}"] for k in range(3)]
+    sp = tuple(g["spacing"])
+    for eps, tag in ((1e-5, "1em05"), (0.3, "0p3")):
+        np.testing.assert_array_equal(M.jacobian_to_volume_change(maps[0], eps), g[f"volume_change_{tag}"])
+        np.testing.assert_allclose(M.average_jacobian(maps, eps), g[f"average_jacobian_{tag}"], rtol=1e-14)
+        np.testing.assert_allclose(M.average_jacobian_from_displacements(fields, eps, sp),
+                                   g[f"average_from_fields_{tag}"], rtol=1e-14)
+
+
+def test_regularise_matches_reference_with_nan():
+    """dt.regularise against the reference's regularise (src/jacobian.c:29-55,
+    through its Python wrapper): values below epsilon, -inf and -0.0 become
+    epsilon; NaN and +inf stay."""
+    import disptools_b200 as dt
+    g = _golden_maps()
+    got = dt.regularise(g["regularise_in"], 0.05)
+    np.testing.assert_array_equal(got, g["regularise_out_0p05"])
+    # the reference C library itself, on the same input
+    from oracle.oracle import Reference
+    if Reference.available("ref64"):
+        np.testing.assert_array_equal(got, Reference("ref64").regularise(g["regularise_in"], 0.05))

@@ -27,3 +27,22 @@ def test_average_jacobian_known_values():
 def test_average_jacobian_from_zero_displacements():
     f = np.zeros((3, 4, 5, 6))
     np.testing.assert_array_equal(O.average_jacobian_from_displacements([f, f]), 1.0)
+
+
+def _golden_maps():
+    import os
+    return dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "maps.npz")))
+
+
+def test_restatement_matches_reference_functions():
+    """The restatement against the reference's own map functions
+    (disptools/displacements.py:486-668, executed by tests/golden/make_golden.py)."""
+    g = _golden_maps()
+    maps = [g[f"map{k}"] for k in range(4)]
+    fields = [g[f"field{k}"] for k in range(3)]
+    sp = tuple(g["spacing"])
+    for eps, tag in ((1e-5, "1em05"), (0.3, "0p3")):
+        np.testing.assert_array_equal(O.jacobian_to_volume_change(maps[0], eps), g[f"volume_change_{tag}"])
+        np.testing.assert_allclose(O.average_jacobian(maps, eps), g[f"average_jacobian_{tag}"], rtol=1e-14)
+        np.testing.assert_allclose(O.average_jacobian_from_displacements(fields, eps, sp),
+                                   g[f"average_from_fields_{tag}"], rtol=1e-14)
