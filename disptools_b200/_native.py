@@ -164,6 +164,8 @@ lib.dtb_set_autotune.argtypes = [_I]
 lib.dtb_set_autotune.restype = _I
 lib.dtb_get_tile_config.argtypes = [C.POINTER(C.c_int)]
 lib.dtb_get_tile_config.restype = _I
+lib.dtb_get_trial_kernel.argtypes = []
+lib.dtb_get_trial_kernel.restype = _I
 
 
 class KernelProfile(C.Structure):
@@ -184,7 +186,7 @@ EXPORTED = [
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
     "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
-    "dtb_set_autotune", "dtb_get_tile_config", "dtb_smooth_device", "dtb_resample_device",
+    "dtb_set_autotune", "dtb_get_tile_config", "dtb_get_trial_kernel", "dtb_smooth_device", "dtb_resample_device",
     "dtb_write_rvf", "dtb_read_rvf_header", "dtb_read_rvf", "dtb_write_vtk", "dtb_read_vtk_header",
     "dtb_read_vtk", "dtb_volume_change_device", "dtb_log_jacobian_accumulate_device",
     "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching", "dtb_set_verbose",

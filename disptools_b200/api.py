@@ -158,11 +158,19 @@ def set_autotune(on: bool) -> bool:
     return bool(N.lib.dtb_set_autotune(1 if on else 0))
 
 
+TRIAL_KERNELS = ("formed", "release")
+
+
 def tile_config() -> dict:
-    """Tile shape of the last solve on the current device."""
+    """Tile shape of the last solve on the current device, and its trial
+    kernel: "formed" (candidate planes formed in a shared ring, one block
+    barrier per plane) or "release" (no barrier in the plane loop)."""
     a = (C.c_int * 4)()
     N.check(N.lib.dtb_get_tile_config(a))
-    return {"tile_x": a[0], "trial_threads_y": a[1], "gradient_threads_y": a[2], "bz": a[3]}
+    kind = N.lib.dtb_get_trial_kernel()
+    N.check(min(kind, 0))
+    return {"tile_x": a[0], "trial_threads_y": a[1], "gradient_threads_y": a[2], "bz": a[3],
+            "trial_kernel": TRIAL_KERNELS[kind]}
 
 
 def release_device_memory() -> None:

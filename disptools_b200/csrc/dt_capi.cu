@@ -369,6 +369,7 @@ struct Engine {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};  // the same steps with either set of events and flags
     GraphKey key;
     int last_cfg[4] = {0, 0, 0, 0};  // tile shapes of the last solve (TileConfig order)
+    int last_trial_kind = -1;        // trial kernel of the last solve (TileConfig::trial_kind)
 };
 std::vector<Engine *> g_engines;
 
@@ -444,9 +445,13 @@ bool verbose_enabled() {
 //             columns per thread; 8: two rows)
 //   bz        planes of a tile along z (capped at nz)
 //   pf        L2 prefetch distance in planes beyond each TMA load (0: off)
+//   trial_kind  trial kernel of the gradient method: 0 k_trial_tma (candidate
+//             planes formed in a shared ring, one block barrier per plane),
+//             1 k_trial_rel (stages held until their plane was the centre,
+//             taps formed where read, no barrier in the plane loop)
 // The greedy method runs 32 x TT_Y tiles of bz planes.
 struct TileConfig {
-    int tile_x = 32, trial_ty = 16, grad_ty = 16, bz = 32, pf = 0;
+    int tile_x = 32, trial_ty = 16, grad_ty = 16, bz = 32, pf = 0, trial_kind = 0;
 };
 
 // Explicit shapes from the environment (DISPTOOLS_B200_TILE_X = 32 | 64,
@@ -470,6 +475,14 @@ bool env_config(size_t tsize, TileConfig *c) {
     num("DISPTOOLS_B200_TRIAL_THREADS_Y", &c->trial_ty, {8, 16});
     num("DISPTOOLS_B200_THREADS_Y", &c->grad_ty, {8, 16});
     num("DISPTOOLS_B200_BZ", &c->bz, {});
+    {
+        // DISPTOOLS_B200_TRIAL_KERNEL = formed | release
+        const char *e = std::getenv("DISPTOOLS_B200_TRIAL_KERNEL");
+        if (e && (std::strcmp(e, "formed") == 0 || std::strcmp(e, "release") == 0)) {
+            c->trial_kind = std::strcmp(e, "release") == 0 ? 1 : 0;
+            any = true;
+        }
+    }
     {
         const char *e = std::getenv("DISPTOOLS_B200_PREFETCH");
         if (e) {
@@ -512,6 +525,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     e->last_cfg[1] = cfg.trial_ty;
     e->last_cfg[2] = cfg.grad_ty;
     e->last_cfg[3] = cfg.bz;
+    e->last_trial_kind = cfg.trial_kind;
     // The greedy trial kernel exists for 32-wide tiles only.
     const int tile_x = algorithm == DTB_ALGORITHM_GRADIENT ? cfg.tile_x : 32;
     const int threads_y = cfg.grad_ty;
@@ -695,10 +709,16 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
 
 
     // Persistent grids: as many blocks as fit on the device at once.
-    const int bps_t = gradient ? trial_tma_blocks_per_sm<T>(tile_x, trial_ty) : greedy_tma_blocks_per_sm<T>();
+    const bool rel = gradient && cfg.trial_kind == 1;
+    const int bps_t = !gradient ? greedy_tma_blocks_per_sm<T>()
+                                : (rel ? trial_rel_blocks_per_sm<T>(tile_x, trial_ty)
+                                       : trial_tma_blocks_per_sm<T>(tile_x, trial_ty));
     const int grid_t = std::min(total_tiles, std::max(1, bps_t) * num_sms());
     const int grid_g = std::min(total_tiles, std::max(1, gradient_tma_blocks_per_sm<T>(tile_x, threads_y)) * num_sms());
     auto launch_t = [&](unsigned char *flag) -> cudaError_t {
+        if (rel)
+            return launch_trial_rel<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, trial_ty,
+                                       d_queues);
         if (gradient) return launch_trial_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, tile_x, trial_ty,
                                                     d_queues, cfg.pf);
         return launch_greedy_tma<T>(d_desc, d_tile_vol, total_tiles, grid_t, stream, flag, d_queues);
@@ -755,7 +775,7 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     key.grid_t = grid_t;
     key.grid_g = grid_g;
     key.K = K;
-    key.threads_y = ((trial_ty * 100 + threads_y) * 1000 + tile_x) * 100 + cfg.pf;
+    key.threads_y = (((trial_ty * 100 + threads_y) * 1000 + tile_x) * 100 + cfg.pf) * 2 + (rel ? 1 : 0);
     key.flags = d_flags;
     // Two graphs of the same K steps, each with its own set of profiling
     // events and work flags, so that one replay can be queued while the
@@ -1014,6 +1034,16 @@ std::vector<TileConfig> tile_candidates(size_t tsize, int bzw) {
         c.push_back({32, 16, 16, bzw});
         c.push_back({32, 16, 8, bzw});
     }
+    // the trial kernel without the per-plane barrier, at the default x-y shape
+    for (int bz : {32, bzw > 0 ? bzw : 32, 16})
+        for (int gty : {16, 8}) {
+            const TileConfig t{32, 16, gty, bz, 0, 1};
+            bool dup = false;
+            for (const TileConfig &o : c)
+                dup |= o.tile_x == t.tile_x && o.trial_ty == t.trial_ty && o.grad_ty == t.grad_ty &&
+                       o.bz == t.bz && o.trial_kind == t.trial_kind;
+            if (!dup) c.push_back(t);
+        }
     return c;
 }
 
@@ -1458,6 +1488,16 @@ extern "C" int dtb_get_tile_config(int *shape) {
         DTB_FAIL(DTB_ERR_ARGUMENT, "no solve has run on this device");
     for (int k = 0; k < 4; ++k) shape[k] = g_engines[dev]->last_cfg[k];
     return DTB_OK;
+}
+
+extern "C" int dtb_get_trial_kernel(void) {
+    disptools_clear_error();
+    std::lock_guard<std::mutex> lock(g_ws_mutex);
+    int dev = 0;
+    DTB_CUDA(cudaGetDevice(&dev));
+    if ((int) g_engines.size() <= dev || !g_engines[dev] || g_engines[dev]->last_trial_kind < 0)
+        DTB_FAIL(DTB_ERR_ARGUMENT, "no solve has run on this device");
+    return g_engines[dev]->last_trial_kind;
 }
 
 extern "C" int dtb_release_device_memory(void) {

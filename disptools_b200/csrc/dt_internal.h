@@ -144,6 +144,14 @@ cudaError_t launch_gradient_tma(const VolumeDesc<T> *vols, const int *tile_vol, 
                                 TileQueue *queue, int pf);
 template <typename T>
 int trial_tma_blocks_per_sm(int tile_x, int threads_y);
+// The trial kernel without a per-plane block barrier: stages stay resident
+// until their plane was the stencil's centre, candidate taps are formed where
+// they are read, and the last warp out of a stage issues its refill.
+template <typename T>
+cudaError_t launch_trial_rel(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *queue);
+template <typename T>
+int trial_rel_blocks_per_sm(int tile_x, int threads_y);
 template <typename T>
 int gradient_tma_blocks_per_sm(int tile_x, int threads_y);
 // TMA trial kernel of the greedy method (tiles 32 x TT_Y).

@@ -1045,6 +1045,454 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     }
 }
 
+// ------------------------------------------------------------------------
+// Trial of the gradient method without a per-plane block barrier
+// (k_trial_rel): the work and results of k_trial_tma<T, TXW, TYT, false>
+// with another schedule.
+//
+// Stage j of a tile holds the field and gradient boxes of plane
+// q = z0 - 2 + j (tile + 4 voxels in x, 2 rows in y) and the target and mask
+// tiles of that plane.  A stage stays resident until its plane has been the
+// stencil's centre plane, two iterations after it arrived, so no candidate
+// plane is formed in shared memory: each stencil tap's candidate value
+// u - eta g is formed where it is read (the expression of the formed plane,
+// so FP64 results keep their bits), and each thread forms its own two
+// columns of plane q for its register z-queue and for the store into the
+// other field buffer.
+//
+// There is no block barrier in the plane loop.  A warp that has read a stage
+// for the last time counts itself out of it (a shared counter); the warp that
+// counts out last issues the stage's next load, the plane S iterations
+// later, into the same slot.  So a warp waits only for data, and a slow warp
+// delays only the refill of the stages it still reads.  A wait that runs out
+// sets a block-wide fault flag that the other warps see at their next plane
+// (or their own waits run out); one block barrier per tile, after the loop,
+// agrees on it before the block reports the fault, waits (bounded) for its
+// loads in flight and leaves.
+// ------------------------------------------------------------------------
+template <typename T, int TXW>
+struct TrialRelLayout {
+    static constexpr int TMA_PX = Box<TXW>::PX;
+    static constexpr int TMA_PLANE = Box<TXW>::PLANE;
+    static constexpr int S = 5;  // planes in use (centre, centre + 1, centre + 2) and two in flight
+    static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
+    static constexpr int G_OFF = U_BYTES;
+    static constexpr int JT_BYTES = TXW * TT_Y * (int) sizeof(T);
+    static constexpr int MASK_BYTES = TXW * TT_Y;
+    static constexpr int JT_OFF = 2 * U_BYTES;
+    static constexpr int MASK_OFF = JT_OFF + JT_BYTES;
+    static constexpr int STAGE_BYTES = MASK_OFF + MASK_BYTES;  // u, g, Jt, mask
+    static_assert(STAGE_BYTES % 128 == 0, "stages stay 128-byte aligned");
+    static constexpr int BAR_OFF = S * STAGE_BYTES;
+    static constexpr int CNT_OFF = BAR_OFF + S * 8;
+    static constexpr int BYTES = CNT_OFF + S * 4;
+};
+
+// Orders this thread's earlier shared-memory accesses (and those ordered
+// before them) before its later async-proxy (TMA) writes to shared memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Candidate pair u - eta g of two adjacent x voxels (box offset o).
+template <typename T>
+__device__ __forceinline__ typename PairOf<T>::type cand_pair(const T *u, const T *g, int o, T eta) {
+    const auto a = ld_pair(u + o), b = ld_pair(g + o);
+    typename PairOf<T>::type c;
+    c.x = a.x - eta * b.x;
+    c.y = a.y - eta * b.y;
+    return c;
+}
+
+template <typename T, int TXW, int TYT>
+__global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof(T) == 4) ? 2 : 1)
+    k_trial_rel(const VolumeDesc<T> *__restrict__ vols, const int *__restrict__ tile_vol, int total_tiles,
+                unsigned char *__restrict__ work_flag, TileQueue *queue) {
+    using L = TrialRelLayout<T, TXW>;
+    constexpr int TPX = TXW / 2, NTH = TPX * TYT, RYT = TT_Y / TYT, NW = NTH / 32, S = L::S;
+    constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
+    static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
+    static_assert(NTH % 32 == 0, "whole warps");
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem = align_smem_128(smem_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    unsigned *cnt = reinterpret_cast<unsigned *>(smem + L::CNT_OFF);
+    __shared__ double red[2 * NW];
+    __shared__ int s_flag, s_tile;
+    __shared__ int s_issued;  // loads issued for the current tile (iterations 0 .. s_issued - 1)
+    __shared__ volatile int s_fault;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx, lane = tid & 31;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&bars[s], 1);
+            cnt[s] = 0;
+        }
+        fence_mbar_init();
+        s_fault = 0;
+    }
+    __syncthreads();
+    uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
+
+    // The current tile's load parameters: any warp may issue a refill, so
+    // they sit in shared memory rather than in every thread's registers.
+    __shared__ const CUtensorMap *s_tm[4];  // field, gradient, target, mask
+    __shared__ int s_box[4];                // x0, y0, z0, z1
+    __shared__ int s_drop;                  // iteration whose loads are dropped (failure-path test), or -1
+    __shared__ int s_done, s_phase, s_old;
+    __shared__ double s_eta;
+    for (int tile = take_tile<TPX>(queue, total_tiles, &s_tile); tile >= 0;
+         tile = take_tile<TPX>(queue, total_tiles, &s_tile)) {
+        const VolumeDesc<T> &V = vols[tile_vol[tile]];
+        SolverState *st = V.st;
+        const Geom g = V.g;
+        const int lt = tile - V.tile_begin;
+        const int txi = lt % V.tiles_x, tyi = (lt / V.tiles_x) % V.tiles_y, tzi = lt / (V.tiles_x * V.tiles_y);
+        const int x0 = txi * TXW, y0 = tyi * TT_Y, z0 = tzi * V.bz;
+        const int z1 = min(z0 + V.bz, g.nz);
+        const int n_it = z1 - z0 + 4;  // planes z0-2 .. z1+1
+        // The volume's state, read once for the whole block: every warp takes
+        // the same path through the tile.
+        if (tid == 0) {
+            s_done = ldcg_int(&st->done);
+            s_phase = ldcg_int(&st->phase);
+            s_old = ldcg_int(&st->old_buf);
+            s_eta = __ldcg(&st->eta);
+            s_tm[0] = V.tm_field[s_old];
+            s_tm[1] = V.tm_grad;
+            s_tm[2] = V.tm_Jt;
+            s_tm[3] = V.tm_mask;
+            s_box[0] = x0;
+            s_box[1] = y0;
+            s_box[2] = z0;
+            s_box[3] = z1;
+            s_drop = (s_phase != PH_EVAL0 && tile == V.drop_tile) ? V.drop_it : -1;
+            s_issued = 0;
+        }
+        __syncthreads();
+        if (s_done) continue;
+        const int phase = s_phase;
+        const int old_b = s_old;
+        const double eta = s_eta;
+        const bool trial = phase != PH_EVAL0;
+        T *dst = V.field[old_b ^ 1];
+        T *ep_out = V.ep[trial ? old_b ^ 1 : old_b];  // e' of the evaluated field
+        // The launch that evaluates the initial field takes it as it is:
+        // eta 0 over the gradient buffer, which the set-up zeroed.
+        const T eta_t = trial ? (T) eta : T(0);
+        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+        const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
+        const unsigned wait_limit = V.wait_limit ? V.wait_limit : (1u << 22);
+
+        // Issues the loads of iteration j (plane z0-2+j) into its slot (one
+        // thread; the tile's parameters come from shared memory).
+        auto issue = [&](int j) {
+            atomicMax(&s_issued, j + 1);
+            if (j == s_drop) return;  // failure-path test only
+            const uint32_t k = kbase + j;
+            const int s = k % S;
+            unsigned char *sb = smem + s * L::STAGE_BYTES;
+            const int bx = s_box[0], by = s_box[1], bz0 = s_box[2], q = bz0 - 2 + j;
+            const bool with_target = q >= bz0 && q < s_box[3];
+            mbar_arrive_expect_tx(&bars[s], 2 * L::U_BYTES + (with_target ? L::JT_BYTES + L::MASK_BYTES : 0));
+            tma_load_4d(sb, s_tm[0], &bars[s], bx - TMA_HX, by - TMA_HY, q, 0);
+            tma_load_4d(sb + L::G_OFF, s_tm[1], &bars[s], bx - TMA_HX, by - TMA_HY, q, 0);
+            if (with_target) {
+                tma_load_3d(sb + L::JT_OFF, s_tm[2], &bars[s], bx, by, q);
+                tma_load_3d(sb + L::MASK_OFF, s_tm[3], &bars[s], bx, by, q);
+            }
+        };
+        // This warp has read iteration j's stage for the last time; the last
+        // warp to say so issues the loads of iteration j + S into the slot.
+        auto release = [&](int j) {
+            __syncwarp();
+            if (lane == 0) {
+                const int s = (kbase + j) % S;
+                __threadfence_block();
+                if (atomicAdd(&cnt[s], 1u) == (unsigned) (NW - 1)) {
+                    cnt[s] = 0;
+                    __threadfence_block();
+                    fence_proxy_async_smem();
+                    issue(j + S);
+                }
+            }
+        };
+        if (tid == 0) {
+            for (int m = 0; m < 4; ++m) tmap_acquire(s_tm[m]);
+            for (int j = 0; j < min(S, n_it); ++j) issue(j);
+        }
+
+        const int x = x0 + 2 * tx;       // this thread's columns: x, x + 1
+        const int lx = 2 * tx + TMA_HX;  // their box column
+        const bool pair_in = x + 1 < g.nx;
+        const bool tile_x_in = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3;
+        // Own columns: candidate values of planes q-4 .. q (z differences).
+        T zq[RYT][2][3][5];
+#pragma unroll
+        for (int r = 0; r < RYT; ++r)
+#pragma unroll
+            for (int v = 0; v < 2; ++v)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
+        double acc_s = 0.0;
+        T acc_mt = T(0);
+        long long qoff = (long long) (z0 - 2) * g.zs;  // offset of plane q
+        for (int it = 0; it < n_it; ++it, qoff += g.zs) {
+            if (s_fault) break;
+            const uint32_t k = kbase + it;
+            if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u, wait_limit)) {
+                s_fault = 1;
+                break;
+            }
+            const T *su = reinterpret_cast<const T *>(smem + (k % S) * L::STAGE_BYTES);
+            const T *sg = su + L::G_OFF / (int) sizeof(T);
+            const int q = z0 - 2 + it, ze = q - 2;
+            // Own columns of plane q: shift the z-queues, store the candidate.
+#pragma unroll
+            for (int r = 0; r < RYT; ++r) {
+                const int ly = ty + r * TYT + TMA_HY;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const auto nv = cand_pair(su, sg, c * TMA_PLANE + ly * TMA_PX + lx, eta_t);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        zq[r][0][c][kk] = zq[r][0][c][kk + 1];
+                        zq[r][1][c][kk] = zq[r][1][c][kk + 1];
+                    }
+                    zq[r][0][c][4] = nv.x;
+                    zq[r][1][c][4] = nv.y;
+                }
+                const int y = y0 + ty + r * TYT;
+                if (trial && x < g.nx && y < g.ny && q >= z0 && q < z1) {
+                    T *o = dst + qoff + (long long) y * g.ys + x;
+                    if (pair_in) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, zq[r][0][c][4], zq[r][1][c][4]);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) o[c * g.cs] = zq[r][0][c][4];
+                    }
+                }
+            }
+            if (ze >= z0 && ze < z1) {
+                // Plane ze is iteration it - 2's stage.
+                const unsigned char *se = smem + ((k - 2) % S) * L::STAGE_BYTES;
+                const T *eu = reinterpret_cast<const T *>(se);
+                const T *eg = eu + L::G_OFF / (int) sizeof(T);
+                const bool plane_in = ze >= 2 && ze <= g.nz - 3;
+                // Fourth-order weights with the spacing folded in (FP32); the
+                // FP64 path keeps the reference's operation order.
+                const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
+                const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1],
+                                 FD<T>::one_twelfth * ih[2]};
+                auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
+                    if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+                    return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
+                };
+#pragma unroll
+                for (int r = 0; r < RYT; ++r) {
+                    const int y = y0 + ty + r * TYT;
+                    const bool row_in = plane_in && y >= 2 && y <= g.ny - 3;
+                    const int ly = ty + r * TYT + TMA_HY;
+                    if (x >= g.nx || y >= g.ny) continue;
+                    const int ot = (ty + r * TYT) * TXW + 2 * tx;
+                    const auto j2 = ld_pair(reinterpret_cast<const T *>(se + L::JT_OFF) + ot);
+                    const unsigned short m2 = *reinterpret_cast<const unsigned short *>(se + L::MASK_OFF + ot);
+                    const T jt[2] = {j2.x, j2.y};
+                    const bool msk[2] = {(m2 & 0xffu) != 0, (m2 >> 8) != 0};
+                    T epv[2];
+                    // Error terms of voxel v from its Jacobian determinant.
+                    auto finish_j = [&](int v, const T J) {
+                        const T vv = voxel_error<T>(J, jt[v], msk[v], tol);
+                        acc_s += (double) vv * (double) vv;
+                        const T av = fabs(vv);  // the maximum is exact in the element type
+                        if (msk[v] && av > acc_mt) acc_mt = av;
+                        T ep = vv;
+                        if (J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
+                        epv[v] = ep;
+                    };
+                    auto finish = [&](int v, const T (&a)[3][3]) { finish_j(v, det_i_plus<T>(a)); };
+                    if (row_in && tile_x_in) {
+                        // Row c of both voxels' matrices (fourth order throughout).
+                        auto row = [&](int c, T (&m)[2][3]) {
+                            const int o = c * TMA_PLANE + ly * TMA_PX + lx;
+                            const T *zc0 = zq[r][0][c], *zc1 = zq[r][1][c];  // own values: planes ze-2 .. ze+2
+                            const auto xm = cand_pair(eu, eg, o - 2, eta_t), xp = cand_pair(eu, eg, o + 2, eta_t);
+                            m[0][0] = c4(zc1[2], xm.y, xp.x, xm.x, 0);
+                            m[1][0] = c4(xp.x, zc0[2], xp.y, xm.y, 0);
+                            const auto ym1 = cand_pair(eu, eg, o - TMA_PX, eta_t);
+                            const auto yp1 = cand_pair(eu, eg, o + TMA_PX, eta_t);
+                            const auto ym2 = cand_pair(eu, eg, o - 2 * TMA_PX, eta_t);
+                            const auto yp2 = cand_pair(eu, eg, o + 2 * TMA_PX, eta_t);
+                            m[0][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
+                            m[1][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+                            m[0][2] = c4(zc0[3], zc0[1], zc0[4], zc0[0], 2);
+                            m[1][2] = c4(zc1[3], zc1[1], zc1[4], zc1[0], 2);
+                        };
+                        // det_i_plus's operations in its order, rows 1 and 2
+                        // folded into the cofactors of row 0 before row 0 is
+                        // formed, so fewer values are live at once.
+                        T cf[2][3];
+                        {
+                            T m1[2][3], m2[2][3];
+                            row(1, m1);
+                            row(2, m2);
+#pragma unroll
+                            for (int v = 0; v < 2; ++v) {
+                                const T a21 = m1[v][0], a22 = m1[v][1] + T(1.0), a23 = m1[v][2];
+                                const T a31 = m2[v][0], a32 = m2[v][1], a33 = m2[v][2] + T(1.0);
+                                cf[v][0] = a22 * a33 - a23 * a32;
+                                cf[v][1] = a21 * a33 - a23 * a31;
+                                cf[v][2] = a21 * a32 - a22 * a31;
+                            }
+                        }
+                        T m0[2][3];
+                        row(0, m0);
+#pragma unroll
+                        for (int v = 0; v < 2; ++v) {
+                            const T a11 = m0[v][0] + T(1.0), a12 = m0[v][1], a13 = m0[v][2];
+                            finish_j(v, a11 * cf[v][0] - a12 * cf[v][1] + a13 * cf[v][2]);
+                        }
+                    } else {
+                        // Interior rows of a tile that reaches an x end, and the
+                        // two outer layers: the case analysis per voxel
+                        // (src/jacobian.c:113-241), taps formed one by one.
+#pragma unroll
+                        for (int v = 0; v < 2; ++v) {
+                            const int xv = x + v;
+                            if (xv >= g.nx) continue;
+                            auto tap = [&](int c, int d) -> T {
+                                const int o = c * TMA_PLANE + ly * TMA_PX + lx + v + d;
+                                return eu[o] - eta_t * eg[o];
+                            };
+                            T a[3][3];
+                            if (row_in) {
+                                const bool xo_lo = xv == 0, xo_hi = xv == g.nx - 1;
+                                const bool second = xo_lo || xo_hi || xv == 1 || xv == g.nx - 2;
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    const T p0 = zq[r][v][c][2];
+                                    const T pm1 = tap(c, -1), pp1 = tap(c, 1), pm2 = tap(c, -2), pp2 = tap(c, 2);
+                                    const T fx = xo_lo ? fd_fwd<T>(p0, pp1, pp2, ih[0])
+                                                       : (xo_hi ? fd_bwd<T>(p0, pm1, pm2, ih[0])
+                                                                : fd_c2<T>(pp1, pm1, ih[0]));
+                                    const T cx4 = c4(pp1, pm1, pp2, pm2, 0);
+                                    a[c][0] = second ? fx : cx4;
+                                    const T ym1 = tap(c, -TMA_PX), yp1 = tap(c, TMA_PX);
+                                    const T ym2 = tap(c, -2 * TMA_PX), yp2 = tap(c, 2 * TMA_PX);
+                                    const T cy4 = c4(yp1, ym1, yp2, ym2, 1);
+                                    const T cy2 = fd_c2<T>(yp1, ym1, ih[1]);
+                                    a[c][1] = second ? cy2 : cy4;
+                                    const T *zv = zq[r][v][c];
+                                    const T cz4 = c4(zv[3], zv[1], zv[4], zv[0], 2);
+                                    const T cz2 = fd_c2<T>(zv[3], zv[1], ih[2]);
+                                    a[c][2] = second ? cz2 : cz4;
+                                }
+                            } else {
+                                int kk[3];
+                                schemes_at(xv, y, ze, g, kk);
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    const T p0 = zq[r][v][c][2];
+                                    const T vx[5] = {tap(c, -2), tap(c, -1), p0, tap(c, 1), tap(c, 2)};
+                                    const T vy[5] = {tap(c, -2 * TMA_PX), tap(c, -TMA_PX), p0, tap(c, TMA_PX),
+                                                     tap(c, 2 * TMA_PX)};
+#pragma unroll
+                                    for (int ax = 0; ax < 3; ++ax) {
+                                        const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[r][v][c]);
+                                        T d;
+                                        switch (kk[ax]) {
+                                        case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
+                                        case S_BWD: d = fd_bwd<T>(w[2], w[1], w[0], ih[ax]); break;
+                                        case S_C2: d = fd_c2<T>(w[3], w[1], ih[ax]); break;
+                                        default: d = c4(w[3], w[1], w[4], w[0], ax); break;
+                                        }
+                                        a[c][ax] = d;
+                                    }
+                                }
+                            }
+                            finish(v, a);
+                        }
+                    }
+                    T *o = ep_out + (qoff - 2 * g.zs) + (long long) y * g.ys + x;
+                    if (pair_in)
+                        st_pair(o, epv[0], epv[1]);
+                    else
+                        o[0] = epv[0];
+                }
+            }
+            // Iteration it - 2's stage is not read again; count out of it
+            // when its slot has a later plane of this tile to take.
+            if (it >= 2 && it - 2 + S < n_it) release(it - 2);
+        }
+        __syncthreads();  // every warp has left the plane loop
+        if (s_fault) {
+            if (tid == 0) {
+                atomicExch(&st->fault, 1);
+                atomicExch(&st->done, 1);
+                // The last load issued into each slot: wait (bounded) until it
+                // has landed, so nothing arrives after the block has left.
+                const int to = s_issued;
+                for (int j = max(0, to - S); j < to; ++j) {
+                    const uint32_t kk = kbase + j;
+                    mbar_wait_bounded(&bars[kk % S], (kk / S) & 1u, 1u << 16);
+                }
+            }
+            __syncthreads();
+            return;
+        }
+        kbase += n_it;
+
+        const double2 rr = block_reduce_n<NTH, TPX>(acc_s, (double) acc_mt, red);
+        if (tid == 0) V.part_t[lt] = rr;
+        if (publish_partial_n<TPX>(&st->ticket_t, V.ntiles, &s_flag)) {
+            // Each thread folds a fixed subset of the tile partials, so the
+            // total does not depend on timing.
+            double ssum = 0.0, smax = 0.0;
+            for (int i = tid; i < V.ntiles; i += NTH) {
+                const double2 pp = __ldcg(&V.part_t[i]);
+                ssum += pp.x;
+                smax = fmax(smax, pp.y);
+            }
+            const double2 tot = block_reduce_n<NTH, TPX>(ssum, smax, red);
+            if (tid == 0) {
+                st->ticket_t = 0;
+                control_after_trial(st, tot.x, tot.y);
+                if (work_flag) *work_flag = 1;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int TXW, int TYT>
+cudaError_t launch_trial_rel_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                               cudaStream_t s, unsigned char *work_flag, TileQueue *queue) {
+    constexpr int smem = TrialRelLayout<T, TXW>::BYTES + 128;
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_trial_rel<T, TXW, TYT>, smem, devs);
+    if (attr != cudaSuccess) return attr;
+    k_trial_rel<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag, queue);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, int TXW, int TYT>
+int trial_rel_blocks_v() {
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_trial_rel<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TrialRelLayout<T, TXW>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_trial_rel<T, TXW, TYT>, TXW / 2 * TYT,
+                                                      TrialRelLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return n;
+}
+
 template <typename T, int TXW, int TYT>
 cudaError_t launch_trial_tma_v(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
                                cudaStream_t s, unsigned char *work_flag, TileQueue *queue, int pf) {
@@ -1140,6 +1588,24 @@ cudaError_t launch_trial_tma(const VolumeDesc<T> *vols, const int *tile_vol, int
             return launch_trial_tma_v<T, 64, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
     if (threads_y == 8) return launch_trial_tma_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
     return launch_trial_tma_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q, pf);
+}
+
+// Trial kernel without the per-plane barrier (same tile shapes as
+// launch_trial_tma, no L2 prefetch option).
+template <typename T>
+cudaError_t launch_trial_rel(const VolumeDesc<T> *vols, const int *tile_vol, int total_tiles, int grid,
+                             cudaStream_t s, unsigned char *work_flag, int tile_x, int threads_y, TileQueue *q) {
+    if constexpr (sizeof(T) == 4)
+        if (tile_x == 64) return launch_trial_rel_v<T, 64, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    if (threads_y == 8) return launch_trial_rel_v<T, 32, 8>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+    return launch_trial_rel_v<T, 32, 16>(vols, tile_vol, total_tiles, grid, s, work_flag, q);
+}
+
+template <typename T>
+int trial_rel_blocks_per_sm(int tile_x, int threads_y) {
+    if constexpr (sizeof(T) == 4)
+        if (tile_x == 64) return trial_rel_blocks_v<T, 64, 16>();
+    return threads_y == 8 ? trial_rel_blocks_v<T, 32, 8>() : trial_rel_blocks_v<T, 32, 16>();
 }
 
 template <typename T>
@@ -1454,6 +1920,9 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
     template int greedy_tma_blocks_per_sm<T>();                                                             \
     template cudaError_t launch_jacobian_tma<T>(const CUtensorMap &, const Geom &, T *, long long, long long, int, \
                                                 cudaStream_t, const T *, T *, long long);                   \
-    template int gradient_tma_blocks_per_sm<T>(int, int);
+    template int gradient_tma_blocks_per_sm<T>(int, int);                                                   \
+    template cudaError_t launch_trial_rel<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
+                                             unsigned char *, int, int, TileQueue *);                       \
+    template int trial_rel_blocks_per_sm<T>(int, int);
 
 }  // namespace dtb

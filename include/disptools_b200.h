@@ -424,6 +424,16 @@ int dtb_set_autotune(int on);
  * DTB_ERR_ARGUMENT before the first solve on the device. */
 int dtb_get_tile_config(int shape[4]);
 
+/* Trial kernel of the last gradient-method solve on the current device: 0
+ * for the kernel that forms each candidate plane in a shared ring (one
+ * block barrier per plane), 1 for the kernel that keeps each stage until its
+ * plane was the stencil's centre, forms the candidate's taps where it reads
+ * them and has no barrier in its plane loop.  The autotuner chooses between
+ * them; DISPTOOLS_B200_TRIAL_KERNEL = formed | release forces one.  Returns
+ * DTB_ERR_ARGUMENT before the first solve on the device.  No counterpart in
+ * the reference. */
+int dtb_get_trial_kernel(void);
+
 /* Frees the device memory the library keeps on the current device between
  * calls: the solver's workspace (pitched field buffers, descriptors, tile
  * partials) and the staging area of host-array calls, both of which grow to

@@ -35,11 +35,15 @@ def test_memory_limit_refuses_then_recovers():
     np.testing.assert_array_equal(good, again)
 
 
-@pytest.mark.parametrize("algorithm", ["gradient", "greedy"])
+@pytest.mark.parametrize("algorithm,trial_kernel", [("gradient", "formed"), ("gradient", "release"),
+                                                    ("greedy", "formed")])
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_dropped_tma_load_is_reported_and_device_recovers(precision, algorithm):
+def test_dropped_tma_load_is_reported_and_device_recovers(precision, algorithm, trial_kernel, monkeypatch):
     """The greedy trial also has element copies of the boundary values in
-    flight when its wait runs out; they complete before the block leaves."""
+    flight when its wait runs out; they complete before the block leaves.
+    The trial kernel without a plane barrier agrees on the fault after its
+    plane loop and waits for the last load of each slot."""
+    monkeypatch.setenv("DISPTOOLS_B200_TRIAL_KERNEL", trial_kernel)
     Jt, m = ball_problem(40, 20, 9, 1.1)
     good, sg = dt.solve(Jt, m, precision=precision, algorithm=algorithm, it_max=15)
     N.check(N.lib.dtb_test_drop_tma_load(0, 5, 1 << 12))

@@ -113,6 +113,21 @@ def test_edge_cases_fp64_vs_oracle(oracle, name, algorithm):
     assert np.max(np.abs(out - ref)) <= 1e-10
 
 
+@pytest.mark.parametrize("trial_kernel", ["formed", "release"])
+@pytest.mark.parametrize("name", sorted(EDGE_CASES))
+def test_edge_cases_fp64_both_trial_kernels(oracle, monkeypatch, name, trial_kernel):
+    """The gradient method's edge cases through each trial kernel, forced."""
+    monkeypatch.setenv("DISPTOOLS_B200_TRIAL_KERNEL", trial_kernel)
+    test_edge_cases_fp64_vs_oracle(oracle, name, "gradient")
+    assert dt.tile_config()["trial_kernel"] == trial_kernel
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_equals_single_release_kernel(monkeypatch, precision):
+    monkeypatch.setenv("DISPTOOLS_B200_TRIAL_KERNEL", "release")
+    test_batched_equals_single(precision, "gradient")
+
+
 @pytest.mark.parametrize("shape", [(37, 45, 70), (70, 18, 33), (9, 40, 131)])
 def test_greedy_multi_tile_fp64_vs_oracle(oracle, shape):
     """Greedy trials over several tiles along every axis, x extents that end
@@ -269,13 +284,27 @@ def test_release_device_memory_then_solve_again():
 
 
 TILE_CANDIDATES = [
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 32},
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 16},
-    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 64},
-    {"tile_x": 32, "trial_threads_y": 8, "gradient_threads_y": 16, "bz": 32},
-    {"tile_x": 64, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 32, "trial_kernel": "formed"},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32, "trial_kernel": "formed"},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 16, "trial_kernel": "formed"},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 64, "trial_kernel": "formed"},
+    {"tile_x": 32, "trial_threads_y": 8, "gradient_threads_y": 16, "bz": 32, "trial_kernel": "formed"},
+    {"tile_x": 64, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32, "trial_kernel": "formed"},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 32, "trial_kernel": "release"},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 16, "trial_kernel": "release"},
+    {"tile_x": 32, "trial_threads_y": 16, "gradient_threads_y": 16, "bz": 29, "trial_kernel": "release"},
+    {"tile_x": 32, "trial_threads_y": 8, "gradient_threads_y": 16, "bz": 32, "trial_kernel": "release"},
+    {"tile_x": 64, "trial_threads_y": 16, "gradient_threads_y": 8, "bz": 32, "trial_kernel": "release"},
 ]
+ENV_OF = (("TILE_X", "tile_x"), ("TRIAL_THREADS_Y", "trial_threads_y"), ("THREADS_Y", "gradient_threads_y"),
+          ("BZ", "bz"), ("TRIAL_KERNEL", "trial_kernel"))
+
+
+def _is_candidate(cfg) -> bool:
+    """A shape the autotuner may choose: a listed x-y shape and kernel, and a
+    z depth that is listed or wave-filled (12..64 planes)."""
+    key = lambda c: (c["tile_x"], c["trial_threads_y"], c["gradient_threads_y"], c["trial_kernel"])  # noqa: E731
+    return any(key(c) == key(cfg) for c in TILE_CANDIDATES) and 12 <= cfg["bz"] <= 64
 
 
 def test_autotuned_shapes(oracle, monkeypatch):
@@ -293,14 +322,12 @@ def test_autotuned_shapes(oracle, monkeypatch):
         cfg32 = dt.tile_config()
     finally:
         dt.set_autotune(prev)
-    assert cfg64 in TILE_CANDIDATES and cfg64["tile_x"] == 32
-    assert cfg32 in TILE_CANDIDATES
+    assert _is_candidate(cfg64) and cfg64["tile_x"] == 32
+    assert _is_candidate(cfg32)
     ref, _ = oracle.solve("gradient", Jt, mask, it_max=3)
     assert np.max(np.abs(out64 - ref)) <= 1e-10
-    monkeypatch.setenv("DISPTOOLS_B200_TILE_X", str(cfg32["tile_x"]))
-    monkeypatch.setenv("DISPTOOLS_B200_TRIAL_THREADS_Y", str(cfg32["trial_threads_y"]))
-    monkeypatch.setenv("DISPTOOLS_B200_THREADS_Y", str(cfg32["gradient_threads_y"]))
-    monkeypatch.setenv("DISPTOOLS_B200_BZ", str(cfg32["bz"]))
+    for k, v in ENV_OF:
+        monkeypatch.setenv("DISPTOOLS_B200_" + k, str(cfg32[v]))
     again, _ = dt.solve(Jt, mask, precision="mixed", it_max=6)
     assert dt.tile_config() == cfg32
     np.testing.assert_array_equal(out32, again)
@@ -312,8 +339,7 @@ def test_every_tile_shape_fp64_matches_oracle(oracle, monkeypatch, shape):
     oracle's FP64 result on a volume with ragged tiles in every axis."""
     if shape["tile_x"] == 64:
         pytest.skip("64-wide tiles are FP32 only")
-    for k, v in (("TILE_X", "tile_x"), ("TRIAL_THREADS_Y", "trial_threads_y"),
-                 ("THREADS_Y", "gradient_threads_y"), ("BZ", "bz")):
+    for k, v in ENV_OF:
         monkeypatch.setenv("DISPTOOLS_B200_" + k, str(shape[v]))
     Jt, mask = ball_problem(45, 20, 9, 0.9)
     out, st = dt.solve(Jt, mask, precision="fp64", it_max=40)
@@ -325,8 +351,7 @@ def test_every_tile_shape_fp64_matches_oracle(oracle, monkeypatch, shape):
 
 @pytest.mark.parametrize("shape", TILE_CANDIDATES)
 def test_every_tile_shape_mixed_residual(oracle, monkeypatch, shape):
-    for k, v in (("TILE_X", "tile_x"), ("TRIAL_THREADS_Y", "trial_threads_y"),
-                 ("THREADS_Y", "gradient_threads_y"), ("BZ", "bz")):
+    for k, v in ENV_OF:
         monkeypatch.setenv("DISPTOOLS_B200_" + k, str(shape[v]))
     Jt, mask = ball_problem(45, 20, 9, 0.9)
     out, st = dt.solve(Jt, mask, precision="mixed", it_max=1000)
