@@ -128,6 +128,8 @@ lib.dtb_release_device_memory.argtypes = []
 lib.dtb_release_device_memory.restype = _I
 lib.dtb_smooth_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
 lib.dtb_smooth_device.restype = _I
+lib.dtb_smooth_recursive_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
+lib.dtb_smooth_recursive_device.restype = _I
 lib.dtb_resample_device.argtypes = [_I, _I, _I, _SZ, _SZ, _SZ, _SZ, _SZ, _SZ, _P, _P, _P]
 lib.dtb_resample_device.restype = _I
 _SZP, _DP = C.POINTER(C.c_size_t), C.POINTER(C.c_double)
@@ -186,7 +188,8 @@ EXPORTED = [
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
     "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
     "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
-    "dtb_set_autotune", "dtb_get_tile_config", "dtb_get_trial_kernel", "dtb_smooth_device", "dtb_resample_device",
+    "dtb_set_autotune", "dtb_get_tile_config", "dtb_get_trial_kernel", "dtb_smooth_device",
+    "dtb_smooth_recursive_device", "dtb_resample_device",
     "dtb_write_rvf", "dtb_read_rvf_header", "dtb_read_rvf", "dtb_write_vtk", "dtb_read_vtk_header",
     "dtb_read_vtk", "dtb_volume_change_device", "dtb_log_jacobian_accumulate_device",
     "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching", "dtb_set_verbose",

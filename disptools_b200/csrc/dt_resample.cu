@@ -8,13 +8,24 @@
 // solution passed through the same function.  These kernels restate both
 // steps on the device.
 //
-// * Smoothing: separable Gaussian, one pass per axis.  The weights are
-//   exp(-k^2 / (2 sigma^2)) for |k| <= ceil(4 sigma), normalised to sum 1.
-//   The border is zero-flux (indices clamped into the volume).  The sums are
-//   formed in double in increasing k with explicitly rounded operations, so
-//   the result is a fixed function of the input that a host restatement
-//   reproduces bit for bit.  The reference uses ITK's recursive Gaussian,
-//   an IIR approximation of the same filter, which is not available here.
+// * Smoothing (dtb_smooth_recursive_device, the pyramid's default): the
+//   recursive Gaussian that ITK's SmoothingRecursiveGaussian is built on,
+//   written from R. Deriche, "Recursively implementing the Gaussian and its
+//   derivatives", INRIA research report 1893 (1993): per axis a fourth-order
+//   causal and a fourth-order anticausal recursion with Deriche's published
+//   coefficients, normalised to unit DC gain.  Each recursion starts in the
+//   steady state of its border value, i.e. the volume is taken to continue
+//   with its edge values (zero flux).  One thread runs one line: the
+//   anticausal pass right to left into the output, then the causal pass left
+//   to right adding itself.  ITK's own code is not available here, so its
+//   results are not pinned; the filter is pinned by its defining properties
+//   (impulse response against a sampled Gaussian, unit gain, border rule).
+// * Smoothing (dtb_smooth_device, on request): a sampled Gaussian, weights
+//   exp(-k^2 / (2 sigma^2)) for |k| <= ceil(4 sigma), normalised to sum 1,
+//   zero-flux border (indices clamped into the volume).
+//   Both filters form their sums in double with explicitly rounded
+//   operations in a fixed order, so the result is a fixed function of the
+//   input that a host restatement reproduces bit for bit.
 // * Resampling: output voxel i of an axis samples the input at the
 //   continuous index p = i * n / n2.  A point is inside the input when
 //   -0.5 <= p < n - 0.5 on every axis (the half-voxel border of ITK's
@@ -58,6 +69,91 @@ __global__ void k_smooth_axis(const T *__restrict__ in, T *__restrict__ out, int
             acc = __dadd_rn(acc, __dmul_rn(sw.w[k + sw.radius], (double) line[(long long) q * stride]));
         }
         out[i] = (T) acc;
+    }
+}
+
+// Coefficients of the recursive Gaussian of one axis (see the file comment):
+// causal y+[i] = sum_k n[k] x[i-k] - sum_k d[k] y+[i-1-k], anticausal
+// y-[i] = sum_k m[k] x[i+1+k] - sum_k d[k] y-[i+1+k] (k = 0..3); gc and ga
+// the steady-state responses to a unit constant; on = 0 copies the axis.
+struct Recursive {
+    double n[4], m[4], d[4], gc, ga;
+    int on;
+};
+
+// One axis of the recursive Gaussian: one thread per line of `len` samples
+// at `stride`; lines along y and z are adjacent in x (coalesced).
+template <typename T>
+__global__ void k_recursive_axis(const T *__restrict__ in, T *__restrict__ out, int nx, int ny, int nz, int comps,
+                                 int axis, Recursive rc) {
+    const int len = axis == 0 ? nx : (axis == 1 ? ny : nz);
+    const long long stride = axis == 0 ? 1 : (axis == 1 ? (long long) nx : (long long) nx * ny);
+    const long long lines = (long long) nx * ny * nz * comps / len;
+    for (long long l = blockIdx.x * (long long) blockDim.x + threadIdx.x; l < lines;
+         l += (long long) gridDim.x * blockDim.x) {
+        long long base;
+        if (axis == 0) {
+            base = l * nx;
+        } else if (axis == 1) {  // l = (c * nz + z) * nx + x
+            const long long x = l % nx, cz = l / nx;
+            base = cz * ny * (long long) nx + x;
+        } else {  // l = c * ny * nx + y * nx + x
+            const long long xy = l % ((long long) nx * ny), c = l / ((long long) nx * ny);
+            base = c * nz * (long long) ny * nx + xy;
+        }
+        const T *x = in + base;
+        T *y = out + base;
+        if (!rc.on) {
+            for (int i = 0; i < len; ++i) y[i * stride] = x[i * stride];
+            continue;
+        }
+        // Anticausal pass, right to left, stored in the output.
+        const double xe = (double) x[(long long) (len - 1) * stride];
+        double xn0 = xe, xn1 = xe, xn2 = xe, xn3 = xe;
+        double yn0 = __dmul_rn(xe, rc.ga), yn1 = yn0, yn2 = yn0, yn3 = yn0;
+        for (int i = len - 1; i >= 0; --i) {
+            double acc = __dmul_rn(rc.m[0], xn0);
+            acc = __dadd_rn(acc, __dmul_rn(rc.m[1], xn1));
+            acc = __dadd_rn(acc, __dmul_rn(rc.m[2], xn2));
+            acc = __dadd_rn(acc, __dmul_rn(rc.m[3], xn3));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[0], yn0));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[1], yn1));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[2], yn2));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[3], yn3));
+            y[(long long) i * stride] = (T) acc;
+            xn3 = xn2;
+            xn2 = xn1;
+            xn1 = xn0;
+            xn0 = (double) x[(long long) i * stride];
+            yn3 = yn2;
+            yn2 = yn1;
+            yn1 = yn0;
+            yn0 = acc;
+        }
+        // Causal pass, left to right, added to the stored anticausal part.
+        const double x0 = (double) x[0];
+        double xp0 = x0, xp1 = x0, xp2 = x0;
+        double yp0 = __dmul_rn(x0, rc.gc), yp1 = yp0, yp2 = yp0, yp3 = yp0;
+        for (int i = 0; i < len; ++i) {
+            const double xi = (double) x[(long long) i * stride];
+            double acc = __dmul_rn(rc.n[0], xi);
+            acc = __dadd_rn(acc, __dmul_rn(rc.n[1], xp0));
+            acc = __dadd_rn(acc, __dmul_rn(rc.n[2], xp1));
+            acc = __dadd_rn(acc, __dmul_rn(rc.n[3], xp2));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[0], yp0));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[1], yp1));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[2], yp2));
+            acc = __dsub_rn(acc, __dmul_rn(rc.d[3], yp3));
+            T *o = y + (long long) i * stride;
+            *o = (T) __dadd_rn(acc, (double) *o);
+            xp2 = xp1;
+            xp1 = xp0;
+            xp0 = xi;
+            yp3 = yp2;
+            yp2 = yp1;
+            yp1 = yp0;
+            yp0 = acc;
+        }
     }
 }
 
@@ -145,6 +241,64 @@ bool make_weights(double sigma, SmoothWeights *sw) {
     return true;
 }
 
+// Deriche's fourth-order approximation of the Gaussian (INRIA RR-1893,
+// 1993): for x >= 0 and unit sigma,
+//   g(x) ~ (a0 cos(w0 x) + a1 sin(w0 x)) exp(-b0 x) + (c0 cos(w1 x) + c1 sin(w1 x)) exp(-b1 x).
+// The recursions' numerators and denominator are the z-transforms of the
+// causal part of g (two damped cosines) and of its mirror image; they are
+// scaled so that the impulse response sums to 1.
+constexpr double DERICHE_A0 = 1.680, DERICHE_A1 = 3.735, DERICHE_B0 = 1.783, DERICHE_W0 = 0.6318;
+constexpr double DERICHE_C0 = -0.6803, DERICHE_C1 = -0.2598, DERICHE_B1 = 1.723, DERICHE_W1 = 1.997;
+constexpr double RECURSIVE_MAX_SIGMA = 256.0;
+
+bool recursive_coefficients(double sigma, Recursive *rc) {
+    std::memset(rc, 0, sizeof *rc);
+    if (!(sigma > 0.0)) return true;  // no smoothing along this axis
+    if (!(sigma <= RECURSIVE_MAX_SIGMA)) return false;
+    const double a0 = DERICHE_A0, a1 = DERICHE_A1, b0 = DERICHE_B0, w0 = DERICHE_W0;
+    const double c0 = DERICHE_C0, c1 = DERICHE_C1, b1 = DERICHE_B1, w1 = DERICHE_W1;
+    const double eb0 = std::exp(-b0 / sigma), eb1 = std::exp(-b1 / sigma);
+    const double cw0 = std::cos(w0 / sigma), sw0 = std::sin(w0 / sigma);
+    const double cw1 = std::cos(w1 / sigma), sw1 = std::sin(w1 / sigma);
+    const double n0 = a0 + c0;
+    const double n1 = eb1 * (c1 * sw1 - (c0 + 2.0 * a0) * cw1) + eb0 * (a1 * sw0 - (2.0 * c0 + a0) * cw0);
+    const double n2 = (2.0 * eb0 * eb1 * ((a0 + c0) * cw1 * cw0 - a1 * cw1 * sw0 - c1 * cw0 * sw1) +
+                       c0 * eb0 * eb0 + a0 * eb1 * eb1);
+    const double n3 = eb1 * eb0 * eb0 * (c1 * sw1 - c0 * cw1) + eb0 * eb1 * eb1 * (a1 * sw0 - a0 * cw0);
+    const double d1 = -2.0 * eb1 * cw1 - 2.0 * eb0 * cw0;
+    const double d2 = 4.0 * cw1 * cw0 * eb0 * eb1 + eb1 * eb1 + eb0 * eb0;
+    const double d3 = -2.0 * cw0 * eb0 * eb1 * eb1 - 2.0 * cw1 * eb1 * eb0 * eb0;
+    const double d4 = eb0 * eb0 * eb1 * eb1;
+    const double m1 = n1 - d1 * n0, m2 = n2 - d2 * n0, m3 = n3 - d3 * n0, m4 = -d4 * n0;
+    const double den = 1.0 + d1 + d2 + d3 + d4;
+    const double gain = (n0 + n1 + n2 + n3 + m1 + m2 + m3 + m4) / den;
+    const double n[4] = {n0 / gain, n1 / gain, n2 / gain, n3 / gain};
+    const double m[4] = {m1 / gain, m2 / gain, m3 / gain, m4 / gain};
+    const double d[4] = {d1, d2, d3, d4};
+    for (int k = 0; k < 4; ++k) {
+        rc->n[k] = n[k];
+        rc->m[k] = m[k];
+        rc->d[k] = d[k];
+    }
+    rc->gc = (n[0] + n[1] + n[2] + n[3]) / den;
+    rc->ga = (m[0] + m[1] + m[2] + m[3]) / den;
+    rc->on = 1;
+    return true;
+}
+
+template <typename T>
+cudaError_t smooth_recursive(int comps, int nx, int ny, int nz, const Recursive (&rc)[3], const T *in, T *out,
+                             T *scratch, cudaStream_t s) {
+    const long long n = (long long) nx * ny * nz * comps;
+    k_recursive_axis<T><<<grid_for(n / nx), 256, 0, s>>>(in, out, nx, ny, nz, comps, 0, rc[0]);
+    count_launch();
+    k_recursive_axis<T><<<grid_for(n / ny), 256, 0, s>>>(out, scratch, nx, ny, nz, comps, 1, rc[1]);
+    count_launch();
+    k_recursive_axis<T><<<grid_for(n / nz), 256, 0, s>>>(scratch, out, nx, ny, nz, comps, 2, rc[2]);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t smooth(int comps, int nx, int ny, int nz, const SmoothWeights (&sw)[3], const T *in, T *out, T *scratch,
                    cudaStream_t s) {
@@ -190,6 +344,44 @@ extern "C" int dtb_smooth_device(int precision, int comps, size_t nx, size_t ny,
     else if (precision == DTB_PRECISION_MIXED)
         e = smooth<float>(comps, (int) nx, (int) ny, (int) nz, sw, static_cast<const float *>(in),
                           static_cast<float *>(out), static_cast<float *>(scratch), s);
+    else {
+        report(__LINE__, __func__, "invalid precision");
+        return DTB_ERR_ARGUMENT;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        report(__LINE__, __func__, cudaGetErrorString(e));
+        return DTB_ERR_CUDA;
+    }
+    return DTB_OK;
+}
+
+extern "C" int dtb_smooth_recursive_device(int precision, int comps, size_t nx, size_t ny, size_t nz,
+                                           double sigma_x, double sigma_y, double sigma_z, const void *in,
+                                           void *out, void *scratch, void *stream) {
+    disptools_clear_error();
+    if (!dims_ok(nx, ny, nz) || comps < 1) {
+        report(__LINE__, __func__, "invalid dimensions");
+        return DTB_ERR_ARGUMENT;
+    }
+    if (!in || !out || !scratch) {
+        report(__LINE__, __func__, "null array");
+        return DTB_ERR_ARGUMENT;
+    }
+    Recursive rc[3];
+    if (!recursive_coefficients(sigma_x, &rc[0]) || !recursive_coefficients(sigma_y, &rc[1]) ||
+        !recursive_coefficients(sigma_z, &rc[2])) {
+        report(__LINE__, __func__, "sigma too large (at most 256 voxels)");
+        return DTB_ERR_ARGUMENT;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e;
+    if (precision == DTB_PRECISION_FP64)
+        e = smooth_recursive<double>(comps, (int) nx, (int) ny, (int) nz, rc, static_cast<const double *>(in),
+                                     static_cast<double *>(out), static_cast<double *>(scratch), s);
+    else if (precision == DTB_PRECISION_MIXED)
+        e = smooth_recursive<float>(comps, (int) nx, (int) ny, (int) nz, rc, static_cast<const float *>(in),
+                                    static_cast<float *>(out), static_cast<float *>(scratch), s);
     else {
         report(__LINE__, __func__, "invalid precision");
         return DTB_ERR_ARGUMENT;

@@ -28,13 +28,15 @@ images.  The steps follow the reference's code, in its order:
 7. The padding is cropped from the finest field (``:483``).
 
 Smoothing and resampling run as this package's CUDA kernels
-(``dtb_smooth_device``, ``dtb_resample_device``), and every level is solved
-by the device solver on device-resident tensors.  Padding and
+(``dtb_smooth_recursive_device``, ``dtb_resample_device``), and every level
+is solved by the device solver on device-resident tensors.  Padding and
 redistribution are one-off steps, in NumPy for NumPy inputs and in torch for
-device tensors.  The reference's filters
-are ITK's recursive Gaussian and ResampleImageFilter; the kernels restate a
-sampled Gaussian and the resampler's interpolation rules (see
-``include/disptools_b200.h``).
+device tensors.  The reference's filters are ITK's recursive Gaussian and
+ResampleImageFilter.  The smoothing kernel implements the same method,
+Deriche's recursive Gaussian (INRIA RR-1893, 1993), from its publication;
+``smoothing="sampled"`` selects a truncated sampled Gaussian
+(``dtb_smooth_device``) instead.  The resampling kernel restates the
+resampler's interpolation rules (see ``include/disptools_b200.h``).
 """
 from __future__ import annotations
 
@@ -53,18 +55,26 @@ def _prec(t: torch.Tensor) -> int:
     return N.precision_code("fp64" if t.dtype == torch.float64 else "mixed")
 
 
-def smooth(vol: torch.Tensor, sigma_vox: Sequence[float]) -> torch.Tensor:
+SMOOTHING = ("recursive", "sampled")
+
+
+def smooth(vol: torch.Tensor, sigma_vox: Sequence[float], method: str = "recursive") -> torch.Tensor:
     """Gaussian smoothing of a ``[C, nz, ny, nx]`` (or ``[nz, ny, nx]``)
-    device tensor; ``sigma_vox`` = (sigma_x, sigma_y, sigma_z) in voxels."""
+    device tensor; ``sigma_vox`` = (sigma_x, sigma_y, sigma_z) in voxels.
+    ``method``: "recursive" (Deriche's recursive Gaussian, the filter behind
+    the reference's sitk.SmoothingRecursiveGaussian; the default) or
+    "sampled" (a truncated sampled Gaussian)."""
+    if method not in SMOOTHING:
+        raise ValueError(f"smoothing method must be one of {SMOOTHING}, got {method!r}")
+    fn = N.lib.dtb_smooth_recursive_device if method == "recursive" else N.lib.dtb_smooth_device
     v = vol if vol.dim() == 4 else vol.unsqueeze(0)
     v = v.contiguous()
     out = torch.empty_like(v)
     scratch = torch.empty_like(v)
     c, nz, ny, nx = v.shape
     with torch.cuda.device(v.device):
-        N.check(N.lib.dtb_smooth_device(_prec(v), c, nx, ny, nz, *map(float, sigma_vox), v.data_ptr(),
-                                        out.data_ptr(), scratch.data_ptr(),
-                                        torch.cuda.current_stream(v.device).cuda_stream))
+        N.check(fn(_prec(v), c, nx, ny, nz, *map(float, sigma_vox), v.data_ptr(), out.data_ptr(),
+                   scratch.data_ptr(), torch.cuda.current_stream(v.device).cuda_stream))
     return out if vol.dim() == 4 else out[0]
 
 
@@ -84,11 +94,11 @@ def resample(vol: torch.Tensor, size_zyx: Sequence[int], nearest: bool = False) 
 
 
 def scale_image(vol: torch.Tensor, spacing_xyz: Sequence[float], size_zyx: Sequence[int],
-                nearest: bool = False) -> torch.Tensor:
+                nearest: bool = False, method: str = "recursive") -> torch.Tensor:
     """scale_image (disptools/drawing.py:23-69): smooth by 2.0 physical units,
     then resample onto ``size_zyx`` voxels over the same extent."""
     sig = [SMOOTH_SIGMA / float(s) for s in spacing_xyz]
-    return resample(smooth(vol, sig), size_zyx, nearest)
+    return resample(smooth(vol, sig, method), size_zyx, nearest)
 
 
 def level_geometry(shape_zyx: Sequence[int], spacing_xyz: Sequence[float], levels: int):
@@ -109,7 +119,7 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
                  beta: float = 0.5, gamma: float = 0.1, delta: float = 1e-3, zeta: float = 10.0,
                  theta: float = 1e-6, iota: float = 1e-9, strict: bool = False, eta: float = 0.1,
                  eta_max: float = 0.4, algorithm: str = "gradient", precision: str = "mixed",
-                 device=None, return_stats: bool = False):
+                 device=None, return_stats: bool = False, smoothing: str = "recursive"):
     """Displacement field ``[3, nz, ny, nx]`` whose Jacobian matches
     ``jacobian`` (``[nz, ny, nx]``) in ``mask``, through a ``levels``-level
     pyramid (see the module docstring for the steps).  NumPy inputs give a
@@ -119,7 +129,10 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
     ``spacing`` is (dx, dy, dz).  ``precision`` selects the device solver
     (``"mixed"``: FP32 fields, ``"fp64"``); the target and mask pyramids are
     built in FP64.  With ``return_stats`` also returns the per-level solver
-    statistics, coarsest first."""
+    statistics, coarsest first.  ``smoothing`` is the anti-aliasing filter
+    of every scaling: "recursive" (the default) or "sampled"."""
+    if smoothing not in SMOOTHING:
+        raise ValueError(f"smoothing must be one of {SMOOTHING}")
     if levels < 1:
         raise ValueError("levels must be at least 1")
     if algorithm not in ("gradient", "greedy"):
@@ -177,8 +190,9 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
 
     ftype = torch.float64 if precision == "fp64" else torch.float32
     sizes, spacings = level_geometry(shape0, spacing, levels)
-    Js = [J0] + [scale_image(J0, spacings[0], sizes[i]) for i in range(1, levels)]
-    ms = [m0] + [scale_image(m0, spacings[0], sizes[i], nearest=True) for i in range(1, levels)]
+    Js = [J0] + [scale_image(J0, spacings[0], sizes[i], method=smoothing) for i in range(1, levels)]
+    ms = [m0] + [scale_image(m0, spacings[0], sizes[i], nearest=True, method=smoothing)
+                 for i in range(1, levels)]
 
     field = None
     field_spacing = spacing
@@ -195,7 +209,7 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
     for lv, it in zip(range(levels - 1, -1, -1), its):
         size, sp = sizes[lv], spacings[lv]
         if field is not None:
-            field = scale_image(field, field_spacing, size)
+            field = scale_image(field, field_spacing, size, method=smoothing)
         else:
             field = torch.zeros((3,) + size, dtype=ftype, device=dev)
         Jl = Js[lv].to(ftype).contiguous()

@@ -290,15 +290,29 @@ enum {
 
 /* Gaussian smoothing of `comps` device volumes [comps][nz][ny][nx] (the
  * anti-aliasing step of scale_image, disptools/drawing.py:62-66, which
- * smooths by 2.0 physical units: sigma = 2.0 / spacing voxels per axis).
- * Separable, weights exp(-k^2 / (2 sigma^2)) for |k| <= ceil(4 sigma)
- * normalised to sum 1, zero-flux border; sigma <= 0 leaves an axis alone,
- * sigma is at most 32 voxels.  Sums are formed in double.  `in`, `out` and
- * `scratch` are device arrays of the precision's element type that must not
- * overlap.  Enqueued on `stream` (a cudaStream_t or NULL). */
+ * smooths by 2.0 physical units: sigma = 2.0 / spacing voxels per axis),
+ * as a sampled Gaussian: weights exp(-k^2 / (2 sigma^2)) for
+ * |k| <= ceil(4 sigma) normalised to sum 1, zero-flux border; sigma <= 0
+ * leaves an axis alone, sigma is at most 32 voxels.  Sums are formed in
+ * double.  `in`, `out` and `scratch` are device arrays of the precision's
+ * element type that must not overlap.  Enqueued on `stream` (a cudaStream_t
+ * or NULL).  The pyramid uses dtb_smooth_recursive_device unless asked for
+ * this filter. */
 int dtb_smooth_device(int precision, int comps, size_t nx, size_t ny, size_t nz,
                       double sigma_x, double sigma_y, double sigma_z,
                       const void *in, void *out, void *scratch, void *stream);
+
+/* The same smoothing as the recursive Gaussian that scale_image's
+ * sitk.SmoothingRecursiveGaussian (disptools/drawing.py:67) is built on:
+ * R. Deriche, "Recursively implementing the Gaussian and its derivatives",
+ * INRIA RR-1893 (1993), fourth-order causal and anticausal recursions per
+ * axis with Deriche's coefficients, unit DC gain, each recursion started in
+ * the steady state of the border value (zero flux).  sigma <= 0 leaves an
+ * axis alone, sigma is at most 256 voxels; arguments as dtb_smooth_device.
+ * Arithmetic in double with a fixed operation order. */
+int dtb_smooth_recursive_device(int precision, int comps, size_t nx, size_t ny, size_t nz,
+                                double sigma_x, double sigma_y, double sigma_z,
+                                const void *in, void *out, void *scratch, void *stream);
 
 /* Resampling of `comps` device volumes onto an nx2 x ny2 x nz2 grid that
  * spans the same physical extent (the resampler of scale_image,

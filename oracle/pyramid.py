@@ -11,7 +11,15 @@ Parity unpinned against the reference itself.  The reference smooths with
 ITK's SmoothingRecursiveGaussian and resamples with ITK's
 ResampleImageFilter, and SimpleITK is not installed here.  The filters below
 are the ones the device kernels implement:
-* a sampled Gaussian of 2.0 physical units, truncated at ceil(4 sigma) and
+* the smoothing of 2.0 physical units as a recursive Gaussian, the method
+  that SmoothingRecursiveGaussian is built on: R. Deriche, "Recursively
+  implementing the Gaussian and its derivatives", INRIA research report
+  1893 (1993), fourth-order causal + anticausal recursions with Deriche's
+  published coefficients, normalised to unit DC gain, each recursion started
+  in the steady state of the border value (a zero-flux border, as if the
+  volume continued with its edge values); pinned by the filter's own
+  properties (tests/test_pyramid_oracle.py), since ITK is absent;
+* or, on request, a sampled Gaussian truncated at ceil(4 sigma) and
   normalised, with zero-flux borders;
 * linear / nearest resampling over the same physical extent with ITK's
   half-voxel inside rule.
@@ -51,14 +59,102 @@ def _smooth_axis(v: np.ndarray, axis: int, r: int, w) -> np.ndarray:
     return acc
 
 
-def smooth(vol: np.ndarray, sigma_xyz) -> np.ndarray:
+# Deriche's fourth-order approximation of the Gaussian (INRIA RR-1893, 1993):
+# for x >= 0 and unit sigma,
+#   g(x) ~ (a0 cos(w0 x) + a1 sin(w0 x)) exp(-b0 x) + (c0 cos(w1 x) + c1 sin(w1 x)) exp(-b1 x).
+DERICHE_GAUSSIAN = (1.680, 3.735, 1.783, 0.6318, -0.6803, -0.2598, 1.723, 1.997)  # a0 a1 b0 w0 c0 c1 b1 w1
+
+
+def deriche_coefficients(sigma: float):
+    """(n, m, d, gc, ga) of the recursive Gaussian of `sigma` samples:
+    causal y+[i] = sum_k n[k] x[i-k] - sum_k d[k] y+[i-1-k] (k = 0..3),
+    anticausal y-[i] = sum_k m[k] x[i+1+k] - sum_k d[k] y-[i+1+k], y = y+ + y-;
+    n and m scaled so the sum of the impulse response is 1; gc and ga the
+    steady-state responses of the two recursions to a unit constant.  The
+    numerators and denominator are the z-transforms of the causal part of
+    g (two damped cosines) and of its mirror image."""
+    a0, a1, b0, w0, c0, c1, b1, w1 = DERICHE_GAUSSIAN
+    eb0, eb1 = math.exp(-b0 / sigma), math.exp(-b1 / sigma)
+    cw0, sw0 = math.cos(w0 / sigma), math.sin(w0 / sigma)
+    cw1, sw1 = math.cos(w1 / sigma), math.sin(w1 / sigma)
+    n0 = a0 + c0
+    n1 = eb1 * (c1 * sw1 - (c0 + 2.0 * a0) * cw1) + eb0 * (a1 * sw0 - (2.0 * c0 + a0) * cw0)
+    n2 = (2.0 * eb0 * eb1 * ((a0 + c0) * cw1 * cw0 - a1 * cw1 * sw0 - c1 * cw0 * sw1)
+          + c0 * eb0 * eb0 + a0 * eb1 * eb1)
+    n3 = eb1 * eb0 * eb0 * (c1 * sw1 - c0 * cw1) + eb0 * eb1 * eb1 * (a1 * sw0 - a0 * cw0)
+    d1 = -2.0 * eb1 * cw1 - 2.0 * eb0 * cw0
+    d2 = 4.0 * cw1 * cw0 * eb0 * eb1 + eb1 * eb1 + eb0 * eb0
+    d3 = -2.0 * cw0 * eb0 * eb1 * eb1 - 2.0 * cw1 * eb1 * eb0 * eb0
+    d4 = eb0 * eb0 * eb1 * eb1
+    m1, m2, m3, m4 = n1 - d1 * n0, n2 - d2 * n0, n3 - d3 * n0, -d4 * n0
+    den = 1.0 + d1 + d2 + d3 + d4
+    gain = (n0 + n1 + n2 + n3 + m1 + m2 + m3 + m4) / den
+    n = [n0 / gain, n1 / gain, n2 / gain, n3 / gain]
+    m = [m1 / gain, m2 / gain, m3 / gain, m4 / gain]
+    gc = (n[0] + n[1] + n[2] + n[3]) / den
+    ga = (m[0] + m[1] + m[2] + m[3]) / den
+    return n, m, [d1, d2, d3, d4], gc, ga
+
+
+def _recursive_axis(v: np.ndarray, axis: int, sigma: float, t) -> np.ndarray:
+    """One axis of the recursive Gaussian over every line of `v` (float64),
+    result rounded to `t`.  The anticausal pass runs first and is stored in
+    `t`; the causal pass adds itself to it.  Every sum is formed left to
+    right, each operation rounded, as in the kernel."""
+    if not sigma > 0.0:
+        return v.astype(t)
+    n, m, d, gc, ga = deriche_coefficients(sigma)
+    x = np.moveaxis(v, axis, 0)
+    L = x.shape[0]
+    ym = np.empty(x.shape, dtype=t)
+    xe = x[L - 1]
+    xn = [xe, xe, xe, xe]                       # x[i+1 .. i+4]
+    yn = [xe * ga, xe * ga, xe * ga, xe * ga]   # y-[i+1 .. i+4]
+    for i in range(L - 1, -1, -1):
+        acc = m[0] * xn[0]
+        acc = acc + m[1] * xn[1]
+        acc = acc + m[2] * xn[2]
+        acc = acc + m[3] * xn[3]
+        acc = acc - d[0] * yn[0]
+        acc = acc - d[1] * yn[1]
+        acc = acc - d[2] * yn[2]
+        acc = acc - d[3] * yn[3]
+        ym[i] = acc
+        xn = [x[i], xn[0], xn[1], xn[2]]
+        yn = [acc, yn[0], yn[1], yn[2]]
+    out = np.empty(x.shape, dtype=t)
+    x0 = x[0]
+    xp = [x0, x0, x0]                           # x[i-1 .. i-3]
+    yp = [x0 * gc, x0 * gc, x0 * gc, x0 * gc]   # y+[i-1 .. i-4]
+    for i in range(L):
+        acc = n[0] * x[i]
+        acc = acc + n[1] * xp[0]
+        acc = acc + n[2] * xp[1]
+        acc = acc + n[3] * xp[2]
+        acc = acc - d[0] * yp[0]
+        acc = acc - d[1] * yp[1]
+        acc = acc - d[2] * yp[2]
+        acc = acc - d[3] * yp[3]
+        out[i] = acc + ym[i].astype(np.float64)
+        xp = [x[i], xp[0], xp[1]]
+        yp = [acc, yp[0], yp[1], yp[2]]
+    return np.moveaxis(out, 0, axis)
+
+
+def smooth(vol: np.ndarray, sigma_xyz, method: str = "recursive") -> np.ndarray:
     """Separable Gaussian of a [C, nz, ny, nx] array (x, then y, then z);
-    each pass computes in float64 and rounds to the array's type."""
+    each pass computes in float64 and rounds to the array's type.
+    ``method`` "recursive" (Deriche, the default) or "sampled"."""
     t = vol.dtype
     v = vol
     for axis, sigma in zip((3, 2, 1), sigma_xyz):
-        r, w = gaussian_weights(float(sigma))
-        v = _smooth_axis(v.astype(np.float64), axis, r, w).astype(t)
+        if method == "recursive":
+            v = _recursive_axis(v.astype(np.float64), axis, float(sigma), t)
+        elif method == "sampled":
+            r, w = gaussian_weights(float(sigma))
+            v = _smooth_axis(v.astype(np.float64), axis, r, w).astype(t)
+        else:
+            raise ValueError(f"unknown smoothing method {method!r}")
     return v
 
 
@@ -114,15 +210,16 @@ def resample(vol: np.ndarray, size_zyx, nearest: bool = False) -> np.ndarray:
     return out.astype(t)
 
 
-def scale_image(vol: np.ndarray, spacing_xyz, size_zyx, nearest: bool = False) -> np.ndarray:
+def scale_image(vol: np.ndarray, spacing_xyz, size_zyx, nearest: bool = False,
+                method: str = "recursive") -> np.ndarray:
     """disptools/drawing.py:23-69: smooth by 2.0 physical units, resample."""
     sig = [2.0 / float(s) for s in spacing_xyz]
-    return resample(smooth(vol, sig), size_zyx, nearest)
+    return resample(smooth(vol, sig, method), size_zyx, nearest)
 
 
 def displacement(jacobian, *, levels=1, pad=0, redistribute=False, mask=None, initial_guess=None,
                  spacing=(1.0, 1.0, 1.0), it_max=50000, algorithm="gradient", field_dtype=np.float64,
-                 **params):
+                 smoothing="recursive", **params):
     """disptools/displacements.py:238-480 on NumPy arrays, each level solved
     by the C oracle.  ``field_dtype`` float32 rounds the fields passed
     between levels like the mixed-precision device path."""
@@ -141,13 +238,14 @@ def displacement(jacobian, *, levels=1, pad=0, redistribute=False, mask=None, in
         sizes.append(tuple(s // 2 for s in sizes[-1]))
     n0 = J.shape[::-1]
     spacings = [tuple(float(sp) * n / k for sp, n, k in zip(spacing, n0, sz[::-1])) for sz in sizes]
-    Js = [J] + [scale_image(J[None], spacings[0], sizes[i])[0] for i in range(1, levels)]
-    ms = [m] + [scale_image(m[None], spacings[0], sizes[i], nearest=True)[0] for i in range(1, levels)]
+    Js = [J] + [scale_image(J[None], spacings[0], sizes[i], method=smoothing)[0] for i in range(1, levels)]
+    ms = [m] + [scale_image(m[None], spacings[0], sizes[i], nearest=True, method=smoothing)[0]
+                for i in range(1, levels)]
     field = None if initial_guess is None else np.asarray(initial_guess, dtype=field_dtype)
     field_spacing = spacing
     for lv, it in zip(range(levels - 1, -1, -1), its):              # :476-480
         if field is not None:
-            field = scale_image(field.astype(field_dtype), field_spacing, sizes[lv])
+            field = scale_image(field.astype(field_dtype), field_spacing, sizes[lv], method=smoothing)
         f0 = None if field is None else field.astype(np.float64)
         out, _ = o.solve(algorithm, np.ascontiguousarray(Js[lv]), np.ascontiguousarray(ms[lv] != 0),
                          field=f0, spacing=spacings[lv], it_max=it, **params)

@@ -21,10 +21,20 @@ pytestmark = pytest.mark.gpu
     (3, (9, 10, 23), (2.0, 0.7, 1.3)),
     (1, (5, 6, 4), (0.0, 3.0, 0.5)),
 ])
-def test_smooth_bitwise(dtype, comps, shape, sigma):
+@pytest.mark.parametrize("method", ["recursive", "sampled"])
+def test_smooth_bitwise(dtype, comps, shape, sigma, method):
     v = np.random.default_rng(comps).standard_normal((comps,) + shape).astype(dtype)
-    got = D.smooth(torch.from_numpy(v).cuda(), sigma).cpu().numpy()
-    np.testing.assert_array_equal(got, P.smooth(v, sigma))
+    got = D.smooth(torch.from_numpy(v).cuda(), sigma, method).cpu().numpy()
+    np.testing.assert_array_equal(got, P.smooth(v, sigma, method))
+
+
+def test_recursive_smooth_long_lines_bitwise():
+    """Lines longer than the filter's memory along every axis, large sigma
+    (the config-5 level sizes' scale), FP32."""
+    v = np.random.default_rng(8).standard_normal((1, 40, 70, 130)).astype(np.float32)
+    sig = (8.0, 4.0, 2.0)
+    got = D.smooth(torch.from_numpy(v).cuda(), sig).cpu().numpy()
+    np.testing.assert_array_equal(got, P.smooth(v, sig))
 
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
@@ -54,6 +64,7 @@ def test_scale_image_anisotropic_bitwise():
     dict(levels=2, it_max=[20, 15], redistribute=True),
     dict(levels=2, it_max=30, initial_guess=True, spacing=(1.0, 1.2, 0.9)),
     dict(levels=2, it_max=[20, 20], algorithm="greedy"),
+    dict(levels=2, it_max=[20, 20], smoothing="sampled"),
 ])
 def test_driver_fp64_matches_oracle(kw):
     kw = dict(kw)

@@ -19,11 +19,12 @@ def test_gaussian_weights():
 
 
 def test_smooth_keeps_constants_and_mass_of_interior_impulse():
+    """The sampled filter (method "sampled")."""
     v = np.full((2, 9, 10, 11), 3.25)
-    np.testing.assert_allclose(P.smooth(v, (1.0, 2.0, 0.5)), v, rtol=1e-15)
+    np.testing.assert_allclose(P.smooth(v, (1.0, 2.0, 0.5), "sampled"), v, rtol=1e-15)
     d = np.zeros((1, 31, 31, 31))
     d[0, 15, 15, 15] = 1.0
-    s = P.smooth(d, (1.5, 1.0, 2.0))
+    s = P.smooth(d, (1.5, 1.0, 2.0), "sampled")
     assert abs(s.sum() - 1.0) < 1e-14
     # separable: the x profile through the centre is the x kernel times the
     # centre weights of y and z
@@ -101,3 +102,70 @@ def test_pyramid_rejects_levels_below_three_voxels_before_device_work():
     from disptools_b200 import pyramid
     with pytest.raises(ValueError, match="below 3"):
         pyramid.displacement(np.ones((5, 5, 5)), levels=3)
+
+
+# --- the recursive Gaussian (Deriche, INRIA RR-1893, 1993) ------------------
+# ITK is not installed, so the filter is pinned by its defining properties.
+
+def _impulse_response(sigma, n=None):
+    n = n or int(40 * sigma) + 41
+    d = np.zeros((1, 1, 1, n))
+    d[0, 0, 0, n // 2] = 1.0
+    return P.smooth(d, (sigma, 0.0, 0.0))[0, 0, 0], n // 2
+
+
+@pytest.mark.parametrize("sigma", [0.5, 1.0, 2.0, 4.0, 8.0, 16.0])
+def test_recursive_impulse_response_is_a_gaussian(sigma):
+    """Deriche's fourth-order fit of the Gaussian: the impulse response
+    matches the sampled Gaussian exp(-k^2 / (2 sigma^2)) / sum to within
+    1e-3 of its peak, sums to 1 and is symmetric."""
+    h, c = _impulse_response(sigma)
+    k = np.arange(h.size) - c
+    g = np.exp(-k * k / (2.0 * sigma * sigma))
+    g /= g.sum()
+    assert np.max(np.abs(h - g)) <= 1e-3 * g.max()
+    assert abs(h.sum() - 1.0) <= 1e-12
+    np.testing.assert_allclose(h, h[::-1], atol=1e-14)
+
+
+def test_recursive_unit_gain_and_constants():
+    for sigma in (0.7, 2.0, 5.5):
+        n, m, d, gc, ga = P.deriche_coefficients(sigma)
+        den = 1.0 + sum(d)
+        assert abs((sum(n) + sum(m)) / den - 1.0) <= 1e-12
+        assert abs(gc + ga - 1.0) <= 1e-12
+    v = np.full((2, 7, 9, 11), -1.75)
+    np.testing.assert_allclose(P.smooth(v, (1.0, 2.0, 3.0)), v, rtol=1e-12)
+    np.testing.assert_allclose(P.smooth(v.astype(np.float32), (1.0, 2.0, 3.0)), v, rtol=1e-6)
+
+
+@pytest.mark.parametrize("sigma", [1.0, 2.5, 6.0])
+def test_recursive_zero_flux_border(sigma):
+    """Each recursion starts in the steady state of its border value: the
+    result equals that of the signal continued with its edge values far
+    beyond both ends, cropped."""
+    x = np.random.default_rng(int(sigma * 10)).standard_normal(37)
+    pad = int(30 * sigma)
+    xp = np.concatenate([np.full(pad, x[0]), x, np.full(pad, x[-1])])
+    a = P.smooth(x[None, None, None], (sigma, 0.0, 0.0))[0, 0, 0]
+    b = P.smooth(xp[None, None, None], (sigma, 0.0, 0.0))[0, 0, 0, pad:-pad]
+    np.testing.assert_allclose(a, b, rtol=0, atol=1e-10)
+
+
+def test_recursive_separable_linear_and_axis_order():
+    rng = np.random.default_rng(4)
+    u, w = rng.standard_normal((2, 1, 8, 9, 10))
+    s = (1.2, 0.8, 2.0)
+    np.testing.assert_allclose(P.smooth(2.0 * u - 3.0 * w, s), 2.0 * P.smooth(u, s) - 3.0 * P.smooth(w, s),
+                               atol=1e-12)
+    # sigma 0 leaves an axis alone; the passes commute up to rounding
+    np.testing.assert_array_equal(P.smooth(u, (0.0, 0.0, 0.0)), u)
+    ax = P.smooth(P.smooth(u, (0.0, 0.0, s[2])), (s[0], s[1], 0.0))
+    np.testing.assert_allclose(P.smooth(u, s), ax, atol=1e-12)
+
+
+def test_recursive_close_to_sampled_filter():
+    v = np.random.default_rng(9).standard_normal((1, 12, 13, 14))
+    a = P.smooth(v, (2.0, 1.5, 1.0))
+    b = P.smooth(v, (2.0, 1.5, 1.0), "sampled")
+    assert np.max(np.abs(a - b)) <= 5e-3 * np.max(np.abs(v))
