@@ -1376,8 +1376,27 @@ int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
     return DTB_OK;
 }
 
+// The adjoint's path: the fused TMA kernel (order 4, a 16-byte-aligned field
+// whose rows are a multiple of 16 bytes long), unless
+// DISPTOOLS_B200_ADJOINT=two-pass asks for the weight pass and gather.
+bool adjoint_fused_allowed() {
+    const char *e = std::getenv("DISPTOOLS_B200_ADJOINT");
+    return !(e && std::strcmp(e, "two-pass") == 0);
+}
+
 template <typename T>
 int adjoint_device_impl(const Geom &g, const T *field, const T *gJ, T *gout, cudaStream_t s) {
+    // Fused kernel: the weights stay on chip, the tensor map is a kernel
+    // parameter, no device memory of its own: no lock, no wait.
+    if (adjoint_fused_allowed() && g.order == 4 && (g.ys * (long long) sizeof(T)) % 16 == 0 &&
+        reinterpret_cast<uintptr_t>(field) % 16 == 0) {
+        CUtensorMap tm;
+        const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        if (encode_map(&tm, ft, sizeof(T), field, g, 3, 32 + 2 * 4, TT_Y + 2 * 4)) {
+            DTB_CUDA(launch_adjoint_tma<T>(tm, g, gJ, gout, num_sms(), s));
+            return DTB_OK;
+        }
+    }
     std::lock_guard<std::mutex> lock(g_ws_mutex);
     // Weights W[9][wn] in the adjoint's own buffer, each component 256-byte
     // aligned.  Calls are ordered on the device, not on the host: this

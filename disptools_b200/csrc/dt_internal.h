@@ -168,6 +168,12 @@ template <typename T>
 cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
                                 int num_sms, cudaStream_t s, const T *gJ = nullptr, T *W = nullptr,
                                 long long wn = 0);
+// Fused adjoint of the Jacobian stencil of order 4 (one TMA kernel, no
+// weight buffer): `tm_u` maps the field with box 40 x 24 x 1 x 3; gJ and gout
+// in the field's dense layout.
+template <typename T>
+cudaError_t launch_adjoint_tma(const CUtensorMap &tm_u, const Geom &g, const T *gJ, T *gout, int num_sms,
+                               cudaStream_t s);
 // Adjoint of the Jacobian stencil: the weight pass (unless w_done: W already
 // holds the weights) and the gather pass; W is [9][N] with component stride wn.
 template <typename T>

@@ -1909,6 +1909,404 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
     return launch_jacobian_tma_v<T, false>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
 }
 
+// ------------------------------------------------------------------------
+// Fused adjoint of the Jacobian map (autograd backward) with the TMA
+// pipeline: grad_c(q) = sum_a sum_t W[c][a](q - t e_a) kappa(k_a(q - t e_a), t)
+// with W[c][a](p) = gJ(p) cof_ca(I + A(p)) ih_a, A(p) the stencil matrix of
+// the Jacobian map at p (the two-pass path's k_adjoint_w / k_adjoint_gather),
+// without writing W to memory.
+//
+// A block of TXW / 2 x TYT threads marches a TXW x TT_Y tile through its z
+// range.  Field boxes of the tile plus 4 voxels on every x-y side arrive by
+// TMA in S stages; plane m's stage stays until the weights of plane m + 2
+// have been formed (their z differences read planes m .. m + 4).  Per plane:
+// * the z weights W[c][2] of the newest plane at the thread's own two
+//   voxels go into a register queue (they need only in-plane differences);
+// * the x weights W[c][0] of the centre plane on the tile plus two columns
+//   each side, and its y weights W[c][1] on the tile plus two rows each
+//   side, go into shared memory (the halo cells on the last threads);
+// * after the block barrier each thread gathers its two voxels' gradient
+//   from the x and y weights in shared memory and the z weights in its
+//   queue, in the two-pass gather's tap order, and stores it.
+// The weights are those of the two-pass path, formed in the same operation
+// order, so FP64 results agree with it bit for bit.  Tiles, planes and halo
+// cells away from the faces take a fourth-order-only path; near the faces
+// every cell and every tap takes its scheme from schemes_at.
+// ------------------------------------------------------------------------
+template <typename T, int TXW>
+struct AdjTmaLayout {
+    static constexpr int PX = TXW + 8;      // columns x0-4 .. x0+TXW+3
+    static constexpr int PY = TT_Y + 8;     // rows y0-4 .. y0+TT_Y+3
+    static constexpr int PLANE = PX * PY;   // elements of one component plane
+    static constexpr int S = 7;             // planes m-2 .. m+2 in use, two in flight
+    static constexpr int U_BYTES = 3 * PLANE * (int) sizeof(T);
+    static_assert(U_BYTES % 128 == 0, "stages stay 128-byte aligned");
+    static constexpr int WXC = TXW + 4, WXR = TT_Y;  // x weights: columns x0-2 .. x0+TXW+1, tile rows
+    static constexpr int WYC = TXW, WYR = TT_Y + 4;  // y weights: tile columns, rows y0-2 .. y0+TT_Y+1
+    static constexpr int WX_ELEMS = 3 * WXR * WXC;
+    static constexpr int W_ELEMS = WX_ELEMS + 3 * WYR * WYC;  // one plane's x and y weights
+    static constexpr int W_OFF = S * U_BYTES;
+    static constexpr int W_BYTES = 2 * W_ELEMS * (int) sizeof(T);  // two planes (double buffer)
+    static constexpr int BAR_OFF = (W_OFF + W_BYTES + 7) / 8 * 8;
+    static constexpr int BYTES = BAR_OFF + S * 8;
+};
+
+// The stages of planes m-2 .. m+2 (the cell's plane is c0).
+template <typename T>
+struct Planes5 {
+    const T *m2, *m1, *c0, *p1, *p2;
+    __device__ __forceinline__ const T *at(int d) const {
+        return d == -2 ? m2 : (d == -1 ? m1 : (d == 0 ? c0 : (d == 1 ? p1 : p2)));
+    }
+};
+
+// Derivative of component c along `ax` by scheme k at the box cell whose
+// offset in a component plane is `o`, in plane sp.c0 (sp.at(d) the plane d
+// away).  The arithmetic of stencil_pair (the Jacobian map's evaluator):
+// fourth order with the spacing folded into the weights in FP32, the
+// reference's operation order in FP64.
+template <typename T, int PX, int PLANE>
+__device__ __forceinline__ T adj_deriv(const Planes5<T> &sp, int c, int o, int ax, int k, const T (&ih)[3],
+                                       const T (&k1)[3], const T (&k2)[3]) {
+    const int oc = c * PLANE + o;
+    auto v = [&](int d) -> T {
+        if (ax == 0) return sp.c0[oc + d];
+        if (ax == 1) return sp.c0[oc + d * PX];
+        return sp.at(d)[oc];
+    };
+    switch (k) {
+    case S_FWD: return fd_fwd<T>(v(0), v(1), v(2), ih[ax]);
+    case S_BWD: return fd_bwd<T>(v(0), v(-1), v(-2), ih[ax]);
+    case S_C2: return fd_c2<T>(v(1), v(-1), ih[ax]);
+    default:
+        if (sizeof(T) == 4) return (v(1) - v(-1)) * k1[ax] - (v(2) - v(-2)) * k2[ax];
+        return fd_c4<T>(v(1), v(-1), v(2), v(-2), ih[ax]);
+    }
+}
+
+// W[c][b] = w * cof_cb(I + a) * ih_b for the three components c (the weight
+// epilogue's expression and order).
+template <typename T>
+__device__ __forceinline__ void adj_weights(const T (&a)[3][3], T w, int b, T ihb, T (&out)[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+        const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+        const T m00 = a[r0][c0] + (r0 == c0 ? T(1) : T(0));
+        const T m11 = a[r1][c1] + (r1 == c1 ? T(1) : T(0));
+        const T m01 = a[r0][c1] + (r0 == c1 ? T(1) : T(0));
+        const T m10 = a[r1][c0] + (r1 == c0 ? T(1) : T(0));
+        const T minor = m00 * m11 - m01 * m10;
+        const T cof = ((c + b) & 1) ? -minor : minor;
+        out[c] = w * cof * ihb;
+    }
+}
+
+template <typename T, int TXW, int TYT>
+__global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
+    k_adjoint_tma(const __grid_constant__ CUtensorMap tm_u, const Geom g, const T *__restrict__ gJ,
+                  T *__restrict__ gout, int tiles_x, int tiles_y, int ntiles, int bz) {
+    using L = AdjTmaLayout<T, TXW>;
+    constexpr int TPX = TXW / 2, NTH = TPX * TYT, S = L::S, PX = L::PX, PLANE = L::PLANE;
+    constexpr int WXC = L::WXC, WYC = L::WYC;
+    constexpr int NHX = TT_Y * 2, NHY = 4 * TPX, NH = NHX + NHY;  // halo pair tasks: x sides, y sides
+    static_assert(TYT == TT_Y, "one tile row per thread row");
+    static_assert(NH <= NTH - 64, "halo tasks on threads other than the first two warps");
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem = align_smem_128(smem_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    __shared__ int s_fault;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+        tmap_prefetch(&tm_u);
+        s_fault = 0;
+    }
+    __syncthreads();
+    const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
+    const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
+    const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1], FD<T>::one_twelfth * ih[2]};
+    const int n[3] = {g.nx, g.ny, g.nz};
+    uint32_t kbase = 0;
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int txi = tile % tiles_x, tyi = (tile / tiles_x) % tiles_y, tzi = tile / (tiles_x * tiles_y);
+        const int x0 = txi * TXW, y0 = tyi * TT_Y, z0 = tzi * bz;
+        const int z1 = min(z0 + bz, g.nz);
+        const int n_it = z1 - z0 + 4;  // newest planes z0-2 .. z1+1
+        __syncthreads();  // every warp has finished the previous tile's stages
+        int issued_n = 0;
+        auto issue = [&](int j) {
+            issued_n = j + 1;
+            const uint32_t k = kbase + j;
+            uint64_t *bar = &bars[k % S];
+            mbar_arrive_expect_tx(bar, L::U_BYTES);
+            tma_load_4d(smem + (k % S) * L::U_BYTES, &tm_u, bar, x0 - 4, y0 - 4, z0 - 2 + j, 0);
+        };
+        if (tid == 0)
+            for (int j = 0; j < min(S, n_it); ++j) issue(j);
+        auto stage = [&](int j) -> const T * {
+            return reinterpret_cast<const T *>(smem + ((kbase + j) % S) * L::U_BYTES);
+        };
+
+        const int x = x0 + 2 * tx, y = y0 + ty;  // own voxels (x, y), (x + 1, y)
+        const int bxo = 2 * tx + 4, byo = ty + 4;  // their box cell
+        const bool row_vol = y < g.ny;
+        // Own z weights W[c][2] of planes m-2 .. m+2 (queue index 2 + d for plane m + d).
+        T zw[2][3][5];
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 5; ++k) zw[v][c][k] = T(0);
+        const bool tile_c4_own = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3 && y0 >= 2 && y0 + TT_Y - 1 <= g.ny - 3;
+        const bool tile_c4_halo = x0 >= 4 && x0 + TXW + 1 <= g.nx - 3 && y0 >= 4 && y0 + TT_Y + 1 <= g.ny - 3;
+        const bool tile_deep = x0 >= 4 && x0 + TXW - 1 <= g.nx - 5 && y0 >= 4 && y0 + TT_Y - 1 <= g.ny - 5;
+        bool failed = false;
+        for (int it = 0; it < n_it; ++it) {
+            const uint32_t k = kbase + it;
+            if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u)) s_fault = 1;
+            const int p = z0 - 2 + it;  // newest plane
+            const int m = p - 2;        // centre plane of this iteration's x and y weights and gradient
+            // (a) z weights of plane p at the own voxels (in-plane differences only).
+            {
+                const Planes5<T> sp{nullptr, nullptr, stage(it), nullptr, nullptr};
+                const bool p_vol = p >= 0 && p < g.nz;
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) zw[v][c][kk] = zw[v][c][kk + 1];
+                    T wz[3] = {T(0), T(0), T(0)};
+                    const int xv = x + v;
+                    if (p_vol && row_vol && xv < g.nx) {
+                        int ks[3] = {S_C4, S_C4, S_C4};
+                        if (!(tile_c4_own && p >= 2 && p <= g.nz - 3)) schemes_at(xv, y, p, g, ks);
+                        const int o = byo * PX + bxo + v;
+                        T a[3][3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            a[c][0] = adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2);
+                            a[c][1] = adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2);
+                            a[c][2] = T(0);  // not used by the z weights
+                        }
+                        const T w = gJ[(long long) p * g.zs + (long long) y * g.ys + xv];
+                        adj_weights<T>(a, w, 2, ih[2], wz);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) zw[v][c][4] = wz[c];
+                }
+            }
+            const bool centre = m >= z0 && m < z1;
+            T *wb = reinterpret_cast<T *>(smem + L::W_OFF) + (it & 1) * L::W_ELEMS;
+            T *WX = wb, *WY = wb + L::WX_ELEMS;
+            if (centre && !s_fault) {
+                const Planes5<T> sp{stage(it - 4), stage(it - 3), stage(it - 2), stage(it - 1), stage(it)};
+                const bool fast = tile_c4_halo && m >= 2 && m <= g.nz - 3;
+                // (b) own voxels: x and y weights of plane m.
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const int xv = x + v;
+                    T wx[3] = {T(0), T(0), T(0)}, wy[3] = {T(0), T(0), T(0)};
+                    if (row_vol && xv < g.nx) {
+                        int ks[3] = {S_C4, S_C4, S_C4};
+                        if (!fast) schemes_at(xv, y, m, g, ks);
+                        const int o = byo * PX + bxo + v;
+                        T a[3][3];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+#pragma unroll
+                            for (int ax = 0; ax < 3; ++ax) a[c][ax] = adj_deriv<T, PX, PLANE>(sp, c, o, ax, ks[ax], ih, k1, k2);
+                        const T w = gJ[(long long) m * g.zs + (long long) y * g.ys + xv];
+                        adj_weights<T>(a, w, 0, ih[0], wx);
+                        adj_weights<T>(a, w, 1, ih[1], wy);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        WX[(c * TT_Y + ty) * WXC + 2 * tx + 2 + v] = wx[c];
+                        WY[(c * (TT_Y + 4) + ty + 2) * WYC + 2 * tx + v] = wy[c];
+                    }
+                }
+                // (c) halo cells, two adjacent x cells per task: the x
+                // weights of the two columns each side, the y weights of the
+                // two rows each side.
+                const int h = tid - (NTH - NH);
+                if (h >= 0) {
+                    const bool xside = h < NHX;
+                    int cx, cy;  // first cell of the pair
+                    if (xside) {
+                        cx = (h / TT_Y) ? x0 + TXW : x0 - 2;
+                        cy = y0 + h % TT_Y;
+                    } else {
+                        const int h2 = h - NHX, r = h2 / TPX;
+                        cx = x0 + 2 * (h2 % TPX);
+                        cy = r < 2 ? y0 - 2 + r : y0 + TT_Y - 2 + r;
+                    }
+#pragma unroll
+                    for (int v = 0; v < 2; ++v) {
+                        const int xv = cx + v;
+                        T wv[3] = {T(0), T(0), T(0)};
+                        if (xv >= 0 && xv < g.nx && cy >= 0 && cy < g.ny && m >= 0 && m < g.nz) {
+                            int ks[3] = {S_C4, S_C4, S_C4};
+                            if (!fast) schemes_at(xv, cy, m, g, ks);
+                            const int o = (cy - y0 + 4) * PX + (xv - x0 + 4);
+                            const T w = gJ[(long long) m * g.zs + (long long) cy * g.ys + xv];
+                            T a[3][3];
+                            // The x weights use columns 1 and 2 of I + A, the y weights 0 and 2.
+                            if (xside) {
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    a[c][0] = T(0);
+                                    a[c][1] = adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2);
+                                    a[c][2] = adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2);
+                                }
+                                adj_weights<T>(a, w, 0, ih[0], wv);
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    a[c][0] = adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2);
+                                    a[c][1] = T(0);
+                                    a[c][2] = adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2);
+                                }
+                                adj_weights<T>(a, w, 1, ih[1], wv);
+                            }
+                        }
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            if (xside)
+                                WX[(c * TT_Y + (cy - y0)) * WXC + (xv - x0 + 2)] = wv[c];
+                            else
+                                WY[(c * (TT_Y + 4) + (cy - y0 + 2)) * WYC + (xv - x0)] = wv[c];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (s_fault) {
+                failed = true;
+                break;
+            }
+            // Iteration it - 4's stage (plane m - 2) is not read again.
+            if (tid == 0 && it >= 4 && it + 3 < n_it) issue(it + 3);
+            // (d) gradient of the own voxels at plane m.
+            if (centre && row_vol) {
+                const bool deep = tile_deep && m >= 4 && m <= g.nz - 5;
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const int xv = x + v;
+                    if (xv >= g.nx) continue;
+                    T acc[3] = {T(0), T(0), T(0)};
+                    const int q[3] = {xv, y, m};
+                    bool ob[3], pb[3];
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb) {
+                        ob[bb] = q[bb] == 0 || q[bb] == n[bb] - 1;
+                        pb[bb] = q[bb] == 1 || q[bb] == n[bb] - 2;
+                    }
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
+                        const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
+#pragma unroll
+                        for (int t = -2; t <= 2; ++t) {
+                            T kp;
+                            if (deep) {
+                                if (t == 0) continue;
+                                kp = kappa<T>(S_C4, t);
+                            } else {
+                                const int pa = q[a] - t;
+                                if (pa < 0 || pa >= n[a]) continue;
+                                const bool outer = o_other || pa == 0 || pa == n[a] - 1;
+                                const bool pen = p_other || pa == 1 || pa == n[a] - 2;
+                                const int kk = outer ? (pa == 0 ? S_FWD : (pa == n[a] - 1 ? S_BWD : S_C2))
+                                                     : ((g.order == 2 || pen) ? S_C2 : S_C4);
+                                kp = kappa<T>(kk, t);
+                                if (kp == T(0)) continue;
+                            }
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                T wt;
+                                if (a == 0)
+                                    wt = WX[(c * TT_Y + ty) * WXC + 2 * tx + v - t + 2];
+                                else if (a == 1)
+                                    wt = WY[(c * (TT_Y + 4) + ty - t + 2) * WYC + 2 * tx + v];
+                                else
+                                    wt = zw[v][c][2 - t];
+                                acc[c] += wt * kp;
+                            }
+                        }
+                    }
+                    const long long off = (long long) m * g.zs + (long long) y * g.ys + xv;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) gout[c * g.cs + off] = acc[c];
+                }
+            }
+        }
+        if (failed) {
+            // Wait (bounded) for the loads still in flight, mark the tile's
+            // voxels NaN and leave.
+            if (tid == 0)  // the last load issued into each slot
+                for (int j = max(0, issued_n - S); j < issued_n; ++j) {
+                    const uint32_t kk = kbase + j;
+                    mbar_wait_bounded(&bars[kk % S], (kk / S) & 1u, 1u << 16);
+                }
+            const T nan = T(NAN);
+            for (int ze = z0; ze < z1; ++ze)
+                for (int v = 0; v < 2; ++v) {
+                    if (x + v >= g.nx || !row_vol) continue;
+                    const long long off = (long long) ze * g.zs + (long long) y * g.ys + x + v;
+                    for (int c = 0; c < 3; ++c) gout[c * g.cs + off] = nan;
+                }
+            __syncthreads();
+            return;
+        }
+        kbase += n_it;
+    }
+}
+
+template <typename T, int TXW, int TYT>
+int adjoint_tma_blocks_v() {
+    static const int nb = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_adjoint_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             AdjTmaLayout<T, TXW>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_adjoint_tma<T, TXW, TYT>, TXW / 2 * TYT,
+                                                      AdjTmaLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return nb;
+}
+
+// Fused adjoint of the field `tm_u` describes (box 40 x 24 x 1 x 3, order 4),
+// gJ and gout in the field's dense layout (geometry g).  Tiles of 32 x TT_Y,
+// dealt round-robin, z split as the Jacobian map's.
+template <typename T>
+cudaError_t launch_adjoint_tma(const CUtensorMap &tm_u, const Geom &g, const T *gJ, T *gout, int num_sms,
+                               cudaStream_t s) {
+    constexpr int TXW = 32, TYT = 16, BZ = 32;
+    constexpr int smem = AdjTmaLayout<T, TXW>::BYTES + 128;
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_adjoint_tma<T, TXW, TYT>, smem, devs);
+    if (attr != cudaSuccess) return attr;
+    const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
+    const int cols = tiles_x * tiles_y;
+    const int slots = std::max(1, adjoint_tma_blocks_v<T, TXW, TYT>()) * num_sms;
+    int nzt = (g.nz + BZ - 1) / BZ;
+    const int waves = (cols * nzt + slots - 1) / slots;
+    nzt = std::min((g.nz + 7) / 8, std::max(nzt, waves * slots / cols));
+    const int bz = (g.nz + nzt - 1) / nzt;
+    const int ntiles = cols * ((g.nz + bz - 1) / bz);
+    const int grid = std::min(ntiles, slots);
+    k_adjoint_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_u, g, gJ, gout, tiles_x, tiles_y, ntiles,
+                                                                       bz);
+    count_launch();
+    return cudaGetLastError();
+}
+
 #define DTB_INSTANTIATE_TMA(T)                                                                              \
     template cudaError_t launch_trial_tma<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
                                              unsigned char *, int, int, TileQueue *, int);                  \
@@ -1923,6 +2321,8 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
     template int gradient_tma_blocks_per_sm<T>(int, int);                                                   \
     template cudaError_t launch_trial_rel<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
                                              unsigned char *, int, int, TileQueue *);                       \
-    template int trial_rel_blocks_per_sm<T>(int, int);
+    template int trial_rel_blocks_per_sm<T>(int, int);                                                     \
+    template cudaError_t launch_adjoint_tma<T>(const CUtensorMap &, const Geom &, const T *, T *, int,       \
+                                               cudaStream_t);
 
 }  // namespace dtb
