@@ -442,8 +442,9 @@ int dtb_get_tile_config(int shape[4]);
  * for the kernel that forms each candidate plane in a shared ring (one
  * block barrier per plane), 1 for the kernel that keeps each stage until its
  * plane was the stencil's centre, forms the candidate's taps where it reads
- * them and has no barrier in its plane loop.  The autotuner chooses between
- * them; DISPTOOLS_B200_TRIAL_KERNEL = formed | release forces one.  Returns
+ * them and has no barrier in its plane loop.  The autotuner uses the first
+ * (the second measured slower); DISPTOOLS_B200_TRIAL_KERNEL = formed |
+ * release forces one.  Returns
  * DTB_ERR_ARGUMENT before the first solve on the device.  No counterpart in
  * the reference. */
 int dtb_get_trial_kernel(void);

@@ -301,10 +301,12 @@ ENV_OF = (("TILE_X", "tile_x"), ("TRIAL_THREADS_Y", "trial_threads_y"), ("THREAD
 
 
 def _is_candidate(cfg) -> bool:
-    """A shape the autotuner may choose: a listed x-y shape and kernel, and a
-    z depth that is listed or wave-filled (12..64 planes)."""
+    """A shape the autotuner may choose: a listed x-y shape with the
+    formed-plane trial kernel, and a z depth that is listed or wave-filled
+    (12..64 planes)."""
     key = lambda c: (c["tile_x"], c["trial_threads_y"], c["gradient_threads_y"], c["trial_kernel"])  # noqa: E731
-    return any(key(c) == key(cfg) for c in TILE_CANDIDATES) and 12 <= cfg["bz"] <= 64
+    return (cfg["trial_kernel"] == "formed" and any(key(c) == key(cfg) for c in TILE_CANDIDATES)
+            and 12 <= cfg["bz"] <= 64)
 
 
 def test_autotuned_shapes(oracle, monkeypatch):
