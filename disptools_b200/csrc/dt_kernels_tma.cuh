@@ -2029,6 +2029,34 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
     const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1], FD<T>::one_twelfth * ih[2]};
     const int n[3] = {g.nx, g.ny, g.nz};
+    // Fourth-order difference (the generic path's arithmetic for S_C4).
+    auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
+        if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+        return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
+    };
+    // x and y differences (rows: a0 of the pair's first cell, a1 of its
+    // second) of the cell pair at box offset o of plane pl, component c.
+    auto xy_pair = [&](const T *pl, int c, int o, T (&a0)[3][3], T (&a1)[3][3], bool want_x, bool want_y) {
+        const T *q = pl + c * PLANE + o;
+        if (want_x) {
+            const auto xm = ld_pair(q - 2), xc = ld_pair(q), xp = ld_pair(q + 2);
+            a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
+            a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
+        }
+        if (want_y) {
+            const auto ym1 = ld_pair(q - PX), yp1 = ld_pair(q + PX), ym2 = ld_pair(q - 2 * PX), yp2 = ld_pair(q + 2 * PX);
+            a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
+            a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+        }
+    };
+    // z differences of the cell pair at box offset o, component c, plane m.
+    auto z_pair = [&](const Planes5<T> &sp, int c, int o, T (&a0)[3][3], T (&a1)[3][3]) {
+        const int oc = c * PLANE + o;
+        const auto zm2 = ld_pair(sp.m2 + oc), zm1 = ld_pair(sp.m1 + oc);
+        const auto zp1 = ld_pair(sp.p1 + oc), zp2 = ld_pair(sp.p2 + oc);
+        a0[c][2] = c4(zp1.x, zm1.x, zp2.x, zm2.x, 2);
+        a1[c][2] = c4(zp1.y, zm1.y, zp2.y, zm2.y, 2);
+    };
     uint32_t kbase = 0;
 
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -2072,7 +2100,29 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
             const int p = z0 - 2 + it;  // newest plane
             const int m = p - 2;        // centre plane of this iteration's x and y weights and gradient
             // (a) z weights of plane p at the own voxels (in-plane differences only).
-            {
+            if (tile_c4_own && p >= 2 && p <= g.nz - 3) {
+                // Every own cell of the plane is fourth order in x and y.
+                T a0[3][3], a1[3][3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    xy_pair(stage(it), c, byo * PX + bxo, a0, a1, true, true);
+                    a0[c][2] = a1[c][2] = T(0);  // not used by the z weights
+                }
+                const long long go = (long long) p * g.zs + (long long) y * g.ys + x;
+                T wz0[3], wz1[3];
+                adj_weights<T>(a0, gJ[go], 2, ih[2], wz0);
+                adj_weights<T>(a1, gJ[go + 1], 2, ih[2], wz1);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        zw[0][c][kk] = zw[0][c][kk + 1];
+                        zw[1][c][kk] = zw[1][c][kk + 1];
+                    }
+                    zw[0][c][4] = wz0[c];
+                    zw[1][c][4] = wz1[c];
+                }
+            } else {
                 const Planes5<T> sp{nullptr, nullptr, stage(it), nullptr, nullptr};
                 const bool p_vol = p >= 0 && p < g.nz;
 #pragma unroll
@@ -2107,6 +2157,74 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
             if (centre && !s_fault) {
                 const Planes5<T> sp{stage(it - 4), stage(it - 3), stage(it - 2), stage(it - 1), stage(it)};
                 const bool fast = tile_c4_halo && m >= 2 && m <= g.nz - 3;
+                const int h = tid - (NTH - NH);
+                if (fast) {
+                    // Own pair: all nine differences, fourth order.
+                    {
+                        T a0[3][3], a1[3][3];
+                        const int o = byo * PX + bxo;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            xy_pair(sp.c0, c, o, a0, a1, true, true);
+                            z_pair(sp, c, o, a0, a1);
+                        }
+                        const long long go = (long long) m * g.zs + (long long) y * g.ys + x;
+                        const T w0 = gJ[go], w1 = gJ[go + 1];
+                        T wx0[3], wx1[3], wy0[3], wy1[3];
+                        adj_weights<T>(a0, w0, 0, ih[0], wx0);
+                        adj_weights<T>(a1, w1, 0, ih[0], wx1);
+                        adj_weights<T>(a0, w0, 1, ih[1], wy0);
+                        adj_weights<T>(a1, w1, 1, ih[1], wy1);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            st_pair(WX + (c * TT_Y + ty) * WXC + 2 * tx + 2, wx0[c], wx1[c]);
+                            st_pair(WY + (c * (TT_Y + 4) + ty + 2) * WYC + 2 * tx, wy0[c], wy1[c]);
+                        }
+                    }
+                    // Halo pairs: the x weights need differences along y
+                    // and z, the y weights along x and z.
+                    if (h >= 0) {
+                        const bool xside = h < NHX;
+                        int cx, cy;
+                        if (xside) {
+                            cx = (h / TT_Y) ? x0 + TXW : x0 - 2;
+                            cy = y0 + h % TT_Y;
+                        } else {
+                            const int h2 = h - NHX, r = h2 / TPX;
+                            cx = x0 + 2 * (h2 % TPX);
+                            cy = r < 2 ? y0 - 2 + r : y0 + TT_Y - 2 + r;
+                        }
+                        const int o = (cy - y0 + 4) * PX + (cx - x0 + 4);
+                        const long long go = (long long) m * g.zs + (long long) cy * g.ys + cx;
+                        const T w0 = gJ[go], w1 = gJ[go + 1];
+                        T a0[3][3], a1[3][3], wv0[3], wv1[3];
+                        if (xside) {
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                a0[c][0] = a1[c][0] = T(0);
+                                xy_pair(sp.c0, c, o, a0, a1, false, true);
+                                z_pair(sp, c, o, a0, a1);
+                            }
+                            adj_weights<T>(a0, w0, 0, ih[0], wv0);
+                            adj_weights<T>(a1, w1, 0, ih[0], wv1);
+#pragma unroll
+                            for (int c = 0; c < 3; ++c)
+                                st_pair(WX + (c * TT_Y + (cy - y0)) * WXC + (cx - x0 + 2), wv0[c], wv1[c]);
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                a0[c][1] = a1[c][1] = T(0);
+                                xy_pair(sp.c0, c, o, a0, a1, true, false);
+                                z_pair(sp, c, o, a0, a1);
+                            }
+                            adj_weights<T>(a0, w0, 1, ih[1], wv0);
+                            adj_weights<T>(a1, w1, 1, ih[1], wv1);
+#pragma unroll
+                            for (int c = 0; c < 3; ++c)
+                                st_pair(WY + (c * (TT_Y + 4) + (cy - y0 + 2)) * WYC + (cx - x0), wv0[c], wv1[c]);
+                        }
+                    }
+                } else {
                 // (b) own voxels: x and y weights of plane m.
 #pragma unroll
                 for (int v = 0; v < 2; ++v) {
@@ -2134,7 +2252,6 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                 // (c) halo cells, two adjacent x cells per task: the x
                 // weights of the two columns each side, the y weights of the
                 // two rows each side.
-                const int h = tid - (NTH - NH);
                 if (h >= 0) {
                     const bool xside = h < NHX;
                     int cx, cy;  // first cell of the pair
@@ -2184,6 +2301,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                         }
                     }
                 }
+                }  // generic path
             }
             __syncthreads();
             if (s_fault) {
@@ -2193,8 +2311,47 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
             // Iteration it - 4's stage (plane m - 2) is not read again.
             if (tid == 0 && it >= 4 && it + 3 < n_it) issue(it + 3);
             // (d) gradient of the own voxels at plane m.
-            if (centre && row_vol) {
-                const bool deep = tile_deep && m >= 4 && m <= g.nz - 5;
+            const bool deep = tile_deep && m >= 4 && m <= g.nz - 5;
+            if (centre && deep) {
+                // Every tap of the tile is fourth order: constant weights,
+                // the general path's tap and summation order.
+                T acc0[3] = {T(0), T(0), T(0)}, acc1[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const T *wxr = WX + (c * TT_Y + ty) * WXC + 2 * tx;  // columns x-2 .. x+3
+                    const auto xa = ld_pair(wxr), xb = ld_pair(wxr + 2), xc = ld_pair(wxr + 4);
+                    const T wxv[6] = {xa.x, xa.y, xb.x, xb.y, xc.x, xc.y};
+#pragma unroll
+                    for (int t = -2; t <= 2; ++t) {
+                        if (t == 0) continue;
+                        const T kp = kappa<T>(S_C4, t);
+                        acc0[c] += wxv[2 - t] * kp;
+                        acc1[c] += wxv[3 - t] * kp;
+                    }
+                    const T *wyc = WY + (c * (TT_Y + 4) + ty + 2) * WYC + 2 * tx;
+#pragma unroll
+                    for (int t = -2; t <= 2; ++t) {
+                        if (t == 0) continue;
+                        const T kp = kappa<T>(S_C4, t);
+                        const auto wy = ld_pair(wyc - t * WYC);
+                        acc0[c] += wy.x * kp;
+                        acc1[c] += wy.y * kp;
+                    }
+#pragma unroll
+                    for (int t = -2; t <= 2; ++t) {
+                        if (t == 0) continue;
+                        const T kp = kappa<T>(S_C4, t);
+                        acc0[c] += zw[0][c][2 - t] * kp;
+                        acc1[c] += zw[1][c][2 - t] * kp;
+                    }
+                }
+                const long long off = (long long) m * g.zs + (long long) y * g.ys + x;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    gout[c * g.cs + off] = acc0[c];
+                    gout[c * g.cs + off + 1] = acc1[c];
+                }
+            } else if (centre && row_vol) {
 #pragma unroll
                 for (int v = 0; v < 2; ++v) {
                     const int xv = x + v;

@@ -10,6 +10,7 @@ as small .npz files.  Run it where the reference sources are available:
 
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py --maps   # maps.npz only
+    python tests/golden/make_golden.py --config2   # config2_converged.json (minutes)
 
 maps.npz comes from the reference's own Python map functions
 (disptools/displacements.py), executed from its source with the SimpleITK
@@ -183,7 +184,38 @@ def map_fixtures(ref) -> dict:
     return out
 
 
+def config2_converged(ref_verbose) -> dict:
+    """The headline volume (config 2: 256^3, 16 Gaussian blobs, seed 0) solved
+    by the reference C library (FP64, verbose build) from the zero field with
+    the default parameters and it_max 50000 (the reference wrapper's), i.e.
+    to its own termination.  Stored as a summary: iterations, the last
+    printed line, the final masked max |J - J_t| of the returned field
+    (recomputed by the reference's jacobian), the field's sums and one line."""
+    from disptools_b200.synthetic import blob_problem
+    Jt, mask = blob_problem((256, 256, 256), blobs=16, seed=0)
+    field, lines, its = ref_verbose.solve_logged("gradient", Jt, mask, it_max=50000)
+    J = Reference("ref64").jacobian(field)
+    last = [ln for ln in lines if ln.startswith("Iteration")][-1].split()
+    return {
+        "iterations": its,
+        "stop_line": lines[-1],
+        "total_error": float(last[4]),
+        "max_voxel_error": float(last[8]),
+        "masked_max": float(np.max(np.abs(J - Jt)[mask])),
+        "field_abs_sum": float(np.abs(field).sum()),
+        "field_line": field[:, 128, 128, ::8].tolist(),
+        "threads": os.environ.get("OMP_NUM_THREADS", str(os.cpu_count())),
+    }
+
+
 def main() -> None:
+    if "--config2" in sys.argv:
+        build(ref=True)
+        out = config2_converged(Reference("ref64_verbose"))
+        with open(os.path.join(HERE, "config2_converged.json"), "w") as fh:
+            json.dump(out, fh, indent=1)
+        print("config-2 summary written to", HERE)
+        return
     if "--maps" in sys.argv:
         build(ref=True)
         np.savez_compressed(os.path.join(HERE, "maps.npz"), **map_fixtures(Reference("ref64")))

@@ -141,7 +141,8 @@ def test_batched_fp32_autograd_config3():
 
 
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
-@pytest.mark.parametrize("shape", [(3, 3, 4), (5, 9, 12), (7, 17, 36), (40, 40, 96), (37, 21, 100)])
+@pytest.mark.parametrize("shape", [(3, 3, 4), (5, 9, 12), (7, 17, 36), (40, 40, 96), (37, 21, 100),
+                                   (30, 53, 132)])
 def test_fused_adjoint_equals_two_pass(monkeypatch, dtype, shape):
     """The fused adjoint kernel (one launch, weights on chip) against the
     weight pass + gather (DISPTOOLS_B200_ADJOINT=two-pass): bit for bit in
