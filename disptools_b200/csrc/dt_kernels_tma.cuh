@@ -818,6 +818,14 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const CUtensorMap *tm_u = V.tm_field[old_b];
         const CUtensorMap *tm_e = V.tm_ep[old_b];
         const T ihx = (T) g.ih[0], ihy = (T) g.ih[1], ihz = (T) g.ih[2];
+        // Second-order central difference (p1 - m1) * ih * 0.5.  In FP32 the
+        // factor 0.5 ih is folded into one constant: halving is exact, so the
+        // result is the same, with one multiply fewer.
+        const T hx = ihx * T(0.5), hy = ihy * T(0.5), hz = ihz * T(0.5);
+        auto c2 = [&](T p1, T m1, int ax) -> T {
+            if (sizeof(T) == 4) return (p1 - m1) * (ax == 0 ? hx : (ax == 1 ? hy : hz));
+            return fd_c2<T>(p1, m1, ax == 0 ? ihx : (ax == 1 ? ihy : ihz));
+        };
 
         int issued_n = 0;
         auto issue = [&](int j) {
@@ -891,9 +899,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const int o = c * TMA_PLANE + cy * TMA_PX + cx;
-                        m[c][0] = fd_c2<T>(u0[o + 1], u0[o - 1], ihx);
-                        m[c][1] = fd_c2<T>(u0[o + TMA_PX], u0[o - TMA_PX], ihy);
-                        m[c][2] = fd_c2<T>(up[o], um[o], ihz);
+                        m[c][0] = c2(u0[o + 1], u0[o - 1], 0);
+                        m[c][1] = c2(u0[o + TMA_PX], u0[o - TMA_PX], 1);
+                        m[c][2] = c2(up[o], um[o], 2);
                         m[c][c] += T(1.0);
                     }
                 };
@@ -905,12 +913,12 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                         const auto xm = ld_pair(u0 + o - 2), xc = ld_pair(u0 + o), xp = ld_pair(u0 + o + 2);
                         const auto ym = ld_pair(u0 + o - TMA_PX), yp = ld_pair(u0 + o + TMA_PX);
                         const auto zm = ld_pair(um + o), zp = ld_pair(up + o);
-                        m0[c][0] = fd_c2<T>(xc.y, xm.y, ihx);
-                        m1[c][0] = fd_c2<T>(xp.x, xc.x, ihx);
-                        m0[c][1] = fd_c2<T>(yp.x, ym.x, ihy);
-                        m1[c][1] = fd_c2<T>(yp.y, ym.y, ihy);
-                        m0[c][2] = fd_c2<T>(zp.x, zm.x, ihz);
-                        m1[c][2] = fd_c2<T>(zp.y, zm.y, ihz);
+                        m0[c][0] = c2(xc.y, xm.y, 0);
+                        m1[c][0] = c2(xp.x, xc.x, 0);
+                        m0[c][1] = c2(yp.x, ym.x, 1);
+                        m1[c][1] = c2(yp.y, ym.y, 1);
+                        m0[c][2] = c2(zp.x, zm.x, 2);
+                        m1[c][2] = c2(zp.y, zm.y, 2);
                         m0[c][c] += T(1.0);
                         m1[c][c] += T(1.0);
                     }
