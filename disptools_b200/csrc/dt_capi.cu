@@ -1369,12 +1369,12 @@ int jacobian_device_impl(const Geom &g, const T *field, T *J, cudaStream_t s) {
     return DTB_OK;
 }
 
-// The adjoint's path: the fused TMA kernel (order 4, a 16-byte-aligned field
-// whose rows are a multiple of 16 bytes long), unless
-// DISPTOOLS_B200_ADJOINT=two-pass asks for the weight pass and gather.
+// The adjoint's path: the weight pass and gather by default, the fused TMA
+// kernel (order 4, a 16-byte-aligned field whose rows are a multiple of 16
+// bytes long) when DISPTOOLS_B200_ADJOINT=fused asks for it.
 bool adjoint_fused_allowed() {
     const char *e = std::getenv("DISPTOOLS_B200_ADJOINT");
-    return !(e && std::strcmp(e, "two-pass") == 0);
+    return e && std::strcmp(e, "fused") == 0;
 }
 
 template <typename T>

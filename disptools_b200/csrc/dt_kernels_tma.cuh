@@ -2018,7 +2018,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     constexpr int TPX = TXW / 2, NTH = TPX * TYT, S = L::S, PX = L::PX, PLANE = L::PLANE;
     constexpr int WXC = L::WXC, WYC = L::WYC;
     constexpr int NHX = TT_Y * 2, NHY = 4 * TPX, NH = NHX + NHY;  // halo pair tasks: x sides, y sides
-    static_assert(TYT == TT_Y, "one tile row per thread row");
+    static_assert(TYT == TT_Y && TPX == 16, "one tile row per thread row, two rows per warp");
     static_assert(NH <= NTH - 64, "halo tasks on threads other than the first two warps");
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char *smem = align_smem_128(smem_dyn);
@@ -2042,28 +2042,75 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
         if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
         return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
     };
-    // x and y differences (rows: a0 of the pair's first cell, a1 of its
-    // second) of the cell pair at box offset o of plane pl, component c.
-    auto xy_pair = [&](const T *pl, int c, int o, T (&a0)[3][3], T (&a1)[3][3], bool want_x, bool want_y) {
-        const T *q = pl + c * PLANE + o;
-        if (want_x) {
-            const auto xm = ld_pair(q - 2), xc = ld_pair(q), xp = ld_pair(q + 2);
-            a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
-            a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
+    // Differences of the cell pair (xf, xf + 1) at box offset o (row and
+    // plane at least two cells inside the volume): along x, y and z as
+    // requested, with each cell's scheme chosen by its x position
+    // (src/jacobian.c:113-241): outer column -> one-sided in x and second
+    // order in y and z; penultimate column -> second order; else fourth
+    // order.  With all_c4 every cell is fourth order (no selects).  Rows a0
+    // of the first cell, a1 of the second.
+    auto pair_diffs = [&](const Planes5<T> &sp, int c, int o, int xf, bool all_c4, bool wx, bool wy, bool wz,
+                          T (&a0)[3][3], T (&a1)[3][3]) {
+        const T *q = sp.c0 + c * PLANE + o;
+        const int oc = c * PLANE + o;
+        if (all_c4) {
+            if (wx) {
+                const auto xm = ld_pair(q - 2), xc = ld_pair(q), xp = ld_pair(q + 2);
+                a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
+                a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
+            }
+            if (wy) {
+                const auto ym1 = ld_pair(q - PX), yp1 = ld_pair(q + PX), ym2 = ld_pair(q - 2 * PX),
+                           yp2 = ld_pair(q + 2 * PX);
+                a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
+                a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+            }
+            if (wz) {
+                const auto zm2 = ld_pair(sp.m2 + oc), zm1 = ld_pair(sp.m1 + oc);
+                const auto zp1 = ld_pair(sp.p1 + oc), zp2 = ld_pair(sp.p2 + oc);
+                a0[c][2] = c4(zp1.x, zm1.x, zp2.x, zm2.x, 2);
+                a1[c][2] = c4(zp1.y, zm1.y, zp2.y, zm2.y, 2);
+            }
+            return;
         }
-        if (want_y) {
-            const auto ym1 = ld_pair(q - PX), yp1 = ld_pair(q + PX), ym2 = ld_pair(q - 2 * PX), yp2 = ld_pair(q + 2 * PX);
-            a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
-            a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+            T(&a)[3][3] = v ? a1 : a0;
+            const int xv = xf + v;
+            const bool xo_lo = xv == 0, xo_hi = xv == g.nx - 1;
+            const bool second = xo_lo || xo_hi || xv == 1 || xv == g.nx - 2;
+            const T *p = q + v;
+            if (wx) {
+                const T fx = xo_lo ? fd_fwd<T>(p[0], p[1], p[2], ih[0])
+                                   : (xo_hi ? fd_bwd<T>(p[0], p[-1], p[-2], ih[0]) : fd_c2<T>(p[1], p[-1], ih[0]));
+                const T cx4 = c4(p[1], p[-1], p[2], p[-2], 0);
+                a[c][0] = second ? fx : cx4;
+            }
+            if (wy) {
+                const T cy4 = c4(p[PX], p[-PX], p[2 * PX], p[-2 * PX], 1);
+                const T cy2 = fd_c2<T>(p[PX], p[-PX], ih[1]);
+                a[c][1] = second ? cy2 : cy4;
+            }
+            if (wz) {
+                const T zp1 = sp.p1[oc + v], zm1 = sp.m1[oc + v], zp2 = sp.p2[oc + v], zm2 = sp.m2[oc + v];
+                const T cz4 = c4(zp1, zm1, zp2, zm2, 2);
+                const T cz2 = fd_c2<T>(zp1, zm1, ih[2]);
+                a[c][2] = second ? cz2 : cz4;
+            }
         }
     };
-    // z differences of the cell pair at box offset o, component c, plane m.
-    auto z_pair = [&](const Planes5<T> &sp, int c, int o, T (&a0)[3][3], T (&a1)[3][3]) {
-        const int oc = c * PLANE + o;
-        const auto zm2 = ld_pair(sp.m2 + oc), zm1 = ld_pair(sp.m1 + oc);
-        const auto zp1 = ld_pair(sp.p1 + oc), zp2 = ld_pair(sp.p2 + oc);
-        a0[c][2] = c4(zp1.x, zm1.x, zp2.x, zm2.x, 2);
-        a1[c][2] = c4(zp1.y, zm1.y, zp2.y, zm2.y, 2);
+    // Differences of one cell by the schemes schemes_at gives it (any
+    // position in the volume).
+    auto cell_diffs = [&](const Planes5<T> &sp, int x, int y, int z, int o, bool wx, bool wy, bool wz,
+                          T (&a)[3][3]) {
+        int ks[3];
+        schemes_at(x, y, z, g, ks);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            a[c][0] = wx ? adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2) : T(0);
+            a[c][1] = wy ? adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2) : T(0);
+            a[c][2] = wz ? adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2) : T(0);
+        }
     };
     uint32_t kbase = 0;
 
@@ -2090,36 +2137,94 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
         const int x = x0 + 2 * tx, y = y0 + ty;  // own voxels (x, y), (x + 1, y)
         const int bxo = 2 * tx + 4, byo = ty + 4;  // their box cell
         const bool row_vol = y < g.ny;
-        // Own z weights W[c][2] of planes m-2 .. m+2 (queue index 2 + d for plane m + d).
+        const bool x0_vol = x < g.nx, x1_vol = x + 1 < g.nx;
+        // Rows of this thread's warp (two tile rows) at least two cells
+        // inside the volume; tile columns likewise (fourth order in x).
+        const int yw = y0 + (ty & ~1);
+        const bool warp_rows_in = yw >= 2 && yw + 1 <= g.ny - 3;
+        const bool cols_c4 = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3;
+        const bool warp_rows_deep = yw >= 4 && yw + 1 <= g.ny - 5;
+        const bool cols_deep = x0 >= 4 && x0 + TXW - 1 <= g.nx - 5;
+        // Own z weights W[c][2] of planes m-2 .. m+2 (queue index 2 + d for
+        // plane m + d), and own gJ of planes p-2 .. p (index 0 .. 2).
         T zw[2][3][5];
+        T gq[2][3];
 #pragma unroll
-        for (int v = 0; v < 2; ++v)
+        for (int v = 0; v < 2; ++v) {
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
                 for (int k = 0; k < 5; ++k) zw[v][c][k] = T(0);
-        const bool tile_c4_own = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3 && y0 >= 2 && y0 + TT_Y - 1 <= g.ny - 3;
-        const bool tile_c4_halo = x0 >= 4 && x0 + TXW + 1 <= g.nx - 3 && y0 >= 4 && y0 + TT_Y + 1 <= g.ny - 3;
-        const bool tile_deep = x0 >= 4 && x0 + TXW - 1 <= g.nx - 5 && y0 >= 4 && y0 + TT_Y - 1 <= g.ny - 5;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) gq[v][k] = T(0);
+        }
+        auto own_gj = [&](int z, int v) -> T {
+            const bool in = z >= 0 && z < g.nz && row_vol && (v ? x1_vol : x0_vol);
+            return in ? gJ[(long long) z * g.zs + (long long) y * g.ys + x + v] : T(0);
+        };
+        T gnext[2] = {own_gj(z0 - 2, 0), own_gj(z0 - 2, 1)};  // gJ of the next newest plane
         bool failed = false;
         for (int it = 0; it < n_it; ++it) {
             const uint32_t k = kbase + it;
             if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u)) s_fault = 1;
             const int p = z0 - 2 + it;  // newest plane
             const int m = p - 2;        // centre plane of this iteration's x and y weights and gradient
-            // (a) z weights of plane p at the own voxels (in-plane differences only).
-            if (tile_c4_own && p >= 2 && p <= g.nz - 3) {
-                // Every own cell of the plane is fourth order in x and y.
-                T a0[3][3], a1[3][3];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    xy_pair(stage(it), c, byo * PX + bxo, a0, a1, true, true);
-                    a0[c][2] = a1[c][2] = T(0);  // not used by the z weights
+            for (int v = 0; v < 2; ++v) {
+                gq[v][0] = gq[v][1];
+                gq[v][1] = gq[v][2];
+                gq[v][2] = gnext[v];
+                gnext[v] = own_gj(p + 1, v);  // used next iteration
+            }
+            const bool centre = m >= z0 && m < z1;
+            // Halo task of this thread (x sides: pairs of columns x0-2, x0-1
+            // or x0+TXW, x0+TXW+1 on a tile row; y sides: pairs of tile
+            // columns on rows y0-2, y0-1, y0+TT_Y, y0+TT_Y+1), and its gJ,
+            // loaded before the weights are formed.
+            const int h = tid - (NTH - NH);
+            const bool xside = h < NHX;
+            int cx = 0, cy = 0;
+            if (h >= 0) {
+                if (xside) {
+                    cx = (h / TT_Y) ? x0 + TXW : x0 - 2;
+                    cy = y0 + h % TT_Y;
+                } else {
+                    const int h2 = h - NHX, r = h2 / TPX;
+                    cx = x0 + 2 * (h2 % TPX);
+                    cy = r < 2 ? y0 - 2 + r : y0 + TT_Y - 2 + r;
                 }
-                const long long go = (long long) p * g.zs + (long long) y * g.ys + x;
-                T wz0[3], wz1[3];
-                adj_weights<T>(a0, gJ[go], 2, ih[2], wz0);
-                adj_weights<T>(a1, gJ[go + 1], 2, ih[2], wz1);
+            }
+            T hw[2] = {T(0), T(0)};
+            if (h >= 0 && centre) {
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const int xv = cx + v;
+                    if (xv >= 0 && xv < g.nx && cy >= 0 && cy < g.ny)
+                        hw[v] = gJ[(long long) m * g.zs + (long long) cy * g.ys + xv];
+                }
+            }
+            // (a) z weights of plane p at the own voxels (in-plane differences only).
+            {
+                const Planes5<T> sp{nullptr, nullptr, stage(it), nullptr, nullptr};
+                T wz0[3] = {T(0), T(0), T(0)}, wz1[3] = {T(0), T(0), T(0)};
+                if (p >= 2 && p <= g.nz - 3 && warp_rows_in) {
+                    T a0[3][3], a1[3][3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        pair_diffs(sp, c, byo * PX + bxo, x, cols_c4, true, true, false, a0, a1);
+                        a0[c][2] = a1[c][2] = T(0);  // not used by the z weights
+                    }
+                    adj_weights<T>(a0, gq[0][2], 2, ih[2], wz0);
+                    adj_weights<T>(a1, gq[1][2], 2, ih[2], wz1);
+                } else if (p >= 0 && p < g.nz && row_vol) {
+#pragma unroll
+                    for (int v = 0; v < 2; ++v) {
+                        if (x + v >= g.nx) continue;
+                        T a[3][3];
+                        cell_diffs(sp, x + v, y, p, byo * PX + bxo + v, true, true, false, a);
+                        adj_weights<T>(a, gq[v][2], 2, ih[2], v ? wz1 : wz0);
+                    }
+                }
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -2130,186 +2235,94 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                     zw[0][c][4] = wz0[c];
                     zw[1][c][4] = wz1[c];
                 }
-            } else {
-                const Planes5<T> sp{nullptr, nullptr, stage(it), nullptr, nullptr};
-                const bool p_vol = p >= 0 && p < g.nz;
-#pragma unroll
-                for (int v = 0; v < 2; ++v) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-#pragma unroll
-                        for (int kk = 0; kk < 4; ++kk) zw[v][c][kk] = zw[v][c][kk + 1];
-                    T wz[3] = {T(0), T(0), T(0)};
-                    const int xv = x + v;
-                    if (p_vol && row_vol && xv < g.nx) {
-                        int ks[3] = {S_C4, S_C4, S_C4};
-                        if (!(tile_c4_own && p >= 2 && p <= g.nz - 3)) schemes_at(xv, y, p, g, ks);
-                        const int o = byo * PX + bxo + v;
-                        T a[3][3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            a[c][0] = adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2);
-                            a[c][1] = adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2);
-                            a[c][2] = T(0);  // not used by the z weights
-                        }
-                        const T w = gJ[(long long) p * g.zs + (long long) y * g.ys + xv];
-                        adj_weights<T>(a, w, 2, ih[2], wz);
-                    }
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) zw[v][c][4] = wz[c];
-                }
             }
-            const bool centre = m >= z0 && m < z1;
             T *wb = reinterpret_cast<T *>(smem + L::W_OFF) + (it & 1) * L::W_ELEMS;
             T *WX = wb, *WY = wb + L::WX_ELEMS;
             if (centre && !s_fault) {
                 const Planes5<T> sp{stage(it - 4), stage(it - 3), stage(it - 2), stage(it - 1), stage(it)};
-                const bool fast = tile_c4_halo && m >= 2 && m <= g.nz - 3;
-                const int h = tid - (NTH - NH);
-                if (fast) {
-                    // Own pair: all nine differences, fourth order.
-                    {
+                const bool plane_in = m >= 2 && m <= g.nz - 3;
+                // (b) own voxels: x and y weights of plane m.
+                {
+                    T wx0[3] = {T(0), T(0), T(0)}, wx1[3] = {T(0), T(0), T(0)};
+                    T wy0[3] = {T(0), T(0), T(0)}, wy1[3] = {T(0), T(0), T(0)};
+                    if (plane_in && warp_rows_in) {
                         T a0[3][3], a1[3][3];
-                        const int o = byo * PX + bxo;
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            xy_pair(sp.c0, c, o, a0, a1, true, true);
-                            z_pair(sp, c, o, a0, a1);
-                        }
-                        const long long go = (long long) m * g.zs + (long long) y * g.ys + x;
-                        const T w0 = gJ[go], w1 = gJ[go + 1];
-                        T wx0[3], wx1[3], wy0[3], wy1[3];
-                        adj_weights<T>(a0, w0, 0, ih[0], wx0);
-                        adj_weights<T>(a1, w1, 0, ih[0], wx1);
-                        adj_weights<T>(a0, w0, 1, ih[1], wy0);
-                        adj_weights<T>(a1, w1, 1, ih[1], wy1);
+                        for (int c = 0; c < 3; ++c)
+                            pair_diffs(sp, c, byo * PX + bxo, x, cols_c4, true, true, true, a0, a1);
+                        adj_weights<T>(a0, gq[0][0], 0, ih[0], wx0);
+                        adj_weights<T>(a1, gq[1][0], 0, ih[0], wx1);
+                        adj_weights<T>(a0, gq[0][0], 1, ih[1], wy0);
+                        adj_weights<T>(a1, gq[1][0], 1, ih[1], wy1);
+                    } else if (row_vol) {
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            st_pair(WX + (c * TT_Y + ty) * WXC + 2 * tx + 2, wx0[c], wx1[c]);
-                            st_pair(WY + (c * (TT_Y + 4) + ty + 2) * WYC + 2 * tx, wy0[c], wy1[c]);
+                        for (int v = 0; v < 2; ++v) {
+                            if (x + v >= g.nx) continue;
+                            T a[3][3];
+                            cell_diffs(sp, x + v, y, m, byo * PX + bxo + v, true, true, true, a);
+                            adj_weights<T>(a, gq[v][0], 0, ih[0], v ? wx1 : wx0);
+                            adj_weights<T>(a, gq[v][0], 1, ih[1], v ? wy1 : wy0);
                         }
                     }
-                    // Halo pairs: the x weights need differences along y
-                    // and z, the y weights along x and z.
-                    if (h >= 0) {
-                        const bool xside = h < NHX;
-                        int cx, cy;
-                        if (xside) {
-                            cx = (h / TT_Y) ? x0 + TXW : x0 - 2;
-                            cy = y0 + h % TT_Y;
-                        } else {
-                            const int h2 = h - NHX, r = h2 / TPX;
-                            cx = x0 + 2 * (h2 % TPX);
-                            cy = r < 2 ? y0 - 2 + r : y0 + TT_Y - 2 + r;
-                        }
-                        const int o = (cy - y0 + 4) * PX + (cx - x0 + 4);
-                        const long long go = (long long) m * g.zs + (long long) cy * g.ys + cx;
-                        const T w0 = gJ[go], w1 = gJ[go + 1];
-                        T a0[3][3], a1[3][3], wv0[3], wv1[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        st_pair(WX + (c * TT_Y + ty) * WXC + 2 * tx + 2, wx0[c], wx1[c]);
+                        st_pair(WY + (c * (TT_Y + 4) + ty + 2) * WYC + 2 * tx, wy0[c], wy1[c]);
+                    }
+                }
+                // (c) halo pairs: the x weights use columns 1 and 2 of I + A
+                // (differences along y and z), the y weights 0 and 2.
+                if (h >= 0) {
+                    const int o = (cy - y0 + 4) * PX + (cx - x0 + 4);
+                    T wv0[3] = {T(0), T(0), T(0)}, wv1[3] = {T(0), T(0), T(0)};
+                    const bool cells_in = cx >= 0 && cx + 1 < g.nx && cy >= 0 && cy < g.ny;
+                    const bool row_in = cy >= 2 && cy <= g.ny - 3;
+                    // x sides: two columns at least two inside the volume;
+                    // y sides: any columns, selects at the x ends.
+                    const bool pair_ok = plane_in && row_in && cells_in && (!xside || (cx >= 2 && cx + 1 <= g.nx - 3));
+                    const bool pair_c4 = cx >= 2 && cx + 1 <= g.nx - 3;
+                    if (pair_ok) {
+                        T a0[3][3], a1[3][3];
                         if (xside) {
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
                                 a0[c][0] = a1[c][0] = T(0);
-                                xy_pair(sp.c0, c, o, a0, a1, false, true);
-                                z_pair(sp, c, o, a0, a1);
+                                pair_diffs(sp, c, o, cx, true, false, true, true, a0, a1);
                             }
-                            adj_weights<T>(a0, w0, 0, ih[0], wv0);
-                            adj_weights<T>(a1, w1, 0, ih[0], wv1);
-#pragma unroll
-                            for (int c = 0; c < 3; ++c)
-                                st_pair(WX + (c * TT_Y + (cy - y0)) * WXC + (cx - x0 + 2), wv0[c], wv1[c]);
+                            adj_weights<T>(a0, hw[0], 0, ih[0], wv0);
+                            adj_weights<T>(a1, hw[1], 0, ih[0], wv1);
                         } else {
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
                                 a0[c][1] = a1[c][1] = T(0);
-                                xy_pair(sp.c0, c, o, a0, a1, true, false);
-                                z_pair(sp, c, o, a0, a1);
+                                pair_diffs(sp, c, o, cx, pair_c4, true, false, true, a0, a1);
                             }
-                            adj_weights<T>(a0, w0, 1, ih[1], wv0);
-                            adj_weights<T>(a1, w1, 1, ih[1], wv1);
-#pragma unroll
-                            for (int c = 0; c < 3; ++c)
-                                st_pair(WY + (c * (TT_Y + 4) + (cy - y0 + 2)) * WYC + (cx - x0), wv0[c], wv1[c]);
+                            adj_weights<T>(a0, hw[0], 1, ih[1], wv0);
+                            adj_weights<T>(a1, hw[1], 1, ih[1], wv1);
                         }
-                    }
-                } else {
-                // (b) own voxels: x and y weights of plane m.
+                    } else {
 #pragma unroll
-                for (int v = 0; v < 2; ++v) {
-                    const int xv = x + v;
-                    T wx[3] = {T(0), T(0), T(0)}, wy[3] = {T(0), T(0), T(0)};
-                    if (row_vol && xv < g.nx) {
-                        int ks[3] = {S_C4, S_C4, S_C4};
-                        if (!fast) schemes_at(xv, y, m, g, ks);
-                        const int o = byo * PX + bxo + v;
-                        T a[3][3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-#pragma unroll
-                            for (int ax = 0; ax < 3; ++ax) a[c][ax] = adj_deriv<T, PX, PLANE>(sp, c, o, ax, ks[ax], ih, k1, k2);
-                        const T w = gJ[(long long) m * g.zs + (long long) y * g.ys + xv];
-                        adj_weights<T>(a, w, 0, ih[0], wx);
-                        adj_weights<T>(a, w, 1, ih[1], wy);
+                        for (int v = 0; v < 2; ++v) {
+                            const int xv = cx + v;
+                            if (!(xv >= 0 && xv < g.nx && cy >= 0 && cy < g.ny)) continue;
+                            T a[3][3];
+                            if (xside) {
+                                cell_diffs(sp, xv, cy, m, o + v, false, true, true, a);
+                                adj_weights<T>(a, hw[v], 0, ih[0], v ? wv1 : wv0);
+                            } else {
+                                cell_diffs(sp, xv, cy, m, o + v, true, false, true, a);
+                                adj_weights<T>(a, hw[v], 1, ih[1], v ? wv1 : wv0);
+                            }
+                        }
                     }
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        WX[(c * TT_Y + ty) * WXC + 2 * tx + 2 + v] = wx[c];
-                        WY[(c * (TT_Y + 4) + ty + 2) * WYC + 2 * tx + v] = wy[c];
+                        if (xside)
+                            st_pair(WX + (c * TT_Y + (cy - y0)) * WXC + (cx - x0 + 2), wv0[c], wv1[c]);
+                        else
+                            st_pair(WY + (c * (TT_Y + 4) + (cy - y0 + 2)) * WYC + (cx - x0), wv0[c], wv1[c]);
                     }
                 }
-                // (c) halo cells, two adjacent x cells per task: the x
-                // weights of the two columns each side, the y weights of the
-                // two rows each side.
-                if (h >= 0) {
-                    const bool xside = h < NHX;
-                    int cx, cy;  // first cell of the pair
-                    if (xside) {
-                        cx = (h / TT_Y) ? x0 + TXW : x0 - 2;
-                        cy = y0 + h % TT_Y;
-                    } else {
-                        const int h2 = h - NHX, r = h2 / TPX;
-                        cx = x0 + 2 * (h2 % TPX);
-                        cy = r < 2 ? y0 - 2 + r : y0 + TT_Y - 2 + r;
-                    }
-#pragma unroll
-                    for (int v = 0; v < 2; ++v) {
-                        const int xv = cx + v;
-                        T wv[3] = {T(0), T(0), T(0)};
-                        if (xv >= 0 && xv < g.nx && cy >= 0 && cy < g.ny && m >= 0 && m < g.nz) {
-                            int ks[3] = {S_C4, S_C4, S_C4};
-                            if (!fast) schemes_at(xv, cy, m, g, ks);
-                            const int o = (cy - y0 + 4) * PX + (xv - x0 + 4);
-                            const T w = gJ[(long long) m * g.zs + (long long) cy * g.ys + xv];
-                            T a[3][3];
-                            // The x weights use columns 1 and 2 of I + A, the y weights 0 and 2.
-                            if (xside) {
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) {
-                                    a[c][0] = T(0);
-                                    a[c][1] = adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2);
-                                    a[c][2] = adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2);
-                                }
-                                adj_weights<T>(a, w, 0, ih[0], wv);
-                            } else {
-#pragma unroll
-                                for (int c = 0; c < 3; ++c) {
-                                    a[c][0] = adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2);
-                                    a[c][1] = T(0);
-                                    a[c][2] = adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2);
-                                }
-                                adj_weights<T>(a, w, 1, ih[1], wv);
-                            }
-                        }
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            if (xside)
-                                WX[(c * TT_Y + (cy - y0)) * WXC + (xv - x0 + 2)] = wv[c];
-                            else
-                                WY[(c * (TT_Y + 4) + (cy - y0 + 2)) * WYC + (xv - x0)] = wv[c];
-                        }
-                    }
-                }
-                }  // generic path
             }
             __syncthreads();
             if (s_fault) {
@@ -2319,10 +2332,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
             // Iteration it - 4's stage (plane m - 2) is not read again.
             if (tid == 0 && it >= 4 && it + 3 < n_it) issue(it + 3);
             // (d) gradient of the own voxels at plane m.
-            const bool deep = tile_deep && m >= 4 && m <= g.nz - 5;
-            if (centre && deep) {
-                // Every tap of the tile is fourth order: constant weights,
-                // the general path's tap and summation order.
+            if (!centre || !row_vol) continue;
+            if (cols_deep && warp_rows_deep && m >= 4 && m <= g.nz - 5) {
+                // Every tap is fourth order: constant weights, the general
+                // path's tap and summation order.
                 T acc0[3] = {T(0), T(0), T(0)}, acc1[3] = {T(0), T(0), T(0)};
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
@@ -2359,56 +2372,50 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                     gout[c * g.cs + off] = acc0[c];
                     gout[c * g.cs + off + 1] = acc1[c];
                 }
-            } else if (centre && row_vol) {
+                continue;
+            }
+            // Taps with their schemes (the two-pass gather's general path),
+            // out-of-volume and zero-weight taps predicated off.
 #pragma unroll
-                for (int v = 0; v < 2; ++v) {
-                    const int xv = x + v;
-                    if (xv >= g.nx) continue;
-                    T acc[3] = {T(0), T(0), T(0)};
-                    const int q[3] = {xv, y, m};
-                    bool ob[3], pb[3];
+            for (int v = 0; v < 2; ++v) {
+                const int xv = x + v;
+                if (xv >= g.nx) continue;
+                T acc[3] = {T(0), T(0), T(0)};
+                const int q[3] = {xv, y, m};
+                bool ob[3], pb[3];
 #pragma unroll
-                    for (int bb = 0; bb < 3; ++bb) {
-                        ob[bb] = q[bb] == 0 || q[bb] == n[bb] - 1;
-                        pb[bb] = q[bb] == 1 || q[bb] == n[bb] - 2;
-                    }
+                for (int bb = 0; bb < 3; ++bb) {
+                    ob[bb] = q[bb] == 0 || q[bb] == n[bb] - 1;
+                    pb[bb] = q[bb] == 1 || q[bb] == n[bb] - 2;
+                }
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
-                        const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
+                for (int a = 0; a < 3; ++a) {
+                    const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
+                    const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
 #pragma unroll
-                        for (int t = -2; t <= 2; ++t) {
-                            T kp;
-                            if (deep) {
-                                if (t == 0) continue;
-                                kp = kappa<T>(S_C4, t);
-                            } else {
-                                const int pa = q[a] - t;
-                                if (pa < 0 || pa >= n[a]) continue;
-                                const bool outer = o_other || pa == 0 || pa == n[a] - 1;
-                                const bool pen = p_other || pa == 1 || pa == n[a] - 2;
-                                const int kk = outer ? (pa == 0 ? S_FWD : (pa == n[a] - 1 ? S_BWD : S_C2))
-                                                     : ((g.order == 2 || pen) ? S_C2 : S_C4);
-                                kp = kappa<T>(kk, t);
-                                if (kp == T(0)) continue;
-                            }
+                    for (int t = -2; t <= 2; ++t) {
+                        const int pa = q[a] - t;
+                        const bool outer = o_other || pa == 0 || pa == n[a] - 1;
+                        const bool pen = p_other || pa == 1 || pa == n[a] - 2;
+                        const int kk = outer ? (pa == 0 ? S_FWD : (pa == n[a] - 1 ? S_BWD : S_C2))
+                                             : ((g.order == 2 || pen) ? S_C2 : S_C4);
+                        const T kp = (pa >= 0 && pa < n[a]) ? kappa<T>(kk, t) : T(0);
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) {
-                                T wt;
-                                if (a == 0)
-                                    wt = WX[(c * TT_Y + ty) * WXC + 2 * tx + v - t + 2];
-                                else if (a == 1)
-                                    wt = WY[(c * (TT_Y + 4) + ty - t + 2) * WYC + 2 * tx + v];
-                                else
-                                    wt = zw[v][c][2 - t];
-                                acc[c] += wt * kp;
-                            }
+                        for (int c = 0; c < 3; ++c) {
+                            T wt;
+                            if (a == 0)
+                                wt = WX[(c * TT_Y + ty) * WXC + 2 * tx + v - t + 2];
+                            else if (a == 1)
+                                wt = WY[(c * (TT_Y + 4) + ty - t + 2) * WYC + 2 * tx + v];
+                            else
+                                wt = zw[v][c][2 - t];
+                            if (kp != T(0)) acc[c] += wt * kp;
                         }
                     }
-                    const long long off = (long long) m * g.zs + (long long) y * g.ys + xv;
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) gout[c * g.cs + off] = acc[c];
                 }
+                const long long off = (long long) m * g.zs + (long long) y * g.ys + xv;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) gout[c * g.cs + off] = acc[c];
             }
         }
         if (failed) {

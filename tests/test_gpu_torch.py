@@ -144,8 +144,8 @@ def test_batched_fp32_autograd_config3():
 @pytest.mark.parametrize("shape", [(3, 3, 4), (5, 9, 12), (7, 17, 36), (40, 40, 96), (37, 21, 100),
                                    (30, 53, 132)])
 def test_fused_adjoint_equals_two_pass(monkeypatch, dtype, shape):
-    """The fused adjoint kernel (one launch, weights on chip) against the
-    weight pass + gather (DISPTOOLS_B200_ADJOINT=two-pass): bit for bit in
+    """The fused adjoint kernel (one launch, weights on chip,
+    DISPTOOLS_B200_ADJOINT=fused) against the weight pass + gather: bit for bit in
     FP64, to float rounding in FP32.  The shapes give partial tiles on every
     axis, volumes of 3 voxels, and (40 x 40 x 96) tiles whose every voxel is
     four cells from the faces (the constant-weight path)."""
@@ -158,11 +158,12 @@ def test_fused_adjoint_equals_two_pass(monkeypatch, dtype, shape):
     f = torch.from_numpy(smooth_field(shape, sigma=2.0, max_disp=0.8, seed=3)).to(t).cuda()
     w = torch.from_numpy(np.random.default_rng(4).standard_normal(shape)).to(t).cuda()
     sp = (0.9, 1.1, 1.3)
+    monkeypatch.setenv("DISPTOOLS_B200_ADJOINT", "fused")
     n0 = dt.kernel_launch_count()
     fused = torch_ops.jacobian_adjoint_raw(f, w, sp)
     torch.cuda.synchronize()
     assert dt.kernel_launch_count() - n0 == 1  # one kernel: the fused path ran
-    monkeypatch.setenv("DISPTOOLS_B200_ADJOINT", "two-pass")
+    monkeypatch.delenv("DISPTOOLS_B200_ADJOINT")
     n0 = dt.kernel_launch_count()
     two = torch_ops.jacobian_adjoint_raw(f, w, sp)
     torch.cuda.synchronize()
