@@ -239,7 +239,10 @@ def test_full_size_256_converged_mixed_within_1e4_of_reference(oracle):
     out64, st64 = dt.solve(Jt, mask, precision="fp64", it_max=50000)
     r64 = masked_max(oracle.jacobian(out64), Jt, mask)
     assert abs(r64 - ref["masked_max"]) <= 1e-9, (r64, ref["masked_max"], st64)
+    assert st64["iterations"] == ref["iterations"], (st64, ref["iterations"])
+    # both stop by the improvement rule ("Error not decreasing, terminating.")
     assert st64["reason"] == st32["reason"] == "improvement < theta"
+    assert ref["stop_line"] == "Error not decreasing, terminating."
 
 
 def test_full_size_256_mixed_properties(oracle):
