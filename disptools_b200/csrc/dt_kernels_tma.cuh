@@ -1149,6 +1149,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     __shared__ int s_drop;                  // iteration whose loads are dropped (failure-path test), or -1
     __shared__ int s_done, s_phase, s_old;
     __shared__ double s_eta;
+    // Per-tile constants read outside the voxel arithmetic (kept out of the
+    // registers, which the plane loop needs): inverse spacing, the wait bound.
+    __shared__ T s_ih[3];
+    __shared__ unsigned s_wait;
     for (int tile = take_tile<TPX>(queue, total_tiles, &s_tile); tile >= 0;
          tile = take_tile<TPX>(queue, total_tiles, &s_tile)) {
         const VolumeDesc<T> &V = vols[tile_vol[tile]];
@@ -1176,6 +1180,8 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             s_box[3] = z1;
             s_drop = (s_phase != PH_EVAL0 && tile == V.drop_tile) ? V.drop_it : -1;
             s_issued = 0;
+            for (int a = 0; a < 3; ++a) s_ih[a] = (T) g.ih[a];
+            s_wait = V.wait_limit ? V.wait_limit : (1u << 22);
         }
         __syncthreads();
         if (s_done) continue;
@@ -1183,14 +1189,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const int old_b = s_old;
         const double eta = s_eta;
         const bool trial = phase != PH_EVAL0;
-        T *dst = V.field[old_b ^ 1];
-        T *ep_out = V.ep[trial ? old_b ^ 1 : old_b];  // e' of the evaluated field
         // The launch that evaluates the initial field takes it as it is:
         // eta 0 over the gradient buffer, which the set-up zeroed.
         const T eta_t = trial ? (T) eta : T(0);
-        const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
         const T tol = (T) st->tolerance, delta = (T) st->delta, zeta = (T) st->zeta;
-        const unsigned wait_limit = V.wait_limit ? V.wait_limit : (1u << 22);
 
         // Issues the loads of iteration j (plane z0-2+j) into its slot (one
         // thread; the tile's parameters come from shared memory).
@@ -1246,11 +1248,15 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                     for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
         double acc_s = 0.0;
         T acc_mt = T(0);
-        long long qoff = (long long) (z0 - 2) * g.zs;  // offset of plane q
-        for (int it = 0; it < n_it; ++it, qoff += g.zs) {
+        // Running pointers at the thread's first row: the candidate of plane
+        // q in the other field buffer, e' of plane q - 2.
+        const long long row0 = (long long) (y0 + ty) * g.ys + x;
+        T *dq = V.field[old_b ^ 1] + (long long) (z0 - 2) * g.zs + row0;
+        T *eq = V.ep[trial ? old_b ^ 1 : old_b] + (long long) (z0 - 4) * g.zs + row0;  // e' of the evaluated field
+        for (int it = 0; it < n_it; ++it, dq += g.zs, eq += g.zs) {
             if (s_fault) break;
             const uint32_t k = kbase + it;
-            if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u, wait_limit)) {
+            if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u, s_wait)) {
                 s_fault = 1;
                 break;
             }
@@ -1274,7 +1280,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 }
                 const int y = y0 + ty + r * TYT;
                 if (trial && x < g.nx && y < g.ny && q >= z0 && q < z1) {
-                    T *o = dst + qoff + (long long) y * g.ys + x;
+                    T *o = dq + (long long) (r * TYT) * g.ys;
                     if (pair_in) {
 #pragma unroll
                         for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, zq[r][0][c][4], zq[r][1][c][4]);
@@ -1292,6 +1298,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 const bool plane_in = ze >= 2 && ze <= g.nz - 3;
                 // Fourth-order weights with the spacing folded in (FP32); the
                 // FP64 path keeps the reference's operation order.
+                const T ih[3] = {s_ih[0], s_ih[1], s_ih[2]};
                 const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
                 const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1],
                                  FD<T>::one_twelfth * ih[2]};
@@ -1424,7 +1431,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                             finish(v, a);
                         }
                     }
-                    T *o = ep_out + (qoff - 2 * g.zs) + (long long) y * g.ys + x;
+                    T *o = eq + (long long) (r * TYT) * g.ys;
                     if (pair_in)
                         st_pair(o, epv[0], epv[1]);
                     else
