@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-greedy", action="store_true")
+    p.add_argument("--no-other-configs", action="store_true",
+                   help="skip the short runs of configs 3, 4 and 5 that the default line carries")
     p.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "greedy"],
                    help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
                         "axes U{48..192} split over the ranks; c5: one 512x512x384 volume per "
@@ -303,7 +305,7 @@ def run_reference_c3(args):
     }))
 
 
-def run_c4(args, world, rank, local):
+def run_c4(args, world, rank, local, quiet=False):
     """Config 4: 64 independent volumes (axes U{48..192}, 1-4 ellipsoids
     each), FP32 fields.  The volumes are split over the ranks by voxel count
     (disptools_b200.sharding.assign_volumes) and each rank solves its share
@@ -381,25 +383,27 @@ def run_c4(args, world, rank, local):
                "steps": ke, "path": "disptools_b200.solve_batched(inplace=True) (C ABI, host float64 "
                                      "arrays in pinned memory)"}
 
-    if rank == 0:
-        print(json.dumps({
-            "metric": "batched gradient-descent voxel-iters/s, 64 volumes (config 4)",
-            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"config 4: 64 volumes, axes U{{48..192}}, 1-4 ellipsoids, "
-                                   f"FP32 fields, it_max={IT} per step",
-                       "voxels": total_vox, "volumes": len(sizes),
-                       "l2": "inputs larger than L2 (fields of all volumes 1.5 GB)",
-                       "iterations_per_step_rank0": iters / args.steps,
-                       "trials_per_iteration_rank0": trials / max(iters, 1),
-                       "parallelism": f"volumes split over {world} ranks by voxel count",
-                       "tiles": tiles},
-            "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-        }))
+    line = {
+        "metric": "batched gradient-descent voxel-iters/s, 64 volumes (config 4)",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"config 4: 64 volumes, axes U{{48..192}}, 1-4 ellipsoids, "
+                               f"FP32 fields, it_max={IT} per step",
+                   "voxels": total_vox, "volumes": len(sizes),
+                   "l2": "inputs larger than L2 (fields of all volumes 1.5 GB)",
+                   "iterations_per_step_rank0": iters / args.steps,
+                   "trials_per_iteration_rank0": trials / max(iters, 1),
+                   "parallelism": f"volumes split over {world} ranks by voxel count",
+                   "tiles": tiles},
+        "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+}
+    if rank == 0 and not quiet:
+        print(json.dumps(line))
+    return line
 
 
-def run_c5(args, world, rank, local):
+def run_c5(args, world, rank, local, quiet=False):
     """Config 5: a 512x512x384 volume (64 blobs as in config 2) per rank,
     FP32 fields.  One step = the 3-level pyramid of the gradient method
     (disptools_b200.pyramid.displacement, it_max per level = --it-max) on
@@ -457,24 +461,26 @@ def run_c5(args, world, rank, local):
     ms = max_over_ranks(world, e0.elapsed_time(e1))
     launches = dt.kernel_launch_count() - launches0
     value = sum_over_ranks(world, vi) / (ms / 1000.0)
-    if rank == 0:
-        print(json.dumps({
-            "metric": "pyramid gradient-descent voxel-iters/s, 512x512x384 (config 5)",
-            "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"config 5: 512x512x384, 64 Gaussian blobs, 3-level pyramid "
-                                   f"(gradient, it_max={IT} per level) + greedy on the coarsest "
-                                   f"level (it_max={IT}), FP32 fields",
-                       "level_sizes_padded": [list(s) for s in sizes],
-                       "iterations_per_solve": its,
-                       "l2": "inputs larger than L2 (finest field 1.2 GB)",
-                       "parallelism": f"{world} independent volumes"},
-            "gpu_launches": launches, "clocks": clk.summary(),
-        }))
+    line = {
+        "metric": "pyramid gradient-descent voxel-iters/s, 512x512x384 (config 5)",
+        "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"config 5: 512x512x384, 64 Gaussian blobs, 3-level pyramid "
+                               f"(gradient, it_max={IT} per level) + greedy on the coarsest "
+                               f"level (it_max={IT}), FP32 fields",
+                   "level_sizes_padded": [list(s) for s in sizes],
+                   "iterations_per_solve": its,
+                   "l2": "inputs larger than L2 (finest field 1.2 GB)",
+                   "parallelism": f"{world} independent volumes"},
+        "gpu_launches": launches, "clocks": clk.summary(),
+}
+    if rank == 0 and not quiet:
+        print(json.dumps(line))
+    return line
 
 
-def run_c3(args, world, rank, local):
+def run_c3(args, world, rank, local, quiet=False):
     """Config 3: the differentiable Jacobian on a batch of 4 FP32 fields of
     192x224x192 per rank (smooth random fields, max |u| = 3).  One step = the
     forward map and the backward adjoint of torch_ops.jacobian for the batch.
@@ -559,25 +565,27 @@ def run_c3(args, world, rank, local):
         cpu = {"value": np.prod(shape) / t, "unit": "voxels/s (forward map only)",
                "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": kind,
                "sample": f"one {shape} field, reference jacobian_dynamic (FP64, OpenMP): {t:.3f} s"}
-    if rank == 0:
-        print(json.dumps({
-            "metric": "differentiable jacobian() forward + backward voxels/s, 4 x 192x224x192 FP32 (config 3)",
-            "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "config 3: torch_ops.jacobian forward + backward on 4 FP32 fields of "
-                                   "192x224x192 (Gaussian-filtered noise, sigma 6, max |u| = 3)",
-                       "forward_ms": fwd_ms, "backward_ms": bwd_ms,
-                       "l2": "inputs larger than L2 (fields 397 MB)",
-                       "parallelism": f"{world} independent batches"},
-            "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma", "achieved": achieved, "peak": hbm,
-                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                         "peak_source": peak_kind, "bytes_per_voxel": 16,
-                         "bytes_per_launch": 16 * nvox // B, "avg_launch_ms": fwd_ms / B},
-            "cpu_baseline": cpu,
-            "e2e": None,
-            "gpu_launches": launches, "clocks": clk.summary(),
-        }))
+    line = {
+        "metric": "differentiable jacobian() forward + backward voxels/s, 4 x 192x224x192 FP32 (config 3)",
+        "value": value, "unit": "voxels/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config 3: torch_ops.jacobian forward + backward on 4 FP32 fields of "
+                               "192x224x192 (Gaussian-filtered noise, sigma 6, max |u| = 3)",
+                   "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                   "l2": "inputs larger than L2 (fields 397 MB)",
+                   "parallelism": f"{world} independent batches"},
+        "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma", "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                     "peak_source": peak_kind, "bytes_per_voxel": 16,
+                     "bytes_per_launch": 16 * nvox // B, "avg_launch_ms": fwd_ms / B},
+        "cpu_baseline": cpu,
+        "e2e": None,
+        "gpu_launches": launches, "clocks": clk.summary(),
+}
+    if rank == 0 and not quiet:
+        print(json.dumps(line))
+    return line
 
 
 def greedy_leg(dt, torch_ops, torch, Jt, mask, field, stream, IT, nvox, world):
@@ -861,6 +869,22 @@ def main():
                 "oracle": "reference C library FP64, default parameters, it_max 50000 "
                           "(tests/golden/config2_converged.json)"}
 
+    # ---- short runs of configs 3, 4 and 5 (two timed steps each), so the
+    # default line carries a number for every configuration.
+    other = None
+    if world == 1 and algorithm == "gradient" and n == 256 and not args.no_other_configs:
+        sub = argparse.Namespace(**{**vars(args), "steps": 2, "warmup": 1, "no_e2e": True,
+                                    "no_cpu_baseline": True})
+        other = {}
+        for name, fn in (("c3", run_c3), ("c4", run_c4), ("c5", run_c5)):
+            line = fn(sub, world, rank, local, quiet=True)
+            other[name] = {k: line.get(k) for k in ("metric", "value", "unit", "ms_per_step", "steps", "warmup",
+                                                    "roofline", "gpu_launches", "clocks")}
+            other[name]["workload"] = line["config"]["workload"]
+            if name == "c3":
+                other[name]["forward_ms"] = line["config"]["forward_ms"]
+                other[name]["backward_ms"] = line["config"]["backward_ms"]
+
     if rank == 0:
         out = {
             "metric": METRIC_GREEDY if algorithm == "greedy" else METRIC, "value": value, "unit": UNIT,
@@ -891,6 +915,7 @@ def main():
             "fp64_plain": fp64,
             "accuracy": accuracy,
             "greedy": greedy,
+            "other_configs": other,
         }
         print(json.dumps(out))
     if world > 1:
