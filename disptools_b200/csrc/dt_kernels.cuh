@@ -62,6 +62,60 @@ __device__ __forceinline__ T det_i_plus(const T a[3][3]) {
            a13 * (a21 * a32 - a22 * a31);
 }
 
+// ------------------------------------------------------------------------
+// FP32 pairs.  sm_100 executes add, sub, mul and fma on the two FP32 halves
+// of a 64-bit register pair as one instruction; each half rounds as the
+// scalar operation does.  The FP32 stencils below state every rounding
+// (no contraction left to the compiler), so the scalar and the paired forms
+// give the same bits for a voxel, whichever evaluator a tile takes.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p_sub(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(d)
+        : "l"(*reinterpret_cast<const unsigned long long *>(&a)),
+          "l"(*reinterpret_cast<const unsigned long long *>(&b)));
+    return *reinterpret_cast<const float2 *>(&d);
+}
+__device__ __forceinline__ float2 p_splat(float a) { return make_float2(a, a); }
+
+// Fourth-order central difference of FP32 values with the spacing folded
+// into the weights, k1 = 2/3 ih and k2n = -1/12 ih:
+// (p1 - m1) k1 + (p2 - m2) k2n, one product and one fused multiply-add.
+__device__ __forceinline__ float c4_folded(float p1, float m1, float p2, float m2, float k1, float k2n) {
+    return __fmaf_rn(__fsub_rn(p1, m1), k1, __fmul_rn(__fsub_rn(p2, m2), k2n));
+}
+__device__ __forceinline__ float2 c4_folded2(float2 p1, float2 m1, float2 p2, float2 m2, float2 k1, float2 k2n) {
+    return p_fma(p_sub(p1, m1), k1, p_mul(p_sub(p2, m2), k2n));
+}
+// The same with the first difference already formed.
+__device__ __forceinline__ float2 c4_folded2d(float2 d1, float2 p2, float2 m2, float2 k1, float2 k2n) {
+    return p_fma(d1, k1, p_mul(p_sub(p2, m2), k2n));
+}
+
+// det(I + a) in FP32, the expansion above with each rounding stated: the
+// three minors as differences of products, then a11 c1 - a12 c2 and the
+// last term fused.
+template <>
+__device__ __forceinline__ float det_i_plus<float>(const float a[3][3]) {
+    const float a11 = __fadd_rn(a[0][0], 1.f), a22 = __fadd_rn(a[1][1], 1.f), a33 = __fadd_rn(a[2][2], 1.f);
+    const float c1 = __fsub_rn(__fmul_rn(a22, a33), __fmul_rn(a[1][2], a[2][1]));
+    const float c2 = __fsub_rn(__fmul_rn(a[1][0], a33), __fmul_rn(a[1][2], a[2][0]));
+    const float c3 = __fsub_rn(__fmul_rn(a[1][0], a[2][1]), __fmul_rn(a22, a[2][0]));
+    return __fmaf_rn(a[0][2], c3, __fsub_rn(__fmul_rn(a11, c1), __fmul_rn(a[0][1], c2)));
+}
+__device__ __forceinline__ float2 det_i_plus2(const float2 a[3][3]) {
+    const float2 one = p_splat(1.f);
+    const float2 a11 = p_add(a[0][0], one), a22 = p_add(a[1][1], one), a33 = p_add(a[2][2], one);
+    const float2 c1 = p_sub(p_mul(a22, a33), p_mul(a[1][2], a[2][1]));
+    const float2 c2 = p_sub(p_mul(a[1][0], a33), p_mul(a[1][2], a[2][0]));
+    const float2 c3 = p_sub(p_mul(a[1][0], a[2][1]), p_mul(a22, a[2][0]));
+    return p_fma(a[0][2], c3, p_sub(p_mul(a11, c1), p_mul(a[0][1], c2)));
+}
+
 // Scheme along each axis at voxel (x, y, z): the case analysis of
 // src/jacobian.c:70-242 stated per voxel.  Outer layer: one-sided along the
 // axes where the voxel is at 0 / n-1, central second order along the others.

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "dt_kernels.cuh"
 #include "dt_tma.cuh"
@@ -292,17 +293,41 @@ __device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, 
 //   voxel without branching;
 // * rows or planes on the two outer layers take the general path.
 // The trial kernel keeps the same evaluator inline: calling this function
-// there changes its register allocation (it then spills).
-template <typename T, int TMA_PX, int TMA_PLANE, typename F>
+// there changes its register allocation (it then spills).  In FP32, a
+// `finish2` functor (not null) takes the first evaluator's two matrices at
+// once, as pairs (x, x + 1) of each entry.
+template <typename T, int TMA_PX, int TMA_PLANE, typename F, typename F2 = std::nullptr_t>
 __device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5], int lx, int ly, int x, int y,
                                              int ze, const Geom &g, const T (&ih)[3], bool row_in,
-                                             bool tile_x_in, F &&finish) {
+                                             bool tile_x_in, F &&finish, F2 &&finish2 = nullptr) {
     const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
-    const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1], FD<T>::one_twelfth * ih[2]};
+    const T k2n[3] = {-FD<T>::one_twelfth * ih[0], -FD<T>::one_twelfth * ih[1], -FD<T>::one_twelfth * ih[2]};
     auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
-        if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+        if constexpr (sizeof(T) == 4) return c4_folded(p1, m1, p2, m2, k1[ax], k2n[ax]);
         return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
     };
+    constexpr bool PAIRED = sizeof(T) == 4 && !std::is_same<typename std::decay<F2>::type, std::nullptr_t>::value;
+    if constexpr (PAIRED) {
+        if (row_in && tile_x_in) {
+            float2 a[3][3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+                const float2 xm = ld_pair(p - 2), xc = ld_pair(p), xp = ld_pair(p + 2);
+                const float2 dx1 = make_float2(__fsub_rn(xc.y, xm.y), __fsub_rn(xp.x, xc.x));
+                a[c][0] = c4_folded2d(dx1, xp, xm, p_splat(k1[0]), p_splat(k2n[0]));
+                const float2 ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
+                const float2 ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
+                a[c][1] = c4_folded2(yp1, ym1, yp2, ym2, p_splat(k1[1]), p_splat(k2n[1]));
+                const T *z0q = zq[0][c], *z1q = zq[1][c];
+                a[c][2] = c4_folded2(make_float2(z0q[3], z1q[3]), make_float2(z0q[1], z1q[1]),
+                                     make_float2(z0q[4], z1q[4]), make_float2(z0q[0], z1q[0]), p_splat(k1[2]),
+                                     p_splat(k2n[2]));
+            }
+            finish2(a);
+            return;
+        }
+    }
     if (row_in && tile_x_in) {
         T a0[3][3], a1[3][3];
 #pragma unroll
@@ -500,16 +525,16 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const int x = x0 + 2 * tx;     // this thread's columns: x, x + 1
         const int lx = 2 * tx + TMA_HX;  // their box column
         const bool pair_in = x + 1 < g.nx;
-        // Own columns: candidate values of planes q-4 .. q (z differences).
-        T zq[RYT][2][3][5];
+        // Own columns: candidate values of planes q-4 .. q (z differences),
+        // one pair (x, x + 1) per row, component and plane.
+        using P2 = typename PairOf<T>::type;
+        P2 zq[RYT][3][5];
 #pragma unroll
         for (int r = 0; r < RYT; ++r)
 #pragma unroll
-            for (int v = 0; v < 2; ++v)
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
+                for (int k = 0; k < 5; ++k) zq[r][c][k] = P2{T(0), T(0)};
         double acc_s = 0.0;
         T acc_mt = T(0);
         bool failed = false;
@@ -594,24 +619,19 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 const int ly = ty + r * TYT + TMA_HY;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const auto nv = ld_pair(slot + c * TMA_PLANE + ly * TMA_PX + lx);
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) {
-                        zq[r][0][c][kk] = zq[r][0][c][kk + 1];
-                        zq[r][1][c][kk] = zq[r][1][c][kk + 1];
-                    }
-                    zq[r][0][c][4] = nv.x;
-                    zq[r][1][c][4] = nv.y;
+                    for (int kk = 0; kk < 4; ++kk) zq[r][c][kk] = zq[r][c][kk + 1];
+                    zq[r][c][4] = ld_pair(slot + c * TMA_PLANE + ly * TMA_PX + lx);
                 }
                 const int y = y0 + ty + r * TYT;
                 if (trial && x < g.nx && y < g.ny && q >= z0 && q < z1) {
                     T *o = dst + qoff + (long long) y * g.ys + x;
                     if (pair_in) {
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, zq[r][0][c][4], zq[r][1][c][4]);
+                        for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, zq[r][c][4].x, zq[r][c][4].y);
                     } else {
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) o[c * g.cs] = zq[r][0][c][4];
+                        for (int c = 0; c < 3; ++c) o[c * g.cs] = zq[r][c][4].x;
                     }
                 }
             }
@@ -620,11 +640,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 // Fourth-order weights with the spacing folded in (FP32); the
                 // FP64 path keeps the reference's operation order.
                 const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
-                const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1],
-                                 FD<T>::one_twelfth * ih[2]};
+                const T k2n[3] = {-FD<T>::one_twelfth * ih[0], -FD<T>::one_twelfth * ih[1],
+                                  -FD<T>::one_twelfth * ih[2]};
                 auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
-                    if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
-                    return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
+                    if constexpr (sizeof(T) == 4) return c4_folded(p1, m1, p2, m2, k1[ax], k2n[ax]);
+                    else return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
                 };
                 // Three evaluators: rows and planes inside [2, n-3] of a tile
                 // whose columns all lie inside [2, nx-3] use the fourth-order
@@ -640,9 +660,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                     const int ly = ty + r * TYT + TMA_HY;
                     if (x >= g.nx || y >= g.ny) continue;
                     T epv[2];
-                    // Error terms of voxel v from its Jacobian matrix minus I.
-                    auto finish = [&](int v, const T (&a)[3][3]) {
-                        const T J = det_i_plus<T>(a);
+                    // Error terms of voxel v from its Jacobian (finish_j) or
+                    // its Jacobian matrix minus I (finish).
+                    auto finish_j = [&](int v, const T J) {
                         const T vv = voxel_error<T>(J, jt[r][v], msk[r][v], tol);
                         acc_s += (double) vv * (double) vv;
                         const T av = fabs(vv);  // the maximum is exact in the element type
@@ -651,24 +671,44 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                         if (!GREEDY && J < delta) ep += zeta * (J - delta);  // src/displacement_field_gradient.c:71-88
                         epv[v] = ep;
                     };
+                    auto finish = [&](int v, const T (&a)[3][3]) { finish_j(v, det_i_plus<T>(a)); };
                     if (row_in && tile_x_in) {
-                        T a0[3][3], a1[3][3];
+                        if constexpr (sizeof(T) == 4) {
+                            // Both voxels at once, as FP32 pairs.
+                            float2 a[3][3];
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
-                            const auto xm = ld_pair(p - 2), xc = ld_pair(p), xp = ld_pair(p + 2);
-                            a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
-                            a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
-                            const auto ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
-                            const auto ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
-                            a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
-                            a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
-                            const T *z0q = zq[r][0][c], *z1q = zq[r][1][c];
-                            a0[c][2] = c4(z0q[3], z0q[1], z0q[4], z0q[0], 2);
-                            a1[c][2] = c4(z1q[3], z1q[1], z1q[4], z1q[0], 2);
+                            for (int c = 0; c < 3; ++c) {
+                                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+                                const float2 xm = ld_pair(p - 2), xc = ld_pair(p), xp = ld_pair(p + 2);
+                                const float2 dx1 = make_float2(__fsub_rn(xc.y, xm.y), __fsub_rn(xp.x, xc.x));
+                                a[c][0] = c4_folded2d(dx1, xp, xm, p_splat(k1[0]), p_splat(k2n[0]));
+                                const float2 ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
+                                const float2 ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
+                                a[c][1] = c4_folded2(yp1, ym1, yp2, ym2, p_splat(k1[1]), p_splat(k2n[1]));
+                                a[c][2] = c4_folded2(zq[r][c][3], zq[r][c][1], zq[r][c][4], zq[r][c][0],
+                                                     p_splat(k1[2]), p_splat(k2n[2]));
+                            }
+                            const float2 J2 = det_i_plus2(a);
+                            finish_j(0, J2.x);
+                            finish_j(1, J2.y);
+                        } else {
+                            T a0[3][3], a1[3][3];
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx;
+                                const auto xm = ld_pair(p - 2), xc = ld_pair(p), xp = ld_pair(p + 2);
+                                a0[c][0] = c4(xc.y, xm.y, xp.x, xm.x, 0);
+                                a1[c][0] = c4(xp.x, xc.x, xp.y, xm.y, 0);
+                                const auto ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
+                                const auto ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
+                                a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
+                                a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
+                                a0[c][2] = c4(zq[r][c][3].x, zq[r][c][1].x, zq[r][c][4].x, zq[r][c][0].x, 2);
+                                a1[c][2] = c4(zq[r][c][3].y, zq[r][c][1].y, zq[r][c][4].y, zq[r][c][0].y, 2);
+                            }
+                            finish(0, a0);
+                            finish(1, a1);
                         }
-                        finish(0, a0);
-                        finish(1, a1);
                     } else if (row_in) {
                         // Interior row: the scheme depends on x only
                         // (src/jacobian.c:113-241): outer column -> one-sided
@@ -692,7 +732,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                                 const T cy4 = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
                                 const T cy2 = fd_c2<T>(p[TMA_PX], p[-TMA_PX], ih[1]);
                                 a[c][1] = second ? cy2 : cy4;
-                                const T *zv = zq[r][v][c];
+                                T zv[5];
+#pragma unroll
+                                for (int k = 0; k < 5; ++k) zv[k] = v ? zq[r][c][k].y : zq[r][c][k].x;
                                 const T cz4 = c4(zv[3], zv[1], zv[4], zv[0], 2);
                                 const T cz2 = fd_c2<T>(zv[3], zv[1], ih[2]);
                                 a[c][2] = second ? cz2 : cz4;
@@ -712,9 +754,12 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                                 const T *p = jp + c * TMA_PLANE + ly * TMA_PX + lx + v;
                                 const T vx[5] = {p[-2], p[-1], p[0], p[1], p[2]};
                                 const T vy[5] = {p[-2 * TMA_PX], p[-TMA_PX], p[0], p[TMA_PX], p[2 * TMA_PX]};
+                                T vz[5];
+#pragma unroll
+                                for (int k = 0; k < 5; ++k) vz[k] = v ? zq[r][c][k].y : zq[r][c][k].x;
 #pragma unroll
                                 for (int ax = 0; ax < 3; ++ax) {
-                                    const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[r][v][c]);
+                                    const T *w = ax == 0 ? vx : (ax == 1 ? vy : vz);
                                     T d;
                                     switch (kk[ax]) {
                                     case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
@@ -858,14 +903,14 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const int x = x0 + 2 * tx;       // this thread's columns: x, x + 1
         const int lx = 2 * tx + TMA_HX;  // their box column
         const int cp = 2 * tx + 2;       // their P column
-        // P_z terms of the own cells: planes p-2, p-1 and the one computed now.
-        T pz_m2[RYT][2][3], pz_m1[RYT][2][3];
+        // P_z terms of the own cells (x, x + 1 as one pair): planes p-2, p-1
+        // and the one computed now.
+        using P2 = typename PairOf<T>::type;
+        P2 pz_m2[RYT][3], pz_m1[RYT][3];
 #pragma unroll
         for (int r = 0; r < RYT; ++r)
 #pragma unroll
-            for (int v = 0; v < 2; ++v)
-#pragma unroll
-                for (int i = 0; i < 3; ++i) pz_m2[r][v][i] = pz_m1[r][v][i] = T(0);
+            for (int i = 0; i < 3; ++i) pz_m2[r][i] = pz_m1[r][i] = P2{T(0), T(0)};
         double acc = 0.0;
         bool failed = false;
         int fail_it = 0;
@@ -878,31 +923,44 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             if (!ok) s_fault = 1;
             const int q = z0 - 2 + it;
             const int p = q - 1;  // plane of P computed now (needs u(q-2..q), e'(q-1))
-            T pz_new[RYT][2][3];
+            P2 pz_new[RYT][3];
 #pragma unroll
             for (int r = 0; r < RYT; ++r)
 #pragma unroll
-                for (int v = 0; v < 2; ++v)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) pz_new[r][v][i] = T(0);
+                for (int i = 0; i < 3; ++i) pz_new[r][i] = P2{T(0), T(0)};
             if (it >= 2 && ok) {
                 const T *um = stage_u(it - 2), *u0 = stage_u(it - 1), *up = stage_u(it);
                 const T *e0 = stage_e(it - 1);
                 const int ps = ring_slot(p, L::NP);
+                // FP32 states every rounding, so the scalar (halo) and the
+                // paired (own) cells give the same bits: a minor is a
+                // difference of two products, a diagonal entry d h + 1 one
+                // fused multiply-add.
                 auto minor = [](const T m[3][3], int i, int kk) -> T {
                     const int r0 = i == 0 ? 1 : 0, r1 = i == 2 ? 1 : 2;
                     const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
-                    return m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
+                    if constexpr (sizeof(T) == 4)
+                        return __fsub_rn(__fmul_rn(m[r0][c0], m[r1][c1]), __fmul_rn(m[r0][c1], m[r1][c0]));
+                    else return m[r0][c0] * m[r1][c1] - m[r0][c1] * m[r1][c0];
                 };
                 // M = I + grad u (second-order central) at box cell (cx, cy).
                 auto mat = [&](int cx, int cy, T m[3][3]) {
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const int o = c * TMA_PLANE + cy * TMA_PX + cx;
-                        m[c][0] = c2(u0[o + 1], u0[o - 1], 0);
-                        m[c][1] = c2(u0[o + TMA_PX], u0[o - TMA_PX], 1);
-                        m[c][2] = c2(up[o], um[o], 2);
-                        m[c][c] += T(1.0);
+                        if constexpr (sizeof(T) == 4) {
+                            const float d[3] = {__fsub_rn(u0[o + 1], u0[o - 1]),
+                                                __fsub_rn(u0[o + TMA_PX], u0[o - TMA_PX]), __fsub_rn(up[o], um[o])};
+                            const float h[3] = {hx, hy, hz};
+#pragma unroll
+                            for (int a = 0; a < 3; ++a)
+                                m[c][a] = a == c ? __fmaf_rn(d[a], h[a], 1.f) : __fmul_rn(d[a], h[a]);
+                        } else {
+                            m[c][0] = c2(u0[o + 1], u0[o - 1], 0);
+                            m[c][1] = c2(u0[o + TMA_PX], u0[o - TMA_PX], 1);
+                            m[c][2] = c2(up[o], um[o], 2);
+                            m[c][c] += T(1.0);
+                        }
                     }
                 };
                 // The same for the pair of box cells (cx, cy), (cx + 1, cy); cx even.
@@ -923,18 +981,56 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                         m1[c][c] += T(1.0);
                     }
                 };
+                // FP32: M of the pair (cx, cy), (cx + 1, cy) as pairs, and
+                // the minors as pairs (the arithmetic of mat and minor).
+                auto mat_pair2 = [&](int cx, int cy, P2 M[3][3]) {
+                    if constexpr (sizeof(T) == 4) {
+                        const float2 h2[3] = {p_splat(hx), p_splat(hy), p_splat(hz)};
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const int o = c * TMA_PLANE + cy * TMA_PX + cx;
+                            const float2 xm = ld_pair(u0 + o - 2), xc = ld_pair(u0 + o), xp = ld_pair(u0 + o + 2);
+                            const float2 ym = ld_pair(u0 + o - TMA_PX), yp = ld_pair(u0 + o + TMA_PX);
+                            const float2 zm = ld_pair(um + o), zp = ld_pair(up + o);
+                            const float2 d[3] = {make_float2(__fsub_rn(xc.y, xm.y), __fsub_rn(xp.x, xc.x)),
+                                                 p_sub(yp, ym), p_sub(zp, zm)};
+#pragma unroll
+                            for (int a = 0; a < 3; ++a)
+                                M[c][a] = a == c ? p_fma(d[a], h2[a], p_splat(1.f)) : p_mul(d[a], h2[a]);
+                        }
+                    }
+                };
+                auto minor2 = [](const P2 M[3][3], int i, int kk) -> P2 {
+                    const int r0 = i == 0 ? 1 : 0, r1 = i == 2 ? 1 : 2;
+                    const int c0 = kk == 0 ? 1 : 0, c1 = kk == 2 ? 1 : 2;
+                    if constexpr (sizeof(T) == 4)
+                        return p_sub(p_mul(M[r0][c0], M[r1][c1]), p_mul(M[r0][c1], M[r1][c0]));
+                    else return P2{};
+                };
+                auto st2 = [](T *p, P2 v) { *reinterpret_cast<P2 *>(p) = v; };
 #pragma unroll
                 for (int r = 0; r < RYT; ++r) {  // own cells: all nine terms (P_z in registers)
                     const int ly = ty + r * TYT + TMA_HY, rp = ty + r * TYT + 1;
-                    T m0[3][3], m1[3][3];
-                    mat_pair(lx, ly, m0, m1);
-                    const auto ep = ld_pair(e0 + ly * TMA_PX + lx);
+                    if constexpr (sizeof(T) == 4) {
+                        float2 M[3][3];
+                        mat_pair2(lx, ly, M);
+                        const float2 ep = ld_pair(e0 + ly * TMA_PX + lx);
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        st_pair(PT(ps, i, rp, cp), ep.x * minor(m0, i, 0), ep.y * minor(m1, i, 0));
-                        st_pair(PT(ps, 3 + i, rp, cp), ep.x * minor(m0, i, 1), ep.y * minor(m1, i, 1));
-                        pz_new[r][0][i] = ep.x * minor(m0, i, 2);
-                        pz_new[r][1][i] = ep.y * minor(m1, i, 2);
+                        for (int i = 0; i < 3; ++i) {
+                            st2(PT(ps, i, rp, cp), p_mul(ep, minor2(M, i, 0)));
+                            st2(PT(ps, 3 + i, rp, cp), p_mul(ep, minor2(M, i, 1)));
+                            pz_new[r][i] = p_mul(ep, minor2(M, i, 2));
+                        }
+                    } else {
+                        T m0[3][3], m1[3][3];
+                        mat_pair(lx, ly, m0, m1);
+                        const auto ep = ld_pair(e0 + ly * TMA_PX + lx);
+#pragma unroll
+                        for (int i = 0; i < 3; ++i) {
+                            st_pair(PT(ps, i, rp, cp), ep.x * minor(m0, i, 0), ep.y * minor(m1, i, 0));
+                            st_pair(PT(ps, 3 + i, rp, cp), ep.x * minor(m0, i, 1), ep.y * minor(m1, i, 1));
+                            pz_new[r][i] = P2{ep.x * minor(m0, i, 2), ep.y * minor(m1, i, 2)};
+                        }
                     }
                 }
                 // Halo cells, on the last threads of the block (thread 0
@@ -949,18 +1045,29 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                     mat(cx, cy, m);
                     const T ep = e0[cy * TMA_PX + cx];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) *PT(ps, i, row + 1, c) = ep * minor(m, i, 0);
+                    for (int i = 0; i < 3; ++i) {
+                        if constexpr (sizeof(T) == 4) *PT(ps, i, row + 1, c) = __fmul_rn(ep, minor(m, i, 0));
+                        else *PT(ps, i, row + 1, c) = ep * minor(m, i, 0);
+                    }
                 } else if (h >= 2 * TT_Y) {
                     const int h2 = h - 2 * TT_Y;
                     const int side = h2 / TPX, col = 2 * (h2 % TPX);
                     const int r = side ? TT_Y + 1 : 0;
                     const int cx = col + TMA_HX, cy = r - 1 + TMA_HY;
-                    T m0[3][3], m1[3][3];
-                    mat_pair(cx, cy, m0, m1);
-                    const auto ep = ld_pair(e0 + cy * TMA_PX + cx);
+                    if constexpr (sizeof(T) == 4) {
+                        float2 M[3][3];
+                        mat_pair2(cx, cy, M);
+                        const float2 ep = ld_pair(e0 + cy * TMA_PX + cx);
 #pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                        st_pair(PT(ps, 3 + i, r, col + 2), ep.x * minor(m0, i, 1), ep.y * minor(m1, i, 1));
+                        for (int i = 0; i < 3; ++i) st2(PT(ps, 3 + i, r, col + 2), p_mul(ep, minor2(M, i, 1)));
+                    } else {
+                        T m0[3][3], m1[3][3];
+                        mat_pair(cx, cy, m0, m1);
+                        const auto ep = ld_pair(e0 + cy * TMA_PX + cx);
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+                            st_pair(PT(ps, 3 + i, r, col + 2), ep.x * minor(m0, i, 1), ep.y * minor(m1, i, 1));
+                    }
                 }
             }
             __syncthreads();
@@ -980,31 +1087,59 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                     if (y < 1 || y >= g.ny - 1) continue;
                     const int rp = ty + r * TYT + 1;
                     T gv[2][3];
-                    T t[2][3][3];
+                    if constexpr (sizeof(T) == 4) {
+                        // Pairs; every rounding stated: t = ih (P(-) - P(+)),
+                        // g = (t_a - t_b) + t_c with the reference's signs.
+                        float2 t[3][3];
 #pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const auto a = ld_pair(PT(ps, i, rp, cp - 2)), b = ld_pair(PT(ps, i, rp, cp)),
-                                   c = ld_pair(PT(ps, i, rp, cp + 2));
-                        t[0][i][0] = ihx * (a.y - b.y);
-                        t[1][i][0] = ihx * (b.x - c.x);
-                        const auto ym = ld_pair(PT(ps, 3 + i, rp - 1, cp)), yp = ld_pair(PT(ps, 3 + i, rp + 1, cp));
-                        t[0][i][1] = ihy * (ym.x - yp.x);
-                        t[1][i][1] = ihy * (ym.y - yp.y);
-                        t[0][i][2] = ihz * (pz_m2[r][0][i] - pz_new[r][0][i]);
-                        t[1][i][2] = ihz * (pz_m2[r][1][i] - pz_new[r][1][i]);
-                    }
+                        for (int i = 0; i < 3; ++i) {
+                            const float2 a = ld_pair(PT(ps, i, rp, cp - 2)), b = ld_pair(PT(ps, i, rp, cp)),
+                                         c = ld_pair(PT(ps, i, rp, cp + 2));
+                            t[i][0] = p_mul(p_splat(ihx), make_float2(__fsub_rn(a.y, b.y), __fsub_rn(b.x, c.x)));
+                            const float2 ym = ld_pair(PT(ps, 3 + i, rp - 1, cp)),
+                                         yp = ld_pair(PT(ps, 3 + i, rp + 1, cp));
+                            t[i][1] = p_mul(p_splat(ihy), p_sub(ym, yp));
+                            t[i][2] = p_mul(p_splat(ihz), p_sub(pz_m2[r][i], pz_new[r][i]));
+                        }
+                        const float2 g0 = p_add(p_sub(t[0][0], t[0][1]), t[0][2]);
+                        const float2 g1 = p_sub(p_sub(t[1][1], t[1][0]), t[1][2]);
+                        const float2 g2 = p_add(p_sub(t[2][0], t[2][1]), t[2][2]);
+                        gv[0][0] = g0.x, gv[0][1] = g1.x, gv[0][2] = g2.x;
+                        gv[1][0] = g0.y, gv[1][1] = g1.y, gv[1][2] = g2.y;
+                    } else {
+                        T t[2][3][3];
 #pragma unroll
-                    for (int v = 0; v < 2; ++v) {
-                        gv[v][0] = t[v][0][0] - t[v][0][1] + t[v][0][2];
-                        gv[v][1] = -t[v][1][0] + t[v][1][1] - t[v][1][2];
-                        gv[v][2] = t[v][2][0] - t[v][2][1] + t[v][2][2];
+                        for (int i = 0; i < 3; ++i) {
+                            const auto a = ld_pair(PT(ps, i, rp, cp - 2)), b = ld_pair(PT(ps, i, rp, cp)),
+                                       c = ld_pair(PT(ps, i, rp, cp + 2));
+                            t[0][i][0] = ihx * (a.y - b.y);
+                            t[1][i][0] = ihx * (b.x - c.x);
+                            const auto ym = ld_pair(PT(ps, 3 + i, rp - 1, cp)),
+                                       yp = ld_pair(PT(ps, 3 + i, rp + 1, cp));
+                            t[0][i][1] = ihy * (ym.x - yp.x);
+                            t[1][i][1] = ihy * (ym.y - yp.y);
+                            t[0][i][2] = ihz * (pz_m2[r][i].x - pz_new[r][i].x);
+                            t[1][i][2] = ihz * (pz_m2[r][i].y - pz_new[r][i].y);
+                        }
+#pragma unroll
+                        for (int v = 0; v < 2; ++v) {
+                            gv[v][0] = t[v][0][0] - t[v][0][1] + t[v][0][2];
+                            gv[v][1] = -t[v][1][0] + t[v][1][1] - t[v][1][2];
+                            gv[v][2] = t[v][2][0] - t[v][2][1] + t[v][2][2];
+                        }
                     }
+                    // |g|^2 of a voxel, summed in the element type, then in FP64.
+                    auto sq = [](const T (&w)[3]) -> double {
+                        if constexpr (sizeof(T) == 4)
+                            return (double) __fmaf_rn(w[2], w[2], __fmaf_rn(w[1], w[1], __fmul_rn(w[0], w[0])));
+                        else return (double) (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+                    };
                     T *o = V.grad + zoff + (long long) y * g.ys + x;
                     if (in0 && in1) {
 #pragma unroll
                         for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, gv[0][c], gv[1][c]);
-                        acc += (double) (gv[0][0] * gv[0][0] + gv[0][1] * gv[0][1] + gv[0][2] * gv[0][2]);
-                        acc += (double) (gv[1][0] * gv[1][0] + gv[1][1] * gv[1][1] + gv[1][2] * gv[1][2]);
+                        acc += sq(gv[0]);
+                        acc += sq(gv[1]);
                     } else {
                         // one voxel of the pair is on the boundary (x = 0 or nx - 1)
                         T w[3];
@@ -1013,19 +1148,17 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                             w[c] = in0 ? gv[0][c] : gv[1][c];
                             o[(in0 ? 0 : 1) + c * g.cs] = w[c];
                         }
-                        acc += (double) (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+                        acc += sq(w);
                     }
                 }
             }
 #pragma unroll
             for (int r = 0; r < RYT; ++r)
 #pragma unroll
-                for (int v = 0; v < 2; ++v)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        pz_m2[r][v][i] = pz_m1[r][v][i];
-                        pz_m1[r][v][i] = pz_new[r][v][i];
-                    }
+                for (int i = 0; i < 3; ++i) {
+                    pz_m2[r][i] = pz_m1[r][i];
+                    pz_m1[r][i] = pz_new[r][i];
+                }
         }
         if (failed) {
             if (tid == 0) tma_fault<L::S>(st, bars, kbase, fail_it + 1, issued_n);
@@ -1300,10 +1433,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 // FP64 path keeps the reference's operation order.
                 const T ih[3] = {s_ih[0], s_ih[1], s_ih[2]};
                 const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
-                const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1],
-                                 FD<T>::one_twelfth * ih[2]};
+                const T k2n[3] = {-FD<T>::one_twelfth * ih[0], -FD<T>::one_twelfth * ih[1],
+                                  -FD<T>::one_twelfth * ih[2]};
                 auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
-                    if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+                    if constexpr (sizeof(T) == 4) return c4_folded(p1, m1, p2, m2, k1[ax], k2n[ax]);
                     return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
                 };
 #pragma unroll
@@ -1834,9 +1967,14 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                     }
                 } else {
                     T jv[2];
-                    stencil_pair<T, TMA_PX, TMA_PLANE>(jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
-                                                       tile_x_in,
-                                                       [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); });
+                    auto det2 = [&](const auto &a) {
+                        const auto J = det_i_plus2(a);
+                        jv[0] = J.x;
+                        jv[1] = J.y;
+                    };
+                    stencil_pair<T, TMA_PX, TMA_PLANE>(
+                        jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in, tile_x_in,
+                        [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); }, det2);
                     T *o = jout + off;
                     if (pair_in)
                         st_pair(o, jv[0], jv[1]);
@@ -1925,6 +2063,292 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
 }
 
 // ------------------------------------------------------------------------
+// k_gather_tma: the gather pass of the adjoint,
+//   grad_c(q) = sum_a sum_t W[c][a](q - t e_a) * kappa(k_a(q - t e_a), t)
+// (the same taps, coefficients and summation order as k_adjoint_gather), on
+// weights streamed by TMA.  W is [c][a][wn] with the field's row and plane
+// strides.  A 32 x TT_Y tile marches through its z range; the stage of plane
+// q holds W[.][z] of the tile at plane q and, for the gradient plane
+// ze = q - 2, W[.][x] of the tile's rows with four columns each side and
+// W[.][y] of its columns with two rows each side.  Each thread keeps its
+// pair's W[.][z] of planes ze-2 .. ze+2 in registers.  A stage is consumed
+// in its own iteration, so a block barrier every B planes is all that
+// guards reuse (loads run LA = S - B iterations ahead).  Pairs whose taps
+// all lie at fourth-order voxels (four or more voxels from every face) take
+// constant coefficients, in FP32 as pairs; the others choose each tap's
+// coefficient by the tap voxel's scheme.
+// ------------------------------------------------------------------------
+template <typename T, int TXW>
+struct GatherTmaLayout {
+    static constexpr int XPX = TXW + 2 * TMA_HX;  // W[.][x] box: TXW + 8 columns, TT_Y rows
+    static constexpr int X_ELEMS = 3 * TT_Y * XPX;
+    static constexpr int YPY = TT_Y + 2 * TMA_HY;  // W[.][y] box: TXW columns, TT_Y + 4 rows
+    static constexpr int Y_ELEMS = 3 * YPY * TXW;
+    static constexpr int Z_ELEMS = 3 * TT_Y * TXW;  // W[.][z] box: the tile
+    static constexpr int X_OFF = 0;
+    static constexpr int Y_OFF = X_ELEMS * (int) sizeof(T);
+    static constexpr int Z_OFF = Y_OFF + Y_ELEMS * (int) sizeof(T);
+    static constexpr int STAGE_BYTES = (Z_OFF + Z_ELEMS * (int) sizeof(T) + 127) / 128 * 128;
+    static constexpr int S = sizeof(T) == 4 ? 5 : 4;  // 105 KB (FP32, two blocks per SM), 168 KB (FP64)
+    static constexpr int B = 2;                       // planes between block barriers
+    static constexpr int LA = S - B;                  // load distance
+    static constexpr int BAR_OFF = S * STAGE_BYTES;
+    static constexpr int BYTES = BAR_OFF + S * 8;
+    static_assert(Y_OFF % 128 == 0 && Z_OFF % 128 == 0, "boxes start 128-byte aligned");
+};
+
+template <typename T, int TXW, int TYT>
+__global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
+    k_gather_tma(const __grid_constant__ CUtensorMap tm_wx, const __grid_constant__ CUtensorMap tm_wy,
+                 const __grid_constant__ CUtensorMap tm_wz, const Geom g, T *__restrict__ gout, int tiles_x,
+                 int tiles_y, int ntiles, int bz) {
+    using L = GatherTmaLayout<T, TXW>;
+    using P2 = typename PairOf<T>::type;
+    constexpr int TPX = TXW / 2, RYT = TT_Y / TYT, S = L::S, LA = L::LA, XPX = L::XPX, YPY = L::YPY;
+    static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char *smem = align_smem_128(smem_dyn);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
+    __shared__ int s_fault;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
+    if (tid == 0) {
+        for (int k = 0; k < S; ++k) mbar_init(&bars[k], 1);
+        fence_mbar_init();
+        tmap_prefetch(&tm_wx);
+        tmap_prefetch(&tm_wy);
+        tmap_prefetch(&tm_wz);
+        s_fault = 0;
+    }
+    __syncthreads();
+    const int n[3] = {g.nx, g.ny, g.nz};
+    // Fourth-order coefficients kappa(S_C4, t) by tap, t = -2, -1, 1, 2.
+    const T kc[4] = {FD<T>::one_twelfth, -FD<T>::two_thirds, FD<T>::two_thirds, -FD<T>::one_twelfth};
+    uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
+
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int txi = tile % tiles_x, tyi = (tile / tiles_x) % tiles_y, tzi = tile / (tiles_x * tiles_y);
+        const int x0 = txi * TXW, y0 = tyi * TT_Y, z0 = tzi * bz;
+        const int z1 = min(z0 + bz, g.nz);
+        const int n_it = z1 - z0 + 4;  // W[.][z] planes z0-2 .. z1+1
+        __syncthreads();  // every warp has left the previous tile's stages
+        int issued_n = 0;
+        auto issue = [&](int j) {
+            issued_n = j + 1;
+            const uint32_t k = kbase + j;
+            uint64_t *bar = &bars[k % S];
+            unsigned char *sb = smem + (k % S) * L::STAGE_BYTES;
+            const int q = z0 - 2 + j, ze = q - 2;
+            const bool with_xy = ze >= z0 && ze < z1;
+            mbar_arrive_expect_tx(bar, (uint32_t) ((L::Z_ELEMS + (with_xy ? L::X_ELEMS + L::Y_ELEMS : 0)) * sizeof(T)));
+            tma_load_5d(sb + L::Z_OFF, &tm_wz, bar, x0, y0, q, 2, 0);
+            if (with_xy) {
+                tma_load_5d(sb + L::X_OFF, &tm_wx, bar, x0 - TMA_HX, y0, ze, 0, 0);
+                tma_load_5d(sb + L::Y_OFF, &tm_wy, bar, x0, y0 - TMA_HY, ze, 1, 0);
+            }
+        };
+        if (tid == 0)
+            for (int j = 0; j < min(LA, n_it); ++j) issue(j);
+
+        const int x = x0 + 2 * tx;  // this thread's columns: x, x + 1
+        const bool pair_in = x + 1 < g.nx;
+        // Own pair's W[c][z] of planes q-4 .. q (index 2 - t holds plane ze - t).
+        P2 wq[RYT][3][5];
+#pragma unroll
+        for (int r = 0; r < RYT; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 5; ++k) wq[r][c][k] = P2{T(0), T(0)};
+        bool failed = false;
+        int fail_it = 0;
+        for (int it = 0; it < n_it; ++it) {
+            const uint32_t k = kbase + it;
+            if (it % L::B == 0) {
+                __syncthreads();
+                if (s_fault) {
+                    failed = true;
+                    fail_it = it;
+                    break;
+                }
+                if (tid == 0)
+                    for (int j = it + LA; j < min(it + LA + L::B, n_it); ++j) issue(j);
+            }
+            // A load that does not arrive stops the block at the next barrier.
+            if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u)) s_fault = 1;
+            const unsigned char *sb = smem + (k % S) * L::STAGE_BYTES;
+            const T *wx = reinterpret_cast<const T *>(sb + L::X_OFF);
+            const T *wy = reinterpret_cast<const T *>(sb + L::Y_OFF);
+            const T *wz = reinterpret_cast<const T *>(sb + L::Z_OFF);
+            const int q = z0 - 2 + it, ze = q - 2;
+#pragma unroll
+            for (int r = 0; r < RYT; ++r) {
+                const int ly = ty + r * TYT;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) wq[r][c][kk] = wq[r][c][kk + 1];
+                    wq[r][c][4] = ld_pair(wz + (c * TT_Y + ly) * TXW + 2 * tx);
+                }
+            }
+            if (ze < z0 || ze >= z1 || x >= g.nx) continue;
+#pragma unroll
+            for (int r = 0; r < RYT; ++r) {
+                const int ly = ty + r * TYT, y = y0 + ly;
+                if (y >= g.ny) continue;
+                T acc[2][3];
+                const bool deep = x >= 4 && x + 1 <= g.nx - 5 && y >= 4 && y <= g.ny - 5 && ze >= 4 && ze <= g.nz - 5;
+                if constexpr (sizeof(T) == 4) {
+                    if (deep) {
+                        // Taps t = -2, -1, 1, 2 along x, y, z; each tap's
+                        // pair is W at (x - t, x + 1 - t), rounded as the
+                        // general path below does (one fma per tap).
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const T *px = wx + (c * TT_Y + ly) * XPX + 2 * tx + TMA_HX;
+                            const float2 xm = ld_pair(px - 2), xc = ld_pair(px), xp = ld_pair(px + 2);
+                            const T *py = wy + (c * YPY + ly + TMA_HY) * TXW + 2 * tx;
+                            const float2 ym2 = ld_pair(py - 2 * TXW), ym1 = ld_pair(py - TXW);
+                            const float2 yp1 = ld_pair(py + TXW), yp2 = ld_pair(py + 2 * TXW);
+                            float2 a2 = p_mul(xp, p_splat(kc[0]));
+                            a2 = p_fma(make_float2(xc.y, xp.x), p_splat(kc[1]), a2);
+                            a2 = p_fma(make_float2(xm.y, xc.x), p_splat(kc[2]), a2);
+                            a2 = p_fma(xm, p_splat(kc[3]), a2);
+                            a2 = p_fma(yp2, p_splat(kc[0]), a2);
+                            a2 = p_fma(yp1, p_splat(kc[1]), a2);
+                            a2 = p_fma(ym1, p_splat(kc[2]), a2);
+                            a2 = p_fma(ym2, p_splat(kc[3]), a2);
+                            a2 = p_fma(wq[r][c][4], p_splat(kc[0]), a2);
+                            a2 = p_fma(wq[r][c][3], p_splat(kc[1]), a2);
+                            a2 = p_fma(wq[r][c][1], p_splat(kc[2]), a2);
+                            a2 = p_fma(wq[r][c][0], p_splat(kc[3]), a2);
+                            acc[0][c] = a2.x;
+                            acc[1][c] = a2.y;
+                        }
+                    }
+                }
+                if (sizeof(T) != 4 || !deep) {
+                    // Per voxel and tap: the tap voxel p = q - t e_a differs
+                    // from q only along a, so the outer / penultimate flags of
+                    // the other axes come from q (src/jacobian.c:70-242).
+#pragma unroll
+                    for (int v = 0; v < 2; ++v) {
+                        const int q3[3] = {x + v, y, ze};
+                        bool ob[3], pb[3];
+#pragma unroll
+                        for (int b = 0; b < 3; ++b) {
+                            ob[b] = q3[b] == 0 || q3[b] == n[b] - 1;
+                            pb[b] = q3[b] == 1 || q3[b] == n[b] - 2;
+                        }
+                        T a3[3] = {T(0), T(0), T(0)};
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
+                            const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
+#pragma unroll
+                            for (int t = -2; t <= 2; ++t) {
+                                const int pa = q3[a] - t;
+                                if (pa < 0 || pa >= n[a]) continue;
+                                const bool outer = o_other || pa == 0 || pa == n[a] - 1;
+                                const bool pen = p_other || pa == 1 || pa == n[a] - 2;
+                                const int kk = outer ? (pa == 0 ? S_FWD : (pa == n[a] - 1 ? S_BWD : S_C2))
+                                                     : (pen ? S_C2 : S_C4);
+                                const T kp = kappa<T>(kk, t);
+                                if (kp == T(0)) continue;
+#pragma unroll
+                                for (int c = 0; c < 3; ++c) {
+                                    T w;
+                                    if (a == 0)
+                                        w = wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX];
+                                    else if (a == 1)
+                                        w = wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v];
+                                    else
+                                        w = v ? wq[r][c][2 - t].y : wq[r][c][2 - t].x;
+                                    if constexpr (sizeof(T) == 4) a3[c] = __fmaf_rn(w, kp, a3[c]);
+                                    else a3[c] = a3[c] + w * kp;
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) acc[v][c] = a3[c];
+                    }
+                }
+                T *o = gout + (long long) ze * g.zs + (long long) y * g.ys + x;
+                if (pair_in) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) st_pair(o + c * g.cs, acc[0][c], acc[1][c]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) o[c * g.cs] = acc[0][c];
+                }
+            }
+        }
+        if (failed) {
+            // Wait (bounded) for the loads still in flight, mark the tile's
+            // gradient NaN and leave.
+            if (tid == 0)
+                for (int j = max(0, fail_it - L::B); j < issued_n; ++j) {
+                    const uint32_t kk = kbase + j;
+                    mbar_wait_bounded(&bars[kk % S], (kk / S) & 1u, 1u << 16);
+                }
+            const T nan = T(NAN);
+            for (int ze = z0; ze < z1; ++ze)
+#pragma unroll
+                for (int r = 0; r < RYT; ++r) {
+                    const int y = y0 + ty + r * TYT;
+                    if (y >= g.ny) continue;
+                    for (int v = 0; v < 2; ++v) {
+                        if (x + v >= g.nx) continue;
+                        for (int c = 0; c < 3; ++c)
+                            gout[c * g.cs + (long long) ze * g.zs + (long long) y * g.ys + x + v] = nan;
+                    }
+                }
+            __syncthreads();
+            return;
+        }
+        kbase += n_it;
+    }
+}
+
+template <typename T, int TXW, int TYT>
+int gather_blocks_v() {
+    static const int n = [] {
+        int v = 0;
+        cudaFuncSetAttribute(k_gather_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GatherTmaLayout<T, TXW>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gather_tma<T, TXW, TYT>, TXW / 2 * TYT,
+                                                      GatherTmaLayout<T, TXW>::BYTES + 128);
+        return v;
+    }();
+    return n;
+}
+
+// Gather pass on TMA-staged weights: tiles of 32 x TT_Y voxels, 16 x 16
+// threads, the z split as in launch_jacobian_tma_v.
+template <typename T>
+cudaError_t launch_gather_tma(const CUtensorMap &tm_wx, const CUtensorMap &tm_wy, const CUtensorMap &tm_wz,
+                              const Geom &g, T *gout, int num_sms, cudaStream_t s) {
+    constexpr int TXW = 32, TYT = 16, BZ = 32;
+    constexpr int smem = GatherTmaLayout<T, TXW>::BYTES + 128;
+    static std::atomic<unsigned long long> devs{0};
+    const cudaError_t attr = opt_in_smem(k_gather_tma<T, TXW, TYT>, smem, devs);
+    if (attr != cudaSuccess) return attr;
+    const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
+    const int cols = tiles_x * tiles_y;
+    const int slots = std::max(1, gather_blocks_v<T, TXW, TYT>()) * num_sms;  // resident blocks
+    int nzt = (g.nz + BZ - 1) / BZ;                                      // z tiles per column
+    const int waves = (cols * nzt + slots - 1) / slots;
+    nzt = std::min((g.nz + 7) / 8, std::max(nzt, waves * slots / cols));  // at least 8 planes a tile
+    const int bz = (g.nz + nzt - 1) / nzt;
+    const int ntiles = cols * ((g.nz + bz - 1) / bz);
+    const int grid = std::min(ntiles, slots);
+    k_gather_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_wx, tm_wy, tm_wz, g, gout, tiles_x, tiles_y,
+                                                                      ntiles, bz);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------
 // Fused adjoint of the Jacobian map (autograd backward) with the TMA
 // pipeline: grad_c(q) = sum_a sum_t W[c][a](q - t e_a) kappa(k_a(q - t e_a), t)
 // with W[c][a](p) = gJ(p) cof_ca(I + A(p)) ih_a, A(p) the stencil matrix of
@@ -1982,7 +2406,7 @@ struct Planes5 {
 // reference's operation order in FP64.
 template <typename T, int PX, int PLANE>
 __device__ __forceinline__ T adj_deriv(const Planes5<T> &sp, int c, int o, int ax, int k, const T (&ih)[3],
-                                       const T (&k1)[3], const T (&k2)[3]) {
+                                       const T (&k1)[3], const T (&k2n)[3]) {
     const int oc = c * PLANE + o;
     auto v = [&](int d) -> T {
         if (ax == 0) return sp.c0[oc + d];
@@ -1994,7 +2418,7 @@ __device__ __forceinline__ T adj_deriv(const Planes5<T> &sp, int c, int o, int a
     case S_BWD: return fd_bwd<T>(v(0), v(-1), v(-2), ih[ax]);
     case S_C2: return fd_c2<T>(v(1), v(-1), ih[ax]);
     default:
-        if (sizeof(T) == 4) return (v(1) - v(-1)) * k1[ax] - (v(2) - v(-2)) * k2[ax];
+        if constexpr (sizeof(T) == 4) return c4_folded(v(1), v(-1), v(2), v(-2), k1[ax], k2n[ax]);
         return fd_c4<T>(v(1), v(-1), v(2), v(-2), ih[ax]);
     }
 }
@@ -2042,11 +2466,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     __syncthreads();
     const T ih[3] = {(T) g.ih[0], (T) g.ih[1], (T) g.ih[2]};
     const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
-    const T k2[3] = {FD<T>::one_twelfth * ih[0], FD<T>::one_twelfth * ih[1], FD<T>::one_twelfth * ih[2]};
+    const T k2n[3] = {-FD<T>::one_twelfth * ih[0], -FD<T>::one_twelfth * ih[1], -FD<T>::one_twelfth * ih[2]};
     const int n[3] = {g.nx, g.ny, g.nz};
     // Fourth-order difference (the generic path's arithmetic for S_C4).
     auto c4 = [&](T p1, T m1, T p2, T m2, int ax) -> T {
-        if (sizeof(T) == 4) return (p1 - m1) * k1[ax] - (p2 - m2) * k2[ax];
+        if constexpr (sizeof(T) == 4) return c4_folded(p1, m1, p2, m2, k1[ax], k2n[ax]);
         return fd_c4<T>(p1, m1, p2, m2, ih[ax]);
     };
     // Differences of the cell pair (xf, xf + 1) at box offset o (row and
@@ -2114,9 +2538,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
         schemes_at(x, y, z, g, ks);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            a[c][0] = wx ? adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2) : T(0);
-            a[c][1] = wy ? adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2) : T(0);
-            a[c][2] = wz ? adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2) : T(0);
+            a[c][0] = wx ? adj_deriv<T, PX, PLANE>(sp, c, o, 0, ks[0], ih, k1, k2n) : T(0);
+            a[c][1] = wy ? adj_deriv<T, PX, PLANE>(sp, c, o, 1, ks[1], ih, k1, k2n) : T(0);
+            a[c][2] = wz ? adj_deriv<T, PX, PLANE>(sp, c, o, 2, ks[2], ih, k1, k2n) : T(0);
         }
     };
     uint32_t kbase = 0;
@@ -2497,6 +2921,8 @@ cudaError_t launch_adjoint_tma(const CUtensorMap &tm_u, const Geom &g, const T *
     template int greedy_tma_blocks_per_sm<T>();                                                             \
     template cudaError_t launch_jacobian_tma<T>(const CUtensorMap &, const Geom &, T *, long long, long long, int, \
                                                 cudaStream_t, const T *, T *, long long);                   \
+    template cudaError_t launch_gather_tma<T>(const CUtensorMap &, const CUtensorMap &, const CUtensorMap &,   \
+                                              const Geom &, T *, int, cudaStream_t);                        \
     template int gradient_tma_blocks_per_sm<T>(int, int);                                                   \
     template cudaError_t launch_trial_rel<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
                                              unsigned char *, int, int, TileQueue *);                       \
