@@ -311,6 +311,23 @@ bool encode_map(CUtensorMap *out, CUtensorMapDataType type, size_t esize, const 
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor map over the adjoint's weights W[c][a][wn] (the field's row and
+// plane strides): dimensions x, y, z, a, c; boxes of box_x x box_y voxels
+// of one plane, one axis a and all three components.
+bool encode_weights_map(CUtensorMap *out, CUtensorMapDataType type, size_t esize, const void *W, const Geom &g,
+                        long long wn, uint32_t box_x, uint32_t box_y) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[5] = {(cuuint64_t) g.nx, (cuuint64_t) g.ny, (cuuint64_t) g.nz, 3, 3};
+    cuuint64_t strides[4] = {(cuuint64_t) g.ys * esize, (cuuint64_t) g.zs * esize, (cuuint64_t) wn * esize,
+                             (cuuint64_t) (3 * wn) * esize};
+    cuuint32_t box[5] = {box_x, box_y, 1, 1, 3};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(out, type, 5, const_cast<void *>(W), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Geometry of the solver's own buffers: rows padded to 16 elements so that
 // every row starts 16-byte aligned (a TMA requirement for all element types).
 Geom pitched(const Geom &g) {
@@ -665,11 +682,11 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
             const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
             // Boxes: the tile plus 4 voxels in x (16-byte aligned start) and 2
             // rows in y for the stencil inputs; the bare tile for J_t and the
-            // mask.  The greedy method's error maps are read as three planes
-            // with 3 rows of halo in y (slots 3 and 4).
+            // mask.  The greedy method's error maps are read one plane at a
+            // time with 3 rows of halo in y (slots 3 and 4).
             const uint32_t bx = (uint32_t) tile_x;
             T *m3 = gradient ? d.ep[0] : d.v[0], *m4 = gradient ? d.ep[1] : d.v[1];
-            const uint32_t my = gradient ? TT_Y + 4 : TT_Y + 6, mz = gradient ? 1 : 3;
+            const uint32_t my = gradient ? TT_Y + 4 : TT_Y + 6, mz = 1;
             bool ok = encode_map(&h_maps[0], ft, sizeof(T), d.field[0], g, 3, bx + 8, TT_Y + 4) &&
                       encode_map(&h_maps[1], ft, sizeof(T), d.field[1], g, 3, bx + 8, TT_Y + 4) &&
                       encode_map(&h_maps[2], ft, sizeof(T), d.grad, g, 3, bx + 8, TT_Y + 4) &&
@@ -1407,18 +1424,27 @@ int adjoint_device_impl(const Geom &g, const T *field, const T *gJ, T *gout, cud
     DTB_CUDA(cudaStreamWaitEvent(s, g_adj_done[dev], 0));
     T *W = reinterpret_cast<T *>(base);
     // The weight pass on the TMA stencil kernel when the layout allows it
-    // (as for the Jacobian map), else on the plain-load kernel.
+    // (as for the Jacobian map), else on the plain-load kernel.  The gather
+    // pass streams W by TMA after a TMA weight pass (W then has rows a
+    // multiple of 16 bytes long) into a pair-aligned gradient.
     bool w_done = false;
+    const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
     if (g.order == 4 && (g.ys * (long long) sizeof(T)) % 16 == 0 && reinterpret_cast<uintptr_t>(field) % 16 == 0 &&
         reinterpret_cast<uintptr_t>(gJ) % (2 * sizeof(T)) == 0) {
         CUtensorMap tm;
-        const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
         if (encode_map(&tm, ft, sizeof(T), field, g, 3, 32 + 2 * 4, TT_Y + 2 * 2)) {
             DTB_CUDA(launch_jacobian_tma<T>(tm, g, nullptr, g.ys, g.zs, num_sms(), s, gJ, W, wn));
             w_done = true;
         }
     }
-    DTB_CUDA(launch_adjoint<T>(g, field, gJ, W, wn, gout, w_done, s));
+    CUtensorMap tw[3];
+    if (w_done && reinterpret_cast<uintptr_t>(gout) % (2 * sizeof(T)) == 0 &&
+        encode_weights_map(&tw[0], ft, sizeof(T), W, g, wn, 32 + 2 * 4, TT_Y) &&
+        encode_weights_map(&tw[1], ft, sizeof(T), W, g, wn, 32, TT_Y + 2 * 2) &&
+        encode_weights_map(&tw[2], ft, sizeof(T), W, g, wn, 32, TT_Y))
+        DTB_CUDA(launch_gather_tma<T>(tw[0], tw[1], tw[2], g, gout, num_sms(), s));
+    else
+        DTB_CUDA(launch_adjoint<T>(g, field, gJ, W, wn, gout, w_done, s));
     DTB_CUDA(cudaEventRecord(g_adj_done[dev], s));
     return DTB_OK;
 }

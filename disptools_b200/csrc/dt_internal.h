@@ -168,6 +168,12 @@ template <typename T>
 cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
                                 int num_sms, cudaStream_t s, const T *gJ = nullptr, T *W = nullptr,
                                 long long wn = 0);
+// Gather pass of the adjoint on TMA-staged weights W[c][a][wn]: maps over W
+// with boxes 40 x TT_Y (axis x), 32 x (TT_Y + 4) (axis y) and 32 x TT_Y
+// (axis z), one plane, three components.
+template <typename T>
+cudaError_t launch_gather_tma(const CUtensorMap &tm_wx, const CUtensorMap &tm_wy, const CUtensorMap &tm_wz,
+                              const Geom &g, T *gout, int num_sms, cudaStream_t s);
 // Fused adjoint of the Jacobian stencil of order 4 (one TMA kernel, no
 // weight buffer): `tm_u` maps the field with box 40 x 24 x 1 x 3; gJ and gout
 // in the field's dense layout.

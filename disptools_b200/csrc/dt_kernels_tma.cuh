@@ -52,12 +52,17 @@ struct TrialTmaLayout {
     // against the current stencil reads.
     static constexpr int R = 4;
     static constexpr int U_BYTES = 3 * TMA_PLANE * (int) sizeof(T);
-    // Greedy method: the error map box of planes q-1, q, q+1, one row wider
-    // on each y side than the field box (the update reads v(p +- e_k)).
+    // Greedy method: the error map, one plane per iteration, one row wider
+    // on each y side than the field box (the update reads v(p +- e_k)), into
+    // a ring of RV planes of its own: forming candidate plane q reads the
+    // planes q-1, q, q+1 loaded by the last three iterations, and loads run
+    // S iterations ahead.  The gradient method's stage holds the g box.
     static constexpr int VPY = TMA_PY + 2;
     static constexpr int V_PLANE = VPY * TMA_PX;
-    static constexpr int V3_BYTES = 3 * V_PLANE * (int) sizeof(T);
-    static constexpr int G_BYTES = GREEDY ? (V3_BYTES + 127) / 128 * 128 : U_BYTES;  // g or the v box
+    static constexpr int V_BYTES = V_PLANE * (int) sizeof(T);
+    static constexpr int V_SLOT = (V_BYTES + 127) / 128 * 128;
+    static constexpr int RV = S + 2;
+    static constexpr int G_BYTES = GREEDY ? 0 : U_BYTES;
     static constexpr int JT_BYTES = TXW * TT_Y * (int) sizeof(T);
     static constexpr int MASK_BYTES = TXW * TT_Y;
     static constexpr int JT_OFF = U_BYTES + G_BYTES;
@@ -65,7 +70,8 @@ struct TrialTmaLayout {
     static constexpr int STAGE_BYTES = MASK_OFF + MASK_BYTES;  // u, g (or v), Jt, mask
     static_assert(STAGE_BYTES % 128 == 0, "stages stay 128-byte aligned");
     static constexpr int RING_OFF = S * STAGE_BYTES;
-    static constexpr int BAR_OFF = RING_OFF + R * U_BYTES;
+    static constexpr int VRING_OFF = RING_OFF + R * U_BYTES;
+    static constexpr int BAR_OFF = VRING_OFF + (GREEDY ? RV * V_SLOT : 0);
     static constexpr int BYTES = BAR_OFF + S * 8;
 };
 
@@ -166,18 +172,18 @@ using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 //   greedy_prefetch_stale has already copied into `out` (the caller waits
 //   for its own copies first);
 // * outside the volume: 0 (the field box arrives zero-filled there).
-// `vb` is the error map box: planes q-1, q, q+1 of rows y0-3 .. y0+TT_Y+2,
-// columns as in the field box.  A thread forms the three components of one
+// `vm`, `vc`, `vn` are the error map's planes q-1, q, q+1, rows
+// y0-3 .. y0+TT_Y+2, columns as in the field box.  A thread forms the three components of one
 // 16-byte run of x with vector reads; a run that is not all interior picks
 // each voxel's value by its class.  Values formed at non-interior voxels
 // (from zero-filled or clamped neighbours) are discarded.  The box's first
 // and last columns lack an x neighbour; no stencil reads them.
 template <typename T, typename L>
-__device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, int tid, int nth, const Geom &g,
-                                            int x0, int y0, int q, const T *dd) {
+__device__ __forceinline__ void greedy_form(const T *ub, const T *vm, const T *vc, const T *vn, T *out, int tid,
+                                            int nth, const Geom &g, int x0, int y0, int q, const T *dd) {
     using V4 = Vec16<T>;
     constexpr int VEC = 16 / (int) sizeof(T);
-    constexpr int PX = L::TMA_PX, VP = L::V_PLANE, UP = L::TMA_PLANE;
+    constexpr int PX = L::TMA_PX, UP = L::TMA_PLANE;
     constexpr int CPR = PX / VEC, NPOS = TMA_PY * CPR;  // runs per row, per plane
     static_assert(PX % VEC == 0, "rows split in whole runs");
     const bool q_in = q >= 1 && q <= g.nz - 2;
@@ -188,8 +194,9 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, in
         const int ly = i / CPR;
         const int lxc = (i - ly * CPR) * VEC;
         const int gy = y0 - TMA_HY + ly, gx = x0 - TMA_HX + lxc;
-        const int o = ly * PX + lxc;                  // run offset in a field-box plane
-        const T *vp = vb + VP + (ly + 1) * PX + lxc;  // v at the run's voxels
+        const int o = ly * PX + lxc;           // run offset in a field-box plane
+        const int vo = (ly + 1) * PX + lxc;    // the same run in an error-map plane
+        const T *vp = vc + vo;                 // v at the run's voxels
         const bool row_in = q_in && gy >= 1 && gy <= g.ny - 2;
         const bool all_in = row_in && gx >= 1 && gx + VEC - 1 <= g.nx - 2;
         // Classes of the run's voxels: formed (interior) or kept (the
@@ -218,8 +225,7 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vb, T *out, in
                     lo[e] = e > 0 ? el(cur, e - 1) : el(prv, VEC - 1);
                 }
             } else {
-                const int step = c == 1 ? PX : VP;
-                const V4 h = ld(vp + step), l = ld(vp - step);
+                const V4 h = c == 1 ? ld(vp + PX) : ld(vn + vo), l = c == 1 ? ld(vp - PX) : ld(vm + vo);
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
                     hi[e] = el(h, e);
@@ -433,6 +439,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     unsigned char *smem = align_smem_128(smem_dyn);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
     T *ring = reinterpret_cast<T *>(smem + L::RING_OFF);
+    T *vring = reinterpret_cast<T *>(smem + L::VRING_OFF);  // greedy: error-map planes
     __shared__ double red[2 * (NTH / 32)];
     __shared__ int s_flag, s_fault;
     __shared__ T s_dd[3];  // greedy steps of the current tile
@@ -445,6 +452,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     }
     __syncthreads();
     uint32_t kbase = 0;  // iterations consumed by this block (mbarrier phases)
+    uint32_t vbase = 0;  // greedy: error-map planes loaded by this block (ring position)
 
     __shared__ int s_tile;
     for (int tile = take_tile<TPX>(queue, total_tiles, &s_tile); tile >= 0;
@@ -488,13 +496,18 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             unsigned char *sb = smem + s * L::STAGE_BYTES;
             const int q = z0 - 2 + j, ze = q - 2;
             const bool with_target = ze >= z0 && ze < z1;
-            const uint32_t bytes = L::U_BYTES + (trial ? (GREEDY ? L::V3_BYTES : L::U_BYTES) : 0) +
+            // Greedy: error-map plane q+1 (and, with the first plane, q-1
+            // and q), plane p into ring slot (vbase + p - z0 + 3) % RV.
+            const int nv = GREEDY && trial ? (j == 0 ? 3 : 1) : 0;
+            const uint32_t bytes = L::U_BYTES + (trial && !GREEDY ? L::U_BYTES : 0) + nv * L::V_BYTES +
                                    (with_target ? L::JT_BYTES + L::MASK_BYTES : 0);
             mbar_arrive_expect_tx(&bars[s], bytes);
             tma_load_4d(sb, tm_u, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
             if (trial) {
                 if (GREEDY)
-                    tma_load_3d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY - 1, q - 1);
+                    for (int p = q + 2 - nv; p <= q + 1; ++p)
+                        tma_load_3d(vring + ((vbase + (uint32_t) (p - z0 + 3)) % L::RV) * (L::V_SLOT / sizeof(T)),
+                                    tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY - 1, p);
                 else
                     tma_load_4d(sb + L::U_BYTES, tm_g, &bars[s], x0 - TMA_HX, y0 - TMA_HY, q, 0);
             }
@@ -565,8 +578,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 V4 *c4 = reinterpret_cast<V4 *>(slot);
                 if (GREEDY && trial) {
                     cp_async_wait_all();  // this thread's stale values of plane q
-                    greedy_form<T, L>(reinterpret_cast<const T *>(sb), reinterpret_cast<const T *>(sb + L::U_BYTES),
-                                      slot, tid, NTH, g, x0, y0, q, s_dd);
+                    auto vplane = [&](int p) -> const T * {
+                        return vring + ((vbase + (uint32_t) (p - z0 + 3)) % L::RV) * (L::V_SLOT / sizeof(T));
+                    };
+                    greedy_form<T, L>(reinterpret_cast<const T *>(sb), vplane(q - 1), vplane(q), vplane(q + 1), slot,
+                                      tid, NTH, g, x0, y0, q, s_dd);
                 } else
                 // Counted from the last thread: the runs left over after
                 // whole sweeps go to the last warps, not to warp 0, whose
@@ -788,6 +804,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             return;
         }
         kbase += n_it;
+        vbase += n_it + 2;
 
         const double2 rr = block_reduce_n<NTH, TPX>(acc_s, (double) acc_mt, red);
         if (tid == 0) V.part_t[lt] = rr;
@@ -2197,12 +2214,23 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                 const int ly = ty + r * TYT, y = y0 + ly;
                 if (y >= g.ny) continue;
                 T acc[2][3];
-                const bool deep = x >= 4 && x + 1 <= g.nx - 5 && y >= 4 && y <= g.ny - 5 && ze >= 4 && ze <= g.nz - 5;
+                // Three paths: the pair and all its taps at fourth-order
+                // voxels (four or more voxels from every face); y and z that
+                // deep but x near a face (only the x taps choose a scheme);
+                // the rest.  In FP32 the first runs on pairs.
+                const bool yz_deep = y >= 4 && y <= g.ny - 5 && ze >= 4 && ze <= g.nz - 5;
+                const bool deep = yz_deep && x >= 4 && x + 1 <= g.nx - 5;
+                auto acc_op = [](T a, T w, T kp) -> T {
+                    if constexpr (sizeof(T) == 4) return __fmaf_rn(w, kp, a);
+                    else return a + w * kp;
+                };
                 if constexpr (sizeof(T) == 4) {
                     if (deep) {
-                        // Taps t = -2, -1, 1, 2 along x, y, z; each tap's
-                        // pair is W at (x - t, x + 1 - t), rounded as the
-                        // general path below does (one fma per tap).
+                        // sum over the axes of (W(+2) - W(-2)) / 12 + (W(-1) - W(+1)) 2/3,
+                        // W(+t) the weight t voxels up the axis: the fourth-order
+                        // taps with the differences formed first, per axis
+                        // independent, for instruction-level parallelism.
+                        const float2 k12 = p_splat(FD<float>::one_twelfth), k23 = p_splat(FD<float>::two_thirds);
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
                             const T *px = wx + (c * TT_Y + ly) * XPX + 2 * tx + TMA_HX;
@@ -2210,62 +2238,97 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                             const T *py = wy + (c * YPY + ly + TMA_HY) * TXW + 2 * tx;
                             const float2 ym2 = ld_pair(py - 2 * TXW), ym1 = ld_pair(py - TXW);
                             const float2 yp1 = ld_pair(py + TXW), yp2 = ld_pair(py + 2 * TXW);
-                            float2 a2 = p_mul(xp, p_splat(kc[0]));
-                            a2 = p_fma(make_float2(xc.y, xp.x), p_splat(kc[1]), a2);
-                            a2 = p_fma(make_float2(xm.y, xc.x), p_splat(kc[2]), a2);
-                            a2 = p_fma(xm, p_splat(kc[3]), a2);
-                            a2 = p_fma(yp2, p_splat(kc[0]), a2);
-                            a2 = p_fma(yp1, p_splat(kc[1]), a2);
-                            a2 = p_fma(ym1, p_splat(kc[2]), a2);
-                            a2 = p_fma(ym2, p_splat(kc[3]), a2);
-                            a2 = p_fma(wq[r][c][4], p_splat(kc[0]), a2);
-                            a2 = p_fma(wq[r][c][3], p_splat(kc[1]), a2);
-                            a2 = p_fma(wq[r][c][1], p_splat(kc[2]), a2);
-                            a2 = p_fma(wq[r][c][0], p_splat(kc[3]), a2);
+                            const float2 d1x = make_float2(__fsub_rn(xm.y, xc.y), __fsub_rn(xc.x, xp.x));
+                            const float2 sx = p_fma(d1x, k23, p_mul(p_sub(xp, xm), k12));
+                            const float2 sy = p_fma(p_sub(ym1, yp1), k23, p_mul(p_sub(yp2, ym2), k12));
+                            const float2 sz = p_fma(p_sub(wq[r][c][1], wq[r][c][3]), k23,
+                                                    p_mul(p_sub(wq[r][c][4], wq[r][c][0]), k12));
+                            const float2 a2 = p_add(p_add(sx, sy), sz);
                             acc[0][c] = a2.x;
                             acc[1][c] = a2.y;
                         }
                     }
                 }
                 if (sizeof(T) != 4 || !deep) {
-                    // Per voxel and tap: the tap voxel p = q - t e_a differs
-                    // from q only along a, so the outer / penultimate flags of
-                    // the other axes come from q (src/jacobian.c:70-242).
 #pragma unroll
                     for (int v = 0; v < 2; ++v) {
-                        const int q3[3] = {x + v, y, ze};
-                        bool ob[3], pb[3];
-#pragma unroll
-                        for (int b = 0; b < 3; ++b) {
-                            ob[b] = q3[b] == 0 || q3[b] == n[b] - 1;
-                            pb[b] = q3[b] == 1 || q3[b] == n[b] - 2;
-                        }
                         T a3[3] = {T(0), T(0), T(0)};
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
-                            const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
+                        if (yz_deep) {
+                            // Only x can be outer or penultimate: the x taps
+                            // choose their schemes; the y and z taps are
+                            // fourth order, or second order when the voxel's
+                            // x is on the two outer layers (its tap voxels
+                            // share that x).  Same order as below.
+                            const int xv = x + v;
+                            const bool x_c2 = xv <= 1 || xv >= g.nx - 2;
 #pragma unroll
                             for (int t = -2; t <= 2; ++t) {
-                                const int pa = q3[a] - t;
-                                if (pa < 0 || pa >= n[a]) continue;
-                                const bool outer = o_other || pa == 0 || pa == n[a] - 1;
-                                const bool pen = p_other || pa == 1 || pa == n[a] - 2;
-                                const int kk = outer ? (pa == 0 ? S_FWD : (pa == n[a] - 1 ? S_BWD : S_C2))
-                                                     : (pen ? S_C2 : S_C4);
+                                const int pa = xv - t;
+                                if (pa < 0 || pa >= g.nx) continue;
+                                const int kk = pa == 0 ? S_FWD
+                                             : pa == g.nx - 1 ? S_BWD
+                                             : (pa == 1 || pa == g.nx - 2) ? S_C2 : S_C4;
                                 const T kp = kappa<T>(kk, t);
                                 if (kp == T(0)) continue;
 #pragma unroll
-                                for (int c = 0; c < 3; ++c) {
-                                    T w;
-                                    if (a == 0)
-                                        w = wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX];
-                                    else if (a == 1)
-                                        w = wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v];
-                                    else
-                                        w = v ? wq[r][c][2 - t].y : wq[r][c][2 - t].x;
-                                    if constexpr (sizeof(T) == 4) a3[c] = __fmaf_rn(w, kp, a3[c]);
-                                    else a3[c] = a3[c] + w * kp;
+                                for (int c = 0; c < 3; ++c)
+                                    a3[c] = acc_op(a3[c], wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX], kp);
+                            }
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) {
+                                const int t = i < 2 ? i - 2 : i - 1;
+                                if (x_c2 && (t == -2 || t == 2)) continue;
+                                const T kp = x_c2 ? kappa<T>(S_C2, t) : kc[i];
+#pragma unroll
+                                for (int c = 0; c < 3; ++c)
+                                    a3[c] = acc_op(a3[c], wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v], kp);
+                            }
+#pragma unroll
+                            for (int i = 0; i < 4; ++i) {
+                                const int t = i < 2 ? i - 2 : i - 1;
+                                if (x_c2 && (t == -2 || t == 2)) continue;
+                                const T kp = x_c2 ? kappa<T>(S_C2, t) : kc[i];
+#pragma unroll
+                                for (int c = 0; c < 3; ++c)
+                                    a3[c] = acc_op(a3[c], v ? wq[r][c][2 - t].y : wq[r][c][2 - t].x, kp);
+                            }
+                        } else {
+                            // Per tap: the tap voxel p = q - t e_a differs
+                            // from q only along a, so the outer / penultimate
+                            // flags of the other axes come from q
+                            // (src/jacobian.c:70-242).
+                            const int q3[3] = {x + v, y, ze};
+                            bool ob[3], pb[3];
+#pragma unroll
+                            for (int b = 0; b < 3; ++b) {
+                                ob[b] = q3[b] == 0 || q3[b] == n[b] - 1;
+                                pb[b] = q3[b] == 1 || q3[b] == n[b] - 2;
+                            }
+#pragma unroll
+                            for (int a = 0; a < 3; ++a) {
+                                const bool o_other = (a != 0 && ob[0]) || (a != 1 && ob[1]) || (a != 2 && ob[2]);
+                                const bool p_other = (a != 0 && pb[0]) || (a != 1 && pb[1]) || (a != 2 && pb[2]);
+#pragma unroll
+                                for (int t = -2; t <= 2; ++t) {
+                                    const int pa = q3[a] - t;
+                                    if (pa < 0 || pa >= n[a]) continue;
+                                    const bool outer = o_other || pa == 0 || pa == n[a] - 1;
+                                    const bool pen = p_other || pa == 1 || pa == n[a] - 2;
+                                    const int kk = outer ? (pa == 0 ? S_FWD : (pa == n[a] - 1 ? S_BWD : S_C2))
+                                                         : (pen ? S_C2 : S_C4);
+                                    const T kp = kappa<T>(kk, t);
+                                    if (kp == T(0)) continue;
+#pragma unroll
+                                    for (int c = 0; c < 3; ++c) {
+                                        T w;
+                                        if (a == 0)
+                                            w = wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX];
+                                        else if (a == 1)
+                                            w = wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v];
+                                        else
+                                            w = v ? wq[r][c][2 - t].y : wq[r][c][2 - t].x;
+                                        a3[c] = acc_op(a3[c], w, kp);
+                                    }
                                 }
                             }
                         }

@@ -80,6 +80,15 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z,
+                                            int a, int c) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(a), "r"(c), "r"(smem_u32(bar))
+        : "memory");
+}
+
 // Per-thread asynchronous copy of one 4- or 8-byte element from global to
 // shared memory (cp.async, L1-allocating), grouped by commit and awaited by
 // the issuing thread only.
