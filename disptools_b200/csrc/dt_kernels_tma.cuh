@@ -1902,6 +1902,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll
                     for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
         const bool tile_x_in = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3;
+        T wnext[RYT][2];  // adjoint weights: gJ of the next plane
+#pragma unroll
+        for (int r = 0; r < RYT; ++r) wnext[r][0] = wnext[r][1] = T(0);
         bool failed = false;
         int fail_it = 0;
         for (int it = 0; it < n_it; ++it) {
@@ -1921,6 +1924,28 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
             if (!mbar_wait_bounded(&bars[k % S], (k / S) & 1u)) s_fault = 1;
             const T *sb = reinterpret_cast<const T *>(smem + (k % S) * L::U_BYTES);
             const int q = z0 - 2 + it, ze = q - 2;
+            // Adjoint weights: this plane's gJ, loaded an iteration ahead,
+            // and the load of the next plane's.
+            T wcur[RYT][2];
+            if (ADJ) {
+#pragma unroll
+                for (int r = 0; r < RYT; ++r) {
+                    wcur[r][0] = wnext[r][0];
+                    wcur[r][1] = wnext[r][1];
+                    const int y = y0 + ty + r * TYT;
+                    if (ze + 1 >= z0 && ze + 1 < z1 && x < g.nx && y < g.ny) {
+                        const long long off = (ze + 1) * jzs + y * jys + x;
+                        if (pair_in) {
+                            const auto w2 = ld_pair(gJ + off);
+                            wnext[r][0] = w2.x;
+                            wnext[r][1] = w2.y;
+                        } else {
+                            wnext[r][0] = gJ[off];
+                            wnext[r][1] = T(0);
+                        }
+                    }
+                }
+            }
 #pragma unroll
             for (int r = 0; r < RYT; ++r) {
                 const int ly = ty + r * TYT + TMA_HY;
@@ -1946,25 +1971,24 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                 const bool row_in = plane_in && y >= 2 && y <= g.ny - 3;
                 const long long off = ze * jzs + y * jys + x;
                 if (ADJ) {
-                    T w[2];
-                    if (pair_in) {
-                        const auto w2 = ld_pair(gJ + off);
-                        w[0] = w2.x;
-                        w[1] = w2.y;
-                    } else {
-                        w[0] = gJ[off];
-                        w[1] = T(0);
-                    }
+                    const T w[2] = {wcur[r][0], wcur[r][1]};
                     T wv[9][2];
-                    stencil_pair<T, TMA_PX, TMA_PLANE>(
-                        jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in, tile_x_in,
-                        [&](int v, const T (&a)[3][3]) {
+                    // FP32 states every rounding (the scalar and the paired
+                    // epilogues give the same bits): a minor is a difference
+                    // of two products, and w * cof * ih is (w * minor) * (+-ih).
+                    auto weights = [&](int v, const T (&a)[3][3]) {
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) {
-                                const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+                        for (int c = 0; c < 3; ++c) {
+                            const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
 #pragma unroll
-                                for (int b = 0; b < 3; ++b) {
-                                    const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+                            for (int b = 0; b < 3; ++b) {
+                                const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+                                if constexpr (sizeof(T) == 4) {
+                                    auto m = [&](int i, int j) { return i == j ? __fadd_rn(a[i][j], 1.f) : a[i][j]; };
+                                    const float minor =
+                                        __fsub_rn(__fmul_rn(m(r0, c0), m(r1, c1)), __fmul_rn(m(r0, c1), m(r1, c0)));
+                                    wv[c * 3 + b][v] = __fmul_rn(__fmul_rn(w[v], minor), ((c + b) & 1) ? -ih[b] : ih[b]);
+                                } else {
                                     const T m00 = a[r0][c0] + (r0 == c0 ? T(1) : T(0));
                                     const T m11 = a[r1][c1] + (r1 == c1 ? T(1) : T(0));
                                     const T m01 = a[r0][c1] + (r0 == c1 ? T(1) : T(0));
@@ -1974,7 +1998,27 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                                     wv[c * 3 + b][v] = w[v] * cof * ih[b];
                                 }
                             }
-                        });
+                        }
+                    };
+                    auto weights2 = [&](const auto &a) {
+                        const float2 w2 = make_float2(w[0], w[1]);
+                        auto m = [&](int i, int j) { return i == j ? p_add(a[i][j], p_splat(1.f)) : a[i][j]; };
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+#pragma unroll
+                            for (int b = 0; b < 3; ++b) {
+                                const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+                                const float2 minor = p_sub(p_mul(m(r0, c0), m(r1, c1)), p_mul(m(r0, c1), m(r1, c0)));
+                                const float2 wq2 =
+                                    p_mul(p_mul(w2, minor), p_splat(((c + b) & 1) ? -ih[b] : ih[b]));
+                                wv[c * 3 + b][0] = wq2.x;
+                                wv[c * 3 + b][1] = wq2.y;
+                            }
+                        }
+                    };
+                    stencil_pair<T, TMA_PX, TMA_PLANE>(jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
+                                                       tile_x_in, weights, weights2);
 #pragma unroll
                     for (int k = 0; k < 9; ++k) {
                         if (pair_in)
@@ -2090,10 +2134,11 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
 // W[.][y] of its columns with two rows each side.  Each thread keeps its
 // pair's W[.][z] of planes ze-2 .. ze+2 in registers.  A stage is consumed
 // in its own iteration, so a block barrier every B planes is all that
-// guards reuse (loads run LA = S - B iterations ahead).  Pairs whose taps
-// all lie at fourth-order voxels (four or more voxels from every face) take
-// constant coefficients, in FP32 as pairs; the others choose each tap's
-// coefficient by the tap voxel's scheme.
+// guards reuse (loads run LA = S - B iterations ahead).  Warps whose pairs
+// all have their taps at fourth-order voxels (four or more voxels from
+// every face) take constant coefficients; warps near an x face take
+// per-lane coefficients for the x taps (both as FP32 pairs); the others
+// choose each tap's coefficient by the tap voxel's scheme.
 // ------------------------------------------------------------------------
 template <typename T, int TXW>
 struct GatherTmaLayout {
@@ -2208,24 +2253,29 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                     wq[r][c][4] = ld_pair(wz + (c * TT_Y + ly) * TXW + 2 * tx);
                 }
             }
-            if (ze < z0 || ze >= z1 || x >= g.nx) continue;
 #pragma unroll
             for (int r = 0; r < RYT; ++r) {
+                if (ze < z0 || ze >= z1) break;
                 const int ly = ty + r * TYT, y = y0 + ly;
-                if (y >= g.ny) continue;
+                const bool valid = x < g.nx && y < g.ny;
                 T acc[2][3];
-                // Three paths: the pair and all its taps at fourth-order
-                // voxels (four or more voxels from every face); y and z that
-                // deep but x near a face (only the x taps choose a scheme);
-                // the rest.  In FP32 the first runs on pairs.
+                // Three paths, chosen per warp (a warp is two rows of the
+                // tile, so a voxel's path depends on where it lies, not on the
+                // launch): every pair of the warp with all its taps at
+                // fourth-order voxels (four or more voxels from every face);
+                // y and z that deep but x near a face (only the x taps choose
+                // a scheme); the rest.  In FP32 the first two run on pairs.
                 const bool yz_deep = y >= 4 && y <= g.ny - 5 && ze >= 4 && ze <= g.nz - 5;
                 const bool deep = yz_deep && x >= 4 && x + 1 <= g.nx - 5;
+                const bool w_deep = __all_sync(0xffffffffu, deep || !valid);
+                const bool w_yz = __all_sync(0xffffffffu, yz_deep || !valid);
                 auto acc_op = [](T a, T w, T kp) -> T {
                     if constexpr (sizeof(T) == 4) return __fmaf_rn(w, kp, a);
                     else return a + w * kp;
                 };
+                bool done = false;
                 if constexpr (sizeof(T) == 4) {
-                    if (deep) {
+                    if (w_deep) {
                         // sum over the axes of (W(+2) - W(-2)) / 12 + (W(-1) - W(+1)) 2/3,
                         // W(+t) the weight t voxels up the axis: the fourth-order
                         // taps with the differences formed first, per axis
@@ -2247,13 +2297,67 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                             acc[0][c] = a2.x;
                             acc[1][c] = a2.y;
                         }
+                        done = true;
+                    } else if (w_yz) {
+                        // x near a face: per-lane coefficients of the x taps
+                        // (the tap voxel's scheme along x) and of the y and z
+                        // taps (second order when the voxel's x is on the two
+                        // outer layers), in the general path's tap order.
+                        float2 kx[5], kyz[4];
+#pragma unroll
+                        for (int i = 0; i < 5; ++i) {
+                            const int t = i - 2;
+                            float kv[2];
+#pragma unroll
+                            for (int v = 0; v < 2; ++v) {
+                                const int pa = x + v - t;
+                                const int kk = pa == 0 ? S_FWD
+                                             : pa == g.nx - 1 ? S_BWD
+                                             : (pa == 1 || pa == g.nx - 2) ? S_C2 : S_C4;
+                                kv[v] = pa < 0 || pa >= g.nx ? 0.f : kappa<float>(kk, t);
+                            }
+                            kx[i] = make_float2(kv[0], kv[1]);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const int t = i < 2 ? i - 2 : i - 1;
+                            float kv[2];
+#pragma unroll
+                            for (int v = 0; v < 2; ++v) {
+                                const bool x_c2 = x + v <= 1 || x + v >= g.nx - 2;
+                                kv[v] = x_c2 ? kappa<float>(S_C2, t) : kc[i];
+                            }
+                            kyz[i] = make_float2(kv[0], kv[1]);
+                        }
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const T *px = wx + (c * TT_Y + ly) * XPX + 2 * tx + TMA_HX;
+                            const float2 xm = ld_pair(px - 2), xc = ld_pair(px), xp = ld_pair(px + 2);
+                            const T *py = wy + (c * YPY + ly + TMA_HY) * TXW + 2 * tx;
+                            float2 a2 = p_mul(xp, kx[0]);
+                            a2 = p_fma(make_float2(xc.y, xp.x), kx[1], a2);
+                            a2 = p_fma(xc, kx[2], a2);
+                            a2 = p_fma(make_float2(xm.y, xc.x), kx[3], a2);
+                            a2 = p_fma(xm, kx[4], a2);
+                            a2 = p_fma(ld_pair(py + 2 * TXW), kyz[0], a2);
+                            a2 = p_fma(ld_pair(py + TXW), kyz[1], a2);
+                            a2 = p_fma(ld_pair(py - TXW), kyz[2], a2);
+                            a2 = p_fma(ld_pair(py - 2 * TXW), kyz[3], a2);
+                            a2 = p_fma(wq[r][c][4], kyz[0], a2);
+                            a2 = p_fma(wq[r][c][3], kyz[1], a2);
+                            a2 = p_fma(wq[r][c][1], kyz[2], a2);
+                            a2 = p_fma(wq[r][c][0], kyz[3], a2);
+                            acc[0][c] = a2.x;
+                            acc[1][c] = a2.y;
+                        }
+                        done = true;
                     }
                 }
-                if (sizeof(T) != 4 || !deep) {
+                if (!done) {
 #pragma unroll
                     for (int v = 0; v < 2; ++v) {
                         T a3[3] = {T(0), T(0), T(0)};
-                        if (yz_deep) {
+                        if (w_yz) {
                             // Only x can be outer or penultimate: the x taps
                             // choose their schemes; the y and z taps are
                             // fourth order, or second order when the voxel's
@@ -2336,6 +2440,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                         for (int c = 0; c < 3; ++c) acc[v][c] = a3[c];
                     }
                 }
+                if (!valid) continue;
                 T *o = gout + (long long) ze * g.zs + (long long) y * g.ys + x;
                 if (pair_in) {
 #pragma unroll
