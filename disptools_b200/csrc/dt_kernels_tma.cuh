@@ -235,14 +235,29 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vm, const T *v
             const T ddc = dd[c];
             V4 a = ld(ub + c * UP + o);
             T *pa = reinterpret_cast<T *>(&a);
+            // u + dd (v(+) - v(-)); FP32 as one fused multiply-add (in pairs
+            // when the whole run is formed), FP64 in the reference's order.
+            auto upd = [&](T u, T h, T l) -> T {
+                if constexpr (sizeof(T) == 4) return __fmaf_rn(ddc, __fsub_rn(h, l), u);
+                else return u + ddc * (h - l);
+            };
             if (all_in) {
+                if constexpr (sizeof(T) == 4) {
+                    const float2 dd2 = p_splat(ddc);
+                    const float2 a01 = p_fma(dd2, p_sub(make_float2(hi[0], hi[1]), make_float2(lo[0], lo[1])),
+                                             make_float2(pa[0], pa[1]));
+                    const float2 a23 = p_fma(dd2, p_sub(make_float2(hi[2], hi[3]), make_float2(lo[2], lo[3])),
+                                             make_float2(pa[2], pa[3]));
+                    a = make_float4(a01.x, a01.y, a23.x, a23.y);
+                } else {
 #pragma unroll
-                for (int e = 0; e < VEC; ++e) pa[e] = pa[e] + ddc * (hi[e] - lo[e]);
+                    for (int e = 0; e < VEC; ++e) pa[e] = upd(pa[e], hi[e], lo[e]);
+                }
             } else {
                 const V4 old = ld(out + c * UP + o);
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
-                    const T f = pa[e] + ddc * (hi[e] - lo[e]);
+                    const T f = upd(pa[e], hi[e], lo[e]);
                     pa[e] = (formed_m >> e) & 1u ? f : ((keep_m >> e) & 1u ? el(old, e) : pa[e]);
                 }
             }
@@ -264,6 +279,10 @@ __device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, 
     constexpr int CPR = PX / VEC, NPOS = TMA_PY * CPR;
     if (q < 0 || q >= g.nz) return;
     const bool q_in = q >= 1 && q <= g.nz - 2;
+    // A box of interior voxels only has no stale values.
+    if (q_in && x0 - TMA_HX >= 1 && x0 - TMA_HX + PX - 1 <= g.nx - 2 && y0 - TMA_HY >= 1 &&
+        y0 - TMA_HY + TMA_PY - 1 <= g.ny - 2)
+        return;
     // Runs counted from the last thread (the first threads' warp issues the
     // loads), the same mapping as greedy_form.
     for (int i = nth - 1 - tid; i < NPOS; i += nth) {
@@ -829,21 +848,32 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     }
 }
 
-// Block of TXW / 2 x TYT threads; each thread owns two adjacent columns
-// (x, x + 1) of TT_Y / TYT rows of the tile, so the field, e' and P-term
-// reads and the gradient stores are pairs.  Two resident blocks per SM for
+// Halo tasks of the gradient kernel's P terms per plane: x sides (one cell
+// each) and y sides (two cells each), one per thread of their own warps.
+template <int TXW>
+__host__ __device__ constexpr int grad_halo_rows() {
+    return (2 * TT_Y + TXW) / (TXW / 2);
+}
+
+// Block of TXW / 2 x (TYT + grad_halo_rows) threads.  The first TYT rows
+// own the tile: each thread two adjacent columns (x, x + 1) of TT_Y / TYT
+// rows, so the field, e' and P-term reads and the gradient stores are pairs.
+// The last rows compute the P terms of the tile's halo cells, so no warp
+// does halo work on top of its own cells.  Two resident blocks per SM for
 // FP32 (shared memory allows no more), one for FP64.
 template <typename T, int TXW, int TYT>
-__global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof(T) == 4) ? 2 : 1)
+__global__ void __launch_bounds__(TXW / 2 * (TYT + grad_halo_rows<TXW>()), sizeof(T) == 4 ? 2 : 1)
     k_gradient_tma(const VolumeDesc<T> *__restrict__ vols, const int *__restrict__ tile_vol, int total_tiles,
                    unsigned char *__restrict__ work_flag, TileQueue *queue, int pf) {
     using L = GradTmaLayout<T, TXW>;
-    constexpr int TPX = TXW / 2, NTH = TPX * TYT, RYT = TT_Y / TYT;
+    constexpr int TPX = TXW / 2, RYT = TT_Y / TYT;
+    constexpr int NHALO = 2 * TT_Y + TXW;  // halo tasks: x sides (one cell each), y sides (two cells each)
+    constexpr int NOWN = TPX * TYT, NTH = NOWN + NHALO;
     constexpr int TMA_PX = L::TMA_PX, TMA_PLANE = L::TMA_PLANE;
     constexpr int PXP = L::PXP, PYP = L::PYP;
-    constexpr int NHALO = 2 * TT_Y + TXW;  // halo threads: x sides (one cell each), y sides (two cells each)
     static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
-    static_assert(NHALO <= NTH, "halo threads");
+    static_assert(NHALO % TPX == 0 && NHALO / TPX == grad_halo_rows<TXW>(), "whole halo rows");
+    static_assert(NOWN % 32 == 0, "owner and halo threads in separate warps");
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     unsigned char *smem = align_smem_128(smem_dyn);
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + L::BAR_OFF);
@@ -856,6 +886,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
     auto PT = [&](int slot, int t, int r, int c) -> T * { return pxy + ((slot * 6 + t) * PYP + r) * PXP + c; };
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TPX + tx;
+    const bool own = ty < TYT;  // owner threads (the others: halo tasks)
     if (tid == 0) {
         for (int s = 0; s < L::S; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -1027,6 +1058,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 auto st2 = [](T *p, P2 v) { *reinterpret_cast<P2 *>(p) = v; };
 #pragma unroll
                 for (int r = 0; r < RYT; ++r) {  // own cells: all nine terms (P_z in registers)
+                    if (!own) break;
                     const int ly = ty + r * TYT + TMA_HY, rp = ty + r * TYT + 1;
                     if constexpr (sizeof(T) == 4) {
                         float2 M[3][3];
@@ -1050,10 +1082,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                         }
                     }
                 }
-                // Halo cells, on the last threads of the block (thread 0
-                // issues the loads): P_x on the two side columns, P_y on the
-                // two end rows (pairs).
-                const int h = tid - (NTH - NHALO);
+                // Halo cells, on the halo threads: P_x on the two side
+                // columns, P_y on the two end rows (pairs).
+                const int h = tid - NOWN;
                 if (h >= 0 && h < 2 * TT_Y) {
                     const int side = h / TT_Y, row = h % TT_Y;
                     const int c = side ? TXW + 2 : 1;
@@ -1095,7 +1126,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             }
             if (tid == 0 && it >= 2 && it - 2 + L::S < n_it) issue(it - 2 + L::S);
             const int z = q - 2;  // gradient plane: P(z-1), P(z), P(z+1) ready
-            if (it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x < g.nx - 1 && x + 1 >= 1) {
+            if (own && it >= 3 && z >= z0 && z < z1 && z >= 1 && z < g.nz - 1 && x < g.nx - 1 && x + 1 >= 1) {
                 const int ps = ring_slot(z, L::NP);
                 const bool in0 = x >= 1, in1 = x + 1 < g.nx - 1;
 #pragma unroll
@@ -1691,8 +1722,8 @@ cudaError_t launch_gradient_tma_v(const VolumeDesc<T> *vols, const int *tile_vol
     static std::atomic<unsigned long long> devs{0};
     const cudaError_t attr = opt_in_smem(k_gradient_tma<T, TXW, TYT>, smem, devs);
     if (attr != cudaSuccess) return attr;
-    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(vols, tile_vol, total_tiles, work_flag,
-                                                                       queue, pf);
+    k_gradient_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT + grad_halo_rows<TXW>()), smem, s>>>(
+        vols, tile_vol, total_tiles, work_flag, queue, pf);
     count_launch();
     return cudaGetLastError();
 }
@@ -1727,7 +1758,8 @@ int gradient_blocks_v() {
         int v = 0;
         cudaFuncSetAttribute(k_gradient_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              GradTmaLayout<T, TXW>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T, TXW, TYT>, TXW / 2 * TYT,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gradient_tma<T, TXW, TYT>,
+                                                      TXW / 2 * (TYT + grad_halo_rows<TXW>()),
                                                       GradTmaLayout<T, TXW>::BYTES + 128);
         return v;
     }();
