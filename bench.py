@@ -547,11 +547,17 @@ def run_c3(args, world, rank, local, quiet=False):
     hbm, peak_kind = peaks()
     achieved = 16.0 * nvox / (fwd_ms / 1000.0) / 1e9
     traffic = None  # DRAM bytes of one launch (one field), from the committed ncu capture
+    bwd_traffic = None  # the backward's two passes, per field
     try:
-        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["jacobian_c3_field"][
-            "bytes_per_launch"]
+        tj = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        traffic = tj["jacobian_c3_field"]["bytes_per_launch"]
+        bwd_traffic = tj["adjoint_c3_field"]["weight_pass_bytes_per_launch"] + tj["adjoint_c3_field"][
+            "gather_bytes_per_launch"]
     except Exception:
-        traffic = None
+        pass
+    # The backward at the adjoint's algorithmic bytes: field 12 and gJ 4 in,
+    # gradient 12 out per voxel (one fused pass would move just these).
+    bwd_achieved = 28.0 * nvox / (bwd_ms / 1000.0) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -578,7 +584,10 @@ def run_c3(args, world, rank, local, quiet=False):
         "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                      "peak_source": peak_kind, "bytes_per_voxel": 16,
-                     "bytes_per_launch": 16 * nvox // B, "avg_launch_ms": fwd_ms / B},
+                     "bytes_per_launch": 16 * nvox // B, "avg_launch_ms": fwd_ms / B,
+                     "backward": {"kernels": "k_jacobian_tma (weights) + k_gather_tma", "bytes_per_voxel": 28,
+                                  "achieved": bwd_achieved, "frac": bwd_achieved / hbm,
+                                  "traffic_per_field": bwd_traffic, "ms_per_field": bwd_ms / B}},
         "cpu_baseline": cpu,
         "e2e": None,
         "gpu_launches": launches, "clocks": clk.summary(),
