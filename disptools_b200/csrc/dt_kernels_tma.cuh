@@ -309,7 +309,7 @@ __device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, 
 // plane ze, each handed to finish(v, a) when the voxel lies in the volume.
 // `jp` is the plane's field box in shared memory ([3][TMA_PY][PX], column lx
 // holds x, row ly holds y); zq holds the two columns' values of planes
-// ze-2 .. ze+2 per component.  FP32 folds the spacing into the fourth-order
+// ze-2 .. ze+2 per component as pairs (x, x + 1).  FP32 folds the spacing into the fourth-order
 // weights; the FP64 path keeps the reference's operation order.  Three
 // evaluators:
 // * rows and planes inside [2, n-3] of a tile whose columns all lie inside
@@ -322,7 +322,8 @@ __device__ __forceinline__ void greedy_prefetch_stale(T *out, int tid, int nth, 
 // `finish2` functor (not null) takes the first evaluator's two matrices at
 // once, as pairs (x, x + 1) of each entry.
 template <typename T, int TMA_PX, int TMA_PLANE, typename F, typename F2 = std::nullptr_t>
-__device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5], int lx, int ly, int x, int y,
+__device__ __forceinline__ void stencil_pair(const typename PairOf<T>::type (&zq)[3][5], const T *jp, int lx,
+                                             int ly, int x, int y,
                                              int ze, const Geom &g, const T (&ih)[3], bool row_in,
                                              bool tile_x_in, F &&finish, F2 &&finish2 = nullptr) {
     const T k1[3] = {FD<T>::two_thirds * ih[0], FD<T>::two_thirds * ih[1], FD<T>::two_thirds * ih[2]};
@@ -344,10 +345,7 @@ __device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5]
                 const float2 ym1 = ld_pair(p - TMA_PX), yp1 = ld_pair(p + TMA_PX);
                 const float2 ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
                 a[c][1] = c4_folded2(yp1, ym1, yp2, ym2, p_splat(k1[1]), p_splat(k2n[1]));
-                const T *z0q = zq[0][c], *z1q = zq[1][c];
-                a[c][2] = c4_folded2(make_float2(z0q[3], z1q[3]), make_float2(z0q[1], z1q[1]),
-                                     make_float2(z0q[4], z1q[4]), make_float2(z0q[0], z1q[0]), p_splat(k1[2]),
-                                     p_splat(k2n[2]));
+                a[c][2] = c4_folded2(zq[c][3], zq[c][1], zq[c][4], zq[c][0], p_splat(k1[2]), p_splat(k2n[2]));
             }
             finish2(a);
             return;
@@ -365,9 +363,8 @@ __device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5]
             const auto ym2 = ld_pair(p - 2 * TMA_PX), yp2 = ld_pair(p + 2 * TMA_PX);
             a0[c][1] = c4(yp1.x, ym1.x, yp2.x, ym2.x, 1);
             a1[c][1] = c4(yp1.y, ym1.y, yp2.y, ym2.y, 1);
-            const T *z0q = zq[0][c], *z1q = zq[1][c];
-            a0[c][2] = c4(z0q[3], z0q[1], z0q[4], z0q[0], 2);
-            a1[c][2] = c4(z1q[3], z1q[1], z1q[4], z1q[0], 2);
+            a0[c][2] = c4(zq[c][3].x, zq[c][1].x, zq[c][4].x, zq[c][0].x, 2);
+            a1[c][2] = c4(zq[c][3].y, zq[c][1].y, zq[c][4].y, zq[c][0].y, 2);
         }
         finish(0, a0);
         finish(1, a1);
@@ -394,7 +391,9 @@ __device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5]
                 const T cy4 = c4(p[TMA_PX], p[-TMA_PX], p[2 * TMA_PX], p[-2 * TMA_PX], 1);
                 const T cy2 = fd_c2<T>(p[TMA_PX], p[-TMA_PX], ih[1]);
                 a[c][1] = second ? cy2 : cy4;
-                const T *zv = zq[v][c];
+                T zv[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) zv[k] = v ? zq[c][k].y : zq[c][k].x;
                 const T cz4 = c4(zv[3], zv[1], zv[4], zv[0], 2);
                 const T cz2 = fd_c2<T>(zv[3], zv[1], ih[2]);
                 a[c][2] = second ? cz2 : cz4;
@@ -416,7 +415,10 @@ __device__ __forceinline__ void stencil_pair(const T *jp, const T (&zq)[2][3][5]
                 const T vy[5] = {p[-2 * TMA_PX], p[-TMA_PX], p[0], p[TMA_PX], p[2 * TMA_PX]};
 #pragma unroll
                 for (int ax = 0; ax < 3; ++ax) {
-                    const T *w = ax == 0 ? vx : (ax == 1 ? vy : zq[v][c]);
+                    T vz[5];
+#pragma unroll
+                    for (int k = 0; k < 5; ++k) vz[k] = v ? zq[c][k].y : zq[c][k].x;
+                    const T *w = ax == 0 ? vx : (ax == 1 ? vy : vz);
                     T d;
                     switch (kk[ax]) {
                     case S_FWD: d = fd_fwd<T>(w[2], w[3], w[4], ih[ax]); break;
@@ -1924,15 +1926,15 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
         const int x = x0 + 2 * tx;       // this thread's columns: x, x + 1
         const int lx = 2 * tx + TMA_HX;  // their box column
         const bool pair_in = x + 1 < g.nx;
-        T zq[RYT][2][3][5];
+        // Own columns (x, x + 1 as one pair): field values of planes ze-2 .. ze+2.
+        using P2 = typename PairOf<T>::type;
+        P2 zq[RYT][3][5];
 #pragma unroll
         for (int r = 0; r < RYT; ++r)
 #pragma unroll
-            for (int v = 0; v < 2; ++v)
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int k = 0; k < 5; ++k) zq[r][v][c][k] = T(0);
+                for (int k = 0; k < 5; ++k) zq[r][c][k] = P2{T(0), T(0)};
         const bool tile_x_in = x0 >= 2 && x0 + TXW - 1 <= g.nx - 3;
         T wnext[RYT][2];  // adjoint weights: gJ of the next plane
 #pragma unroll
@@ -1983,14 +1985,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                 const int ly = ty + r * TYT + TMA_HY;
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const auto nv = ld_pair(sb + c * TMA_PLANE + ly * TMA_PX + lx);
 #pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) {
-                        zq[r][0][c][kk] = zq[r][0][c][kk + 1];
-                        zq[r][1][c][kk] = zq[r][1][c][kk + 1];
-                    }
-                    zq[r][0][c][4] = nv.x;
-                    zq[r][1][c][4] = nv.y;
+                    for (int kk = 0; kk < 4; ++kk) zq[r][c][kk] = zq[r][c][kk + 1];
+                    zq[r][c][4] = ld_pair(sb + c * TMA_PLANE + ly * TMA_PX + lx);
                 }
             }
             if (ze < z0 || ze >= z1) continue;
@@ -2049,7 +2046,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                             }
                         }
                     };
-                    stencil_pair<T, TMA_PX, TMA_PLANE>(jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
+                    stencil_pair<T, TMA_PX, TMA_PLANE>(zq[r], jp, lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in,
                                                        tile_x_in, weights, weights2);
 #pragma unroll
                     for (int k = 0; k < 9; ++k) {
@@ -2066,7 +2063,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                         jv[1] = J.y;
                     };
                     stencil_pair<T, TMA_PX, TMA_PLANE>(
-                        jp, zq[r], lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in, tile_x_in,
+                        zq[r], jp, lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in, tile_x_in,
                         [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); }, det2);
                     T *o = jout + off;
                     if (pair_in)
