@@ -2180,8 +2180,8 @@ struct GatherTmaLayout {
     static constexpr int Y_OFF = X_ELEMS * (int) sizeof(T);
     static constexpr int Z_OFF = Y_OFF + Y_ELEMS * (int) sizeof(T);
     static constexpr int STAGE_BYTES = (Z_OFF + Z_ELEMS * (int) sizeof(T) + 127) / 128 * 128;
-    static constexpr int S = sizeof(T) == 4 ? 5 : 4;  // 105 KB (FP32, two blocks per SM), 168 KB (FP64)
-    static constexpr int B = 2;                       // planes between block barriers
+    static constexpr int S = sizeof(T) == 4 ? 3 : 4;  // 63 KB (FP32, three blocks per SM), 168 KB (FP64)
+    static constexpr int B = sizeof(T) == 4 ? 1 : 2;  // planes between block barriers
     static constexpr int LA = S - B;                  // load distance
     static constexpr int BAR_OFF = S * STAGE_BYTES;
     static constexpr int BYTES = BAR_OFF + S * 8;
@@ -2189,7 +2189,7 @@ struct GatherTmaLayout {
 };
 
 template <typename T, int TXW, int TYT>
-__global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
     k_gather_tma(const __grid_constant__ CUtensorMap tm_wx, const __grid_constant__ CUtensorMap tm_wy,
                  const __grid_constant__ CUtensorMap tm_wz, const Geom g, T *__restrict__ gout, int tiles_x,
                  int tiles_y, int ntiles, int bz) {
