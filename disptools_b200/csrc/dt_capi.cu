@@ -719,6 +719,10 @@ int solve_device_on(Engine *e, int algorithm, const std::vector<DevVol<T>> &vols
     for (int i = 0; i < count; ++i) {
         d_states[i] = desc[i].st;
         DTB_CUDA(cudaMemcpyAsync(desc[i].st, &hst[i], sizeof(SolverState), cudaMemcpyHostToDevice, stream));
+        // Greedy method: whether the trial must copy the new buffer's
+        // boundary values (they are all +0 unless the initial field's are not).
+        if (!gradient && !tune_ms)
+            DTB_CUDA(launch_boundary_nonzero<T>(desc[i].field[0], desc[i].g, &desc[i].st->b0_nonzero, stream));
     }
     DTB_CUDA(cudaMemcpyAsync(d_desc, desc.data(), count * sizeof(VolumeDesc<T>), cudaMemcpyHostToDevice, stream));
     DTB_CUDA(cudaMemcpyAsync(d_tile_vol, tile_vol.data(), total_tiles * sizeof(int), cudaMemcpyHostToDevice,

@@ -60,6 +60,10 @@ struct SolverState {
     int reason;
     int old_buf;             // which field buffer holds the accepted field
     int need_gradient;
+    // Greedy method: some boundary voxel of the initial field (buffer 0) is
+    // not +0 (bitwise).  Buffer 1 starts zeroed, and no buffer's boundary
+    // voxels are ever changed, so otherwise every boundary value is +0.
+    int b0_nonzero;
     int v_cur;               // greedy: which error map is the current one
     unsigned int ticket_t;   // block counters of the trial / gradient launches
     unsigned int ticket_g;
@@ -191,6 +195,10 @@ template <typename T>
 cudaError_t launch_to_double(const T *src, double *dst, long long n, cudaStream_t s);
 template <typename T>
 cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s);
+// Sets *flag = 1 if a boundary voxel of the field [3][nz][ny][nx] (strides
+// of g) is not +0 bitwise; leaves it otherwise.
+template <typename T>
+cudaError_t launch_boundary_nonzero(const T *field, const Geom &g, int *flag, cudaStream_t s);
 
 // Kernel-launch counter (host side).  Launches issued while a stream is being
 // captured are not counted; each replay of a graph counts its kernels.

@@ -643,6 +643,31 @@ cudaError_t launch_adjoint(const Geom &g, const T *field, const T *gJ, T *W, lon
     return cudaGetLastError();
 }
 
+// One thread per (row y, plane z, component): the row's two end voxels, and
+// the whole row on the y and z faces.
+template <typename T>
+__global__ void k_boundary_nonzero(const T *__restrict__ f, Geom g, int *flag) {
+    using U = typename std::conditional<sizeof(T) == 4, unsigned int, unsigned long long>::type;
+    const long long rows = 3ll * g.ny * g.nz;
+    for (long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < rows;
+         i += (long long) gridDim.x * blockDim.x) {
+        const int y = (int) (i % g.ny), z = (int) ((i / g.ny) % g.nz), c = (int) (i / ((long long) g.ny * g.nz));
+        const U *row = reinterpret_cast<const U *>(f + c * g.cs + (long long) z * g.zs + (long long) y * g.ys);
+        U any = row[0] | row[g.nx - 1];
+        if (y == 0 || y == g.ny - 1 || z == 0 || z == g.nz - 1)
+            for (int x = 1; x < g.nx - 1; ++x) any |= row[x];
+        if (any) *flag = 1;
+    }
+}
+
+template <typename T>
+cudaError_t launch_boundary_nonzero(const T *field, const Geom &g, int *flag, cudaStream_t s) {
+    const long long rows = 3ll * g.ny * g.nz;
+    k_boundary_nonzero<T><<<elementwise_grid(rows), 256, 0, s>>>(field, g, flag);
+    count_launch();
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_convert(const void *src, int src_is_double, T *dst, long long n, cudaStream_t s) {
     k_convert<T><<<elementwise_grid(n), 256, 0, s>>>(src, src_is_double, dst, n);
@@ -670,6 +695,7 @@ cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s) {
                                            cudaStream_t);                                                    \
     template cudaError_t launch_convert<T>(const void *, int, T *, long long, cudaStream_t);                 \
     template cudaError_t launch_to_double<T>(const T *, double *, long long, cudaStream_t);                  \
-    template cudaError_t launch_regularise<T>(T *, long long, double, cudaStream_t);
+    template cudaError_t launch_regularise<T>(T *, long long, double, cudaStream_t);                        \
+    template cudaError_t launch_boundary_nonzero<T>(const T *, const Geom &, int *, cudaStream_t);
 
 }  // namespace dtb

@@ -170,7 +170,8 @@ using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 //   (src/displacement_field_greedy.c:30-63, same operation order);
 // * other voxels of the volume: the new field buffer's own content, which
 //   greedy_prefetch_stale has already copied into `out` (the caller waits
-//   for its own copies first);
+//   for its own copies first), or +0 when `stale_zero` says that content is
+//   +0 everywhere on the boundary;
 // * outside the volume: 0 (the field box arrives zero-filled there).
 // `vm`, `vc`, `vn` are the error map's planes q-1, q, q+1, rows
 // y0-3 .. y0+TT_Y+2, columns as in the field box.  A thread forms the three components of one
@@ -180,7 +181,8 @@ using Vec16 = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
 // and last columns lack an x neighbour; no stencil reads them.
 template <typename T, typename L>
 __device__ __forceinline__ void greedy_form(const T *ub, const T *vm, const T *vc, const T *vn, T *out, int tid,
-                                            int nth, const Geom &g, int x0, int y0, int q, const T *dd) {
+                                            int nth, const Geom &g, int x0, int y0, int q, const T *dd,
+                                            bool stale_zero) {
     using V4 = Vec16<T>;
     constexpr int VEC = 16 / (int) sizeof(T);
     constexpr int PX = L::TMA_PX, UP = L::TMA_PLANE;
@@ -254,7 +256,14 @@ __device__ __forceinline__ void greedy_form(const T *ub, const T *vm, const T *v
                     for (int e = 0; e < VEC; ++e) pa[e] = upd(pa[e], hi[e], lo[e]);
                 }
             } else {
-                const V4 old = ld(out + c * UP + o);
+                V4 old;
+                if (stale_zero) {
+                    T *po = reinterpret_cast<T *>(&old);
+#pragma unroll
+                    for (int e = 0; e < VEC; ++e) po[e] = T(0);
+                } else {
+                    old = ld(out + c * UP + o);
+                }
 #pragma unroll
                 for (int e = 0; e < VEC; ++e) {
                     const T f = upd(pa[e], hi[e], lo[e]);
@@ -485,6 +494,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         const int phase = ldcg_int(&st->phase);
         const int old_b = ldcg_int(&st->old_buf);
         const int v_cur = GREEDY ? ldcg_int(&st->v_cur) : 0;
+        // Greedy: the new buffer's boundary values are all +0 when it is
+        // buffer 1 or the initial field's boundary is; no copies then.
+        const bool stale_zero = GREEDY && (old_b == 0 || !ldcg_int(&st->b0_nonzero));
         const double eta = __ldcg(&st->eta);
         const bool trial = phase != PH_EVAL0;
         const int lt = tile - V.tile_begin;
@@ -576,7 +588,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
         long long qoff = (long long) (z0 - 2) * g.zs;  // offset of plane q
         // Greedy trial: stale boundary values of the first candidate plane
         // (its ring slot is free: the tile queue's barrier has passed).
-        if (GREEDY && trial)
+        if (GREEDY && trial && !stale_zero)
             greedy_prefetch_stale<T, L>(ring + (size_t) ((z0 - 2) & (L::R - 1)) * 3 * TMA_PLANE, tid, NTH, g, x0, y0,
                                         z0 - 2, dst);
         for (int it = 0; it < n_it; ++it, qoff += g.zs) {
@@ -598,12 +610,12 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
                 const V4 *g4 = reinterpret_cast<const V4 *>(sb + L::U_BYTES);
                 V4 *c4 = reinterpret_cast<V4 *>(slot);
                 if (GREEDY && trial) {
-                    cp_async_wait_all();  // this thread's stale values of plane q
+                    if (!stale_zero) cp_async_wait_all();  // this thread's stale values of plane q
                     auto vplane = [&](int p) -> const T * {
                         return vring + ((vbase + (uint32_t) (p - z0 + 3)) % L::RV) * (L::V_SLOT / sizeof(T));
                     };
                     greedy_form<T, L>(reinterpret_cast<const T *>(sb), vplane(q - 1), vplane(q), vplane(q + 1), slot,
-                                      tid, NTH, g, x0, y0, q, s_dd);
+                                      tid, NTH, g, x0, y0, q, s_dd, stale_zero);
                 } else
                 // Counted from the last thread: the runs left over after
                 // whole sweeps go to the last warps, not to warp 0, whose
@@ -647,7 +659,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, (TXW / 2 * TYT <= 256 && sizeof
             // Greedy trial: stale boundary values of plane q+1, into its ring
             // slot, which held plane q-3: every warp has finished reading it
             // (the stencil of the previous iteration) at the barrier above.
-            if (GREEDY && trial && it + 1 < n_it)
+            if (GREEDY && trial && !stale_zero && it + 1 < n_it)
                 greedy_prefetch_stale<T, L>(ring + (size_t) ((q + 1) & (L::R - 1)) * 3 * TMA_PLANE, tid, NTH, g, x0,
                                             y0, q + 1, dst);
             // Shift the own-column queues by plane q; store the candidate.
