@@ -128,6 +128,30 @@ def test_batched_equals_single_release_kernel(monkeypatch, precision):
     test_batched_equals_single(precision, "gradient")
 
 
+@pytest.mark.parametrize("boundary", ["zero", "negative_zero", "one_voxel"])
+def test_greedy_boundary_values_fp64_vs_oracle(oracle, boundary):
+    """The greedy trial skips copying the new buffer's boundary values when
+    they are all +0: an initial field that is zero on the boundary (the
+    copies skipped in both buffers), -0.0 there (bitwise not +0: copied), or
+    zero but for one boundary voxel (copied while buffer 0 is the new
+    buffer).  Each must equal the oracle bit for bit."""
+    shape = (37, 45, 70)
+    rng = np.random.default_rng(23)
+    Jt = np.ascontiguousarray(1.0 + 0.08 * rng.standard_normal(shape))
+    mask = np.ascontiguousarray(rng.random(shape) < 0.5)
+    f0 = rng.normal(scale=0.02, size=(3,) + shape)
+    inner = np.zeros(shape, bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    f0[:, ~inner] = -0.0 if boundary == "negative_zero" else 0.0
+    if boundary == "one_voxel":
+        f0[1, 0, 20, 30] = 0.05
+    ref, so = oracle.solve("greedy", Jt, mask, field=f0, it_max=25)
+    out, st = dt.solve(Jt, mask, f0, algorithm="greedy", precision="fp64", it_max=25)
+    assert st["reason"] == so.reason and st["iterations"] == so.iterations, (st, so)
+    assert st["trials"] == so.trials
+    assert np.max(np.abs(out - ref)) <= 1e-12
+
+
 @pytest.mark.parametrize("shape", [(37, 45, 70), (70, 18, 33), (9, 40, 131)])
 def test_greedy_multi_tile_fp64_vs_oracle(oracle, shape):
     """Greedy trials over several tiles along every axis, x extents that end
