@@ -60,17 +60,18 @@ def test_adjoint_fp64_vs_finite_differences(shape):
     np.testing.assert_allclose(got, fd, rtol=1e-6, atol=1e-7)
 
 
+@pytest.mark.parametrize("shape", [(21, 40, 68), (96, 112, 100)])
 @pytest.mark.parametrize("dtype", ["float64", "float32"])
-def test_adjoint_tma_and_plain_paths_agree(dtype):
-    """The weight pass on the TMA stencil kernel (aligned field) and on the
-    plain-load kernel (a field 8 bytes off a 16-byte boundary) give the same
-    gradient: several tiles per axis and a deep interior for the gather's
-    constant-weight path."""
+def test_adjoint_tma_and_plain_paths_agree(dtype, shape):
+    """The TMA passes (aligned field: weight pass on the TMA stencil kernel,
+    TMA gather) and the plain-load passes (a field 8 bytes off a 16-byte
+    boundary) give the same gradient on every voxel: several tiles per axis,
+    tiles on every face (the gather's x-face and general paths) and a deep
+    interior (its fourth-order path); bit for bit in FP64."""
     import torch
     from disptools_b200 import torch_ops
     from disptools_b200.synthetic import smooth_field
     tdt = getattr(torch, dtype)
-    shape = (21, 40, 68)
     f = torch.from_numpy(smooth_field(shape, sigma=3.0, max_disp=1.5, seed=4)).to(tdt).cuda()
     rng = np.random.default_rng(5)
     w = torch.from_numpy(rng.standard_normal(shape)).to(tdt).cuda()
