@@ -157,6 +157,116 @@ __global__ void k_recursive_axis(const T *__restrict__ in, T *__restrict__ out, 
     }
 }
 
+// The x axis of the recursive Gaussian with coalesced memory access.  A warp
+// owns 32 consecutive lines and moves them through shared memory in chunks
+// of 32 samples: it loads and stores 32 consecutive samples of one line at a
+// time, and each lane runs its own line's recursion over the chunk, with the
+// order and roundings of k_recursive_axis (the results are the same bits).
+constexpr int RX_W = 32, RX_P = RX_W + 1, RX_WARPS = 2;
+
+template <typename T>
+__global__ void __launch_bounds__(32 * RX_WARPS) k_recursive_x(const T *__restrict__ in, T *__restrict__ out, int nx,
+                                                               long long lines, Recursive rc) {
+    __shared__ T tiles[RX_WARPS][2][RX_W * RX_P];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T *tx = tiles[warp][0];  // input samples, [line][sample]
+    T *ty = tiles[warp][1];  // output samples
+    const int nchunks = (nx + RX_W - 1) / RX_W;
+    // Moves chunk c0 .. c0+cn-1 of the warp's lines between global and shared memory.
+    auto load = [&](T *tile, const T *src, long long l0, int c0, int cn) {
+#pragma unroll 4
+        for (int j = 0; j < RX_W; ++j)
+            if (l0 + j < lines && lane < cn) tile[j * RX_P + lane] = src[(l0 + j) * nx + c0 + lane];
+    };
+    auto store = [&](const T *tile, long long l0, int c0, int cn) {
+#pragma unroll 4
+        for (int j = 0; j < RX_W; ++j)
+            if (l0 + j < lines && lane < cn) out[(l0 + j) * nx + c0 + lane] = tile[j * RX_P + lane];
+    };
+    for (long long l0 = ((long long) blockIdx.x * RX_WARPS + warp) * RX_W; l0 < lines;
+         l0 += (long long) gridDim.x * RX_WARPS * RX_W) {
+        const long long line = l0 + lane;
+        const bool live = line < lines;
+        const T *row = in + (live ? line : 0) * nx;
+        T *my_x = tx + lane * RX_P, *my_y = ty + lane * RX_P;
+        if (!rc.on) {
+            for (int c0 = 0; c0 < nx; c0 += RX_W) {
+                const int cn = min(RX_W, nx - c0);
+                load(tx, in, l0, c0, cn);
+                __syncwarp();
+                store(tx, l0, c0, cn);
+                __syncwarp();
+            }
+            continue;
+        }
+        // Anticausal pass, chunks right to left, stored in the output.
+        const double xe = live ? (double) row[nx - 1] : 0.0;
+        double xn0 = xe, xn1 = xe, xn2 = xe, xn3 = xe;
+        double yn0 = __dmul_rn(xe, rc.ga), yn1 = yn0, yn2 = yn0, yn3 = yn0;
+        for (int ch = nchunks - 1; ch >= 0; --ch) {
+            const int c0 = ch * RX_W, cn = min(RX_W, nx - c0);
+            load(tx, in, l0, c0, cn);
+            __syncwarp();
+            if (live)
+                for (int i = cn - 1; i >= 0; --i) {
+                    double acc = __dmul_rn(rc.m[0], xn0);
+                    acc = __dadd_rn(acc, __dmul_rn(rc.m[1], xn1));
+                    acc = __dadd_rn(acc, __dmul_rn(rc.m[2], xn2));
+                    acc = __dadd_rn(acc, __dmul_rn(rc.m[3], xn3));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[0], yn0));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[1], yn1));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[2], yn2));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[3], yn3));
+                    my_y[i] = (T) acc;
+                    xn3 = xn2;
+                    xn2 = xn1;
+                    xn1 = xn0;
+                    xn0 = (double) my_x[i];
+                    yn3 = yn2;
+                    yn2 = yn1;
+                    yn1 = yn0;
+                    yn0 = acc;
+                }
+            __syncwarp();
+            store(ty, l0, c0, cn);
+            __syncwarp();
+        }
+        // Causal pass, chunks left to right, added to the stored anticausal part.
+        const double x0 = live ? (double) row[0] : 0.0;
+        double xp0 = x0, xp1 = x0, xp2 = x0;
+        double yp0 = __dmul_rn(x0, rc.gc), yp1 = yp0, yp2 = yp0, yp3 = yp0;
+        for (int ch = 0; ch < nchunks; ++ch) {
+            const int c0 = ch * RX_W, cn = min(RX_W, nx - c0);
+            load(tx, in, l0, c0, cn);
+            load(ty, out, l0, c0, cn);
+            __syncwarp();
+            if (live)
+                for (int i = 0; i < cn; ++i) {
+                    const double xi = (double) my_x[i];
+                    double acc = __dmul_rn(rc.n[0], xi);
+                    acc = __dadd_rn(acc, __dmul_rn(rc.n[1], xp0));
+                    acc = __dadd_rn(acc, __dmul_rn(rc.n[2], xp1));
+                    acc = __dadd_rn(acc, __dmul_rn(rc.n[3], xp2));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[0], yp0));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[1], yp1));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[2], yp2));
+                    acc = __dsub_rn(acc, __dmul_rn(rc.d[3], yp3));
+                    my_y[i] = (T) __dadd_rn(acc, (double) my_y[i]);
+                    xp2 = xp1;
+                    xp1 = xp0;
+                    xp0 = xi;
+                    yp3 = yp2;
+                    yp2 = yp1;
+                    yp1 = yp0;
+                    yp0 = acc;
+                }
+            __syncwarp();
+            store(ty, l0, c0, cn);
+            __syncwarp();
+        }
+    }
+}
+
 __device__ __forceinline__ double lerp_rn(double a, double b, double f) {
     return __dadd_rn(a, __dmul_rn(__dsub_rn(b, a), f));
 }
@@ -290,7 +400,10 @@ template <typename T>
 cudaError_t smooth_recursive(int comps, int nx, int ny, int nz, const Recursive (&rc)[3], const T *in, T *out,
                              T *scratch, cudaStream_t s) {
     const long long n = (long long) nx * ny * nz * comps;
-    k_recursive_axis<T><<<grid_for(n / nx), 256, 0, s>>>(in, out, nx, ny, nz, comps, 0, rc[0]);
+    const long long xlines = n / nx;
+    const long long xblocks = (xlines + 32 * RX_WARPS - 1) / (32 * RX_WARPS);
+    k_recursive_x<T><<<(int) std::min<long long>(xblocks, 1 << 20), 32 * RX_WARPS, 0, s>>>(in, out, nx, xlines,
+                                                                                            rc[0]);
     count_launch();
     k_recursive_axis<T><<<grid_for(n / ny), 256, 0, s>>>(out, scratch, nx, ny, nz, comps, 1, rc[1]);
     count_launch();

@@ -190,9 +190,17 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
 
     ftype = torch.float64 if precision == "fp64" else torch.float32
     sizes, spacings = level_geometry(shape0, spacing, levels)
-    Js = [J0] + [scale_image(J0, spacings[0], sizes[i], method=smoothing) for i in range(1, levels)]
-    ms = [m0] + [scale_image(m0, spacings[0], sizes[i], nearest=True, method=smoothing)
-                 for i in range(1, levels)]
+    # Every coarser level is scaled from the same full-resolution images with
+    # the same smoothing (2.0 physical units at the finest spacing), so each
+    # image is smoothed once and then resampled per level: scale_image's
+    # result for every level, with one smoothing pass instead of one a level.
+    Js, ms = [J0], [m0]
+    if levels > 1:
+        sig0 = [SMOOTH_SIGMA / float(s) for s in spacings[0]]
+        sJ0, sm0 = smooth(J0, sig0, smoothing), smooth(m0, sig0, smoothing)
+        Js += [resample(sJ0, sizes[i]) for i in range(1, levels)]
+        ms += [resample(sm0, sizes[i], nearest=True) for i in range(1, levels)]
+        del sJ0, sm0
 
     field = None
     field_spacing = spacing
