@@ -1,8 +1,9 @@
 // TMA (cp.async.bulk.tensor) and mbarrier helpers for sm_100a, inline PTX.
 //
 // Tensor maps live in global memory (one set per volume), written by a
-// host-to-device copy before the launch.  Loads are tiled, never multicast:
-// every CTA reads its own boxes of this GPU's memory.
+// host-to-device copy before the launch.  Loads are tiled, each into the
+// issuing CTA's own shared memory: every CTA reads its own boxes of this
+// GPU's memory.
 #pragma once
 
 #include <cuda.h>
