@@ -539,20 +539,35 @@ def run_c3(args, world, rank, local, quiet=False):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / reps
 
+    # The two halves as the autograd step runs them: with the cofactor path
+    # (the default for this layout) the forward also writes C = cof * ih
+    # (36 B/voxel) and the backward is one gather of grad_J * C; otherwise
+    # the forward writes the map only and the backward re-reads the field.
     fd = f.detach()
     J = torch.empty((B,) + shape, dtype=torch.float32, device=dev)
     G = torch.empty_like(fd)
-    fwd_ms = timed(lambda: [torch_ops.jacobian_raw(fd[b], out=J[b]) for b in range(B)])
-    bwd_ms = timed(lambda: [torch_ops.jacobian_adjoint_raw(fd[b], w[b], out=G[b]) for b in range(B)])
+    cof = torch_ops.uses_cofactor_path(fd)
+    if cof:
+        Cb = torch.empty((B, 9) + shape, dtype=torch.float32, device=dev)
+        fwd_ms = timed(lambda: [torch_ops.jacobian_cof_raw(fd[b], out=J[b], cof=Cb[b]) for b in range(B)])
+        bwd_ms = timed(lambda: [torch_ops.jacobian_adjoint_cof_raw(Cb[b], w[b], out=G[b]) for b in range(B)])
+    else:
+        fwd_ms = timed(lambda: [torch_ops.jacobian_raw(fd[b], out=J[b]) for b in range(B)])
+        bwd_ms = timed(lambda: [torch_ops.jacobian_adjoint_raw(fd[b], w[b], out=G[b]) for b in range(B)])
     hbm, peak_kind = peaks()
-    achieved = 16.0 * nvox / (fwd_ms / 1000.0) / 1e9
+    fwd_bpv = 52 if cof else 16  # field 12 in, map 4 (and C 36) out
+    achieved = fwd_bpv * nvox / (fwd_ms / 1000.0) / 1e9
     traffic = None  # DRAM bytes of one launch (one field), from the committed ncu capture
-    bwd_traffic = None  # the backward's two passes, per field
+    bwd_traffic = None  # the backward's passes, per field
     try:
         tj = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        traffic = tj["jacobian_c3_field"]["bytes_per_launch"]
-        bwd_traffic = tj["adjoint_c3_field"]["weight_pass_bytes_per_launch"] + tj["adjoint_c3_field"][
-            "gather_bytes_per_launch"]
+        if cof:
+            traffic = tj["jacobian_cof_c3_field"]["bytes_per_launch"]
+            bwd_traffic = tj["adjoint_cof_c3_field"]["gather_bytes_per_launch"]
+        else:
+            traffic = tj["jacobian_c3_field"]["bytes_per_launch"]
+            bwd_traffic = tj["adjoint_c3_field"]["weight_pass_bytes_per_launch"] + tj["adjoint_c3_field"][
+                "gather_bytes_per_launch"]
     except Exception:
         pass
     # The backward at the adjoint's algorithmic bytes: field 12 and gJ 4 in,
@@ -581,11 +596,14 @@ def run_c3(args, world, rank, local, quiet=False):
                    "forward_ms": fwd_ms, "backward_ms": bwd_ms,
                    "l2": "inputs larger than L2 (fields 397 MB)",
                    "parallelism": f"{world} independent batches"},
-        "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma", "achieved": achieved, "peak": hbm,
+        "roofline": {"bound": "hbm", "kernel": "k_jacobian_tma" + (" (map and C)" if cof else ""),
+                     "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                     "peak_source": peak_kind, "bytes_per_voxel": 16,
-                     "bytes_per_launch": 16 * nvox // B, "avg_launch_ms": fwd_ms / B,
-                     "backward": {"kernels": "k_jacobian_tma (weights) + k_gather_tma", "bytes_per_voxel": 28,
+                     "peak_source": peak_kind, "bytes_per_voxel": fwd_bpv,
+                     "bytes_per_launch": fwd_bpv * nvox // B, "avg_launch_ms": fwd_ms / B,
+                     "backward": {"kernels": ("k_gather_tma (grad_J * C)" if cof
+                                              else "k_jacobian_tma (weights) + k_gather_tma"),
+                                  "bytes_per_voxel": 28,
                                   "achieved": bwd_achieved, "frac": bwd_achieved / hbm,
                                   "traffic_per_field": bwd_traffic, "ms_per_field": bwd_ms / B}},
         "cpu_baseline": cpu,

@@ -123,6 +123,10 @@ lib.dtb_jacobian_device_noalloc.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _
 lib.dtb_jacobian_device_noalloc.restype = _I
 lib.dtb_jacobian_adjoint_device.argtypes = [_I, _I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
 lib.dtb_jacobian_adjoint_device.restype = _I
+lib.dtb_jacobian_cof_device.argtypes = [_I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
+lib.dtb_jacobian_cof_device.restype = _I
+lib.dtb_jacobian_adjoint_cof_device.argtypes = [_I, _SZ, _SZ, _SZ, _D, _D, _D, _P, _P, _P, _P]
+lib.dtb_jacobian_adjoint_cof_device.restype = _I
 lib.dtb_kernel_launch_count.restype = C.c_ulonglong
 lib.dtb_release_device_memory.argtypes = []
 lib.dtb_release_device_memory.restype = _I
@@ -186,7 +190,8 @@ EXPORTED = [
     "jacobian_dynamic", "regularise", "dtb_set_default_precision", "dtb_get_default_precision",
     "dtb_generate_displacement", "dtb_generate_displacement_batched",
     "dtb_generate_displacement_batched_device", "dtb_jacobian_device",
-    "dtb_jacobian_adjoint_device", "dtb_kernel_launch_count", "dtb_set_profiling",
+    "dtb_jacobian_adjoint_device", "dtb_jacobian_cof_device", "dtb_jacobian_adjoint_cof_device",
+    "dtb_kernel_launch_count", "dtb_set_profiling",
     "dtb_get_profile", "dtb_jacobian_device_noalloc", "dtb_release_device_memory",
     "dtb_set_autotune", "dtb_get_tile_config", "dtb_get_trial_kernel", "dtb_smooth_device",
     "dtb_smooth_recursive_device", "dtb_resample_device",

@@ -1491,6 +1491,77 @@ extern "C" int dtb_jacobian_adjoint_device(int precision, int order, size_t nx, 
     DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
 }
 
+namespace {
+
+// The cofactor path of the differentiable Jacobian: fourth order, rows a
+// multiple of 16 bytes long, a 16-byte-aligned field, C and gJ, pair-aligned
+// J and gradient.
+template <typename T>
+bool cof_layout_ok(const Geom &g, const void *a16_0, const void *a16_1, const void *pair) {
+    return g.order == 4 && (g.ys * (long long) sizeof(T)) % 16 == 0 && reinterpret_cast<uintptr_t>(a16_0) % 16 == 0 &&
+           reinterpret_cast<uintptr_t>(a16_1) % 16 == 0 && reinterpret_cast<uintptr_t>(pair) % (2 * sizeof(T)) == 0;
+}
+
+template <typename T>
+int jacobian_cof_impl(const Geom &g, const T *field, T *J, T *C, cudaStream_t s) {
+    if (!cof_layout_ok<T>(g, field, C, J)) DTB_FAIL(DTB_ERR_ARGUMENT, "layout not supported by the cofactor path");
+    const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUtensorMap tm;
+    if (!encode_map(&tm, ft, sizeof(T), field, g, 3, 32 + 2 * 4, TT_Y + 2 * 2))
+        DTB_FAIL(DTB_ERR_CUDA, "cannot encode the TMA descriptor (cuTensorMapEncodeTiled)");
+    DTB_CUDA(launch_jacobian_tma<T>(tm, g, J, g.ys, g.zs, num_sms(), s, nullptr, C, g.cs));
+    return DTB_OK;
+}
+
+template <typename T>
+int adjoint_cof_impl(const Geom &g, const T *C, const T *gJ, T *gout, cudaStream_t s) {
+    if (!cof_layout_ok<T>(g, C, gJ, gout)) DTB_FAIL(DTB_ERR_ARGUMENT, "layout not supported by the cofactor path");
+    const CUtensorMapDataType ft = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUtensorMap tw[3], tg;
+    if (!(encode_weights_map(&tw[0], ft, sizeof(T), C, g, g.cs, 32 + 2 * 4, TT_Y) &&
+          encode_weights_map(&tw[1], ft, sizeof(T), C, g, g.cs, 32, TT_Y + 2 * 2) &&
+          encode_weights_map(&tw[2], ft, sizeof(T), C, g, g.cs, 32, TT_Y) &&
+          encode_map(&tg, ft, sizeof(T), gJ, g, 1, 32 + 2 * 4, TT_Y + 2 * 2)))
+        DTB_FAIL(DTB_ERR_CUDA, "cannot encode the TMA descriptors (cuTensorMapEncodeTiled)");
+    DTB_CUDA(launch_gather_tma<T>(tw[0], tw[1], tw[2], g, gout, num_sms(), s, &tg));
+    return DTB_OK;
+}
+
+}  // namespace
+
+extern "C" int dtb_jacobian_cof_device(int precision, size_t nx, size_t ny, size_t nz, double dx, double dy,
+                                       double dz, const void *field, void *J, void *C, void *stream) {
+    disptools_clear_error();
+    if (!valid_dims(nx, ny, nz)) DTB_FAIL(DTB_ERR_ARGUMENT, "every axis needs at least 3 voxels");
+    if (!field || !J || !C) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+    const Geom g = make_geom(nx, ny, nz, dx, dy, dz, 4);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == DTB_PRECISION_FP64)
+        return jacobian_cof_impl<double>(g, static_cast<const double *>(field), static_cast<double *>(J),
+                                         static_cast<double *>(C), s);
+    if (precision == DTB_PRECISION_MIXED)
+        return jacobian_cof_impl<float>(g, static_cast<const float *>(field), static_cast<float *>(J),
+                                        static_cast<float *>(C), s);
+    DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
+extern "C" int dtb_jacobian_adjoint_cof_device(int precision, size_t nx, size_t ny, size_t nz, double dx, double dy,
+                                               double dz, const void *C, const void *grad_J, void *grad_field,
+                                               void *stream) {
+    disptools_clear_error();
+    if (!valid_dims(nx, ny, nz)) DTB_FAIL(DTB_ERR_ARGUMENT, "every axis needs at least 3 voxels");
+    if (!C || !grad_J || !grad_field) DTB_FAIL(DTB_ERR_ARGUMENT, "null array");
+    const Geom g = make_geom(nx, ny, nz, dx, dy, dz, 4);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == DTB_PRECISION_FP64)
+        return adjoint_cof_impl<double>(g, static_cast<const double *>(C), static_cast<const double *>(grad_J),
+                                        static_cast<double *>(grad_field), s);
+    if (precision == DTB_PRECISION_MIXED)
+        return adjoint_cof_impl<float>(g, static_cast<const float *>(C), static_cast<const float *>(grad_J),
+                                       static_cast<float *>(grad_field), s);
+    DTB_FAIL(DTB_ERR_ARGUMENT, "invalid precision");
+}
+
 extern "C" int dtb_set_device_memory_limit(size_t bytes) {
     disptools_clear_error();
     std::lock_guard<std::mutex> lock(g_ws_mutex);

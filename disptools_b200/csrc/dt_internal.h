@@ -166,18 +166,22 @@ template <typename T>
 int greedy_tma_blocks_per_sm();
 // TMA stencil of one field of order 4 (the map `tm_u` over the field with
 // box 40 x 20 x 1 x 3), with element strides jys, jzs for the scalar maps:
-// the Jacobian map into jout, or (adjoint weights) W[c][a] = gJ * cof_ca(I +
-// grad u) * ih_a into W with component stride wn.
+// the Jacobian map into jout; with gJ and W, (adjoint weights) W[c][a] = gJ *
+// cof_ca(I + grad u) * ih_a into W with component stride wn (no map); with W
+// and no gJ, the map and C[c][a] = cof_ca(I + grad u) * ih_a into W.
 template <typename T>
 cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
                                 int num_sms, cudaStream_t s, const T *gJ = nullptr, T *W = nullptr,
                                 long long wn = 0);
 // Gather pass of the adjoint on TMA-staged weights W[c][a][wn]: maps over W
 // with boxes 40 x TT_Y (axis x), 32 x (TT_Y + 4) (axis y) and 32 x TT_Y
-// (axis z), one plane, three components.
+// (axis z), one plane, three components.  With `tm_gj` (a map over gJ, box
+// 40 x (TT_Y + 4)), the maps cover C[c][a] = cof_ca * ih_a instead and each
+// weight is formed as gJ * C.
 template <typename T>
 cudaError_t launch_gather_tma(const CUtensorMap &tm_wx, const CUtensorMap &tm_wy, const CUtensorMap &tm_wz,
-                              const Geom &g, T *gout, int num_sms, cudaStream_t s);
+                              const Geom &g, T *gout, int num_sms, cudaStream_t s,
+                              const CUtensorMap *tm_gj = nullptr);
 // Fused adjoint of the Jacobian stencil of order 4 (one TMA kernel, no
 // weight buffer): `tm_u` maps the field with box 40 x 24 x 1 x 3; gJ and gout
 // in the field's dense layout.

@@ -1891,7 +1891,10 @@ struct JacTmaLayout {
 // ADJ instantiates the weight pass of the Jacobian's adjoint instead: with
 // w = gJ(p), W[c][a](p) = w * cof_ca(I + A(p)) * ih_a for the stencil matrix
 // A(p), W dense with component stride wn (the gather pass follows).
-template <typename T, int TXW, int TYT, bool ADJ = false>
+// COF (the differentiable Jacobian's forward) writes the map and, into W,
+// C[c][a](p) = cof_ca(I + A(p)) * ih_a, so that the backward needs only the
+// gather, with W = gJ * C formed there.
+template <typename T, int TXW, int TYT, bool ADJ = false, bool COF = false>
 __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     k_jacobian_tma(const __grid_constant__ CUtensorMap tm_u, const Geom g, T *__restrict__ jout, long long jys,
                    long long jzs, int tiles_x, int tiles_y, int ntiles, int bz, const T *__restrict__ gJ,
@@ -2069,19 +2072,69 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                     }
                 } else {
                     T jv[2];
+                    T cv[COF ? 9 : 1][2];
+                    // C[c][b] = cof_cb(I + a) * ih_b: a minor (difference of
+                    // two products) times +-ih_b, as the weight epilogue
+                    // rounds it before its factor w.
                     auto det2 = [&](const auto &a) {
                         const auto J = det_i_plus2(a);
                         jv[0] = J.x;
                         jv[1] = J.y;
+                        if constexpr (COF) {
+                            auto m = [&](int i, int j) { return i == j ? p_add(a[i][j], p_splat(1.f)) : a[i][j]; };
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+#pragma unroll
+                                for (int b = 0; b < 3; ++b) {
+                                    const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+                                    const float2 minor =
+                                        p_sub(p_mul(m(r0, c0), m(r1, c1)), p_mul(m(r0, c1), m(r1, c0)));
+                                    const float2 q = p_mul(minor, p_splat(((c + b) & 1) ? -ih[b] : ih[b]));
+                                    cv[c * 3 + b][0] = q.x;
+                                    cv[c * 3 + b][1] = q.y;
+                                }
+                            }
+                        }
                     };
-                    stencil_pair<T, TMA_PX, TMA_PLANE>(
-                        zq[r], jp, lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih, row_in, tile_x_in,
-                        [&](int v, const T (&a)[3][3]) { jv[v] = det_i_plus<T>(a); }, det2);
+                    auto det1 = [&](int v, const T (&a)[3][3]) {
+                        jv[v] = det_i_plus<T>(a);
+                        if constexpr (COF) {
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                const int r0 = c == 0 ? 1 : 0, r1 = c == 2 ? 1 : 2;
+#pragma unroll
+                                for (int b = 0; b < 3; ++b) {
+                                    const int c0 = b == 0 ? 1 : 0, c1 = b == 2 ? 1 : 2;
+                                    const T m00 = a[r0][c0] + (r0 == c0 ? T(1) : T(0));
+                                    const T m11 = a[r1][c1] + (r1 == c1 ? T(1) : T(0));
+                                    const T m01 = a[r0][c1] + (r0 == c1 ? T(1) : T(0));
+                                    const T m10 = a[r1][c0] + (r1 == c0 ? T(1) : T(0));
+                                    const T ihs = ((c + b) & 1) ? -ih[b] : ih[b];
+                                    if constexpr (sizeof(T) == 4)
+                                        cv[c * 3 + b][v] =
+                                            __fmul_rn(__fsub_rn(__fmul_rn(m00, m11), __fmul_rn(m01, m10)), ihs);
+                                    else cv[c * 3 + b][v] = (m00 * m11 - m01 * m10) * ihs;
+                                }
+                            }
+                        }
+                    };
+                    stencil_pair<T, TMA_PX, TMA_PLANE>(zq[r], jp, lx, ty + r * TYT + TMA_HY, x, y, ze, g, ih,
+                                                       row_in, tile_x_in, det1, det2);
                     T *o = jout + off;
                     if (pair_in)
                         st_pair(o, jv[0], jv[1]);
                     else
                         o[0] = jv[0];
+                    if constexpr (COF) {
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) {
+                            if (pair_in)
+                                st_pair(W + k * wn + off, cv[k][0], cv[k][1]);
+                            else
+                                W[k * wn + off] = cv[k][0];
+                        }
+                    }
                 }
             }
         }
@@ -2102,10 +2155,9 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
                     for (int v = 0; v < 2; ++v) {
                         if (x + v >= g.nx) continue;
                         const long long off = ze * jzs + y * jys + x + v;
-                        if (ADJ)
+                        if (ADJ || COF)
                             for (int k = 0; k < 9; ++k) W[k * wn + off] = nan;
-                        else
-                            jout[off] = nan;
+                        if (!ADJ) jout[off] = nan;
                     }
                 }
             __syncthreads();
@@ -2115,13 +2167,13 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 2 : 1)
     }
 }
 
-template <typename T, int TXW, int TYT, bool ADJ>
+template <typename T, int TXW, int TYT, bool ADJ, bool COF>
 int jacobian_blocks_v() {
     static const int n = [] {
         int v = 0;
-        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT, ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_jacobian_tma<T, TXW, TYT, ADJ, COF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              JacTmaLayout<T, TXW>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_jacobian_tma<T, TXW, TYT, ADJ>, TXW / 2 * TYT,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_jacobian_tma<T, TXW, TYT, ADJ, COF>, TXW / 2 * TYT,
                                                       JacTmaLayout<T, TXW>::BYTES + 128);
         return v;
     }();
@@ -2134,25 +2186,25 @@ int jacobian_blocks_v() {
 // is chosen to fill whole waves of the grid: about 32 planes a tile, then as
 // many z tiles per column as fit in that many waves (at least 8 planes a
 // tile, since each tile also loads 4 halo planes).
-template <typename T, bool ADJ>
+template <typename T, bool ADJ, bool COF>
 cudaError_t launch_jacobian_tma_v(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
                                   int num_sms, cudaStream_t s, const T *gJ, T *W, long long wn) {
     constexpr int TXW = 32, TYT = 16, BZ = 32;
     constexpr int smem = JacTmaLayout<T, TXW>::BYTES + 128;
     static std::atomic<unsigned long long> devs{0};
-    const cudaError_t attr = opt_in_smem(k_jacobian_tma<T, TXW, TYT, ADJ>, smem, devs);
+    const cudaError_t attr = opt_in_smem(k_jacobian_tma<T, TXW, TYT, ADJ, COF>, smem, devs);
     if (attr != cudaSuccess) return attr;
     const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
     const int cols = tiles_x * tiles_y;
-    const int slots = std::max(1, jacobian_blocks_v<T, TXW, TYT, ADJ>()) * num_sms;  // resident blocks
+    const int slots = std::max(1, jacobian_blocks_v<T, TXW, TYT, ADJ, COF>()) * num_sms;  // resident blocks
     int nzt = (g.nz + BZ - 1) / BZ;                                             // z tiles per column
     const int waves = (cols * nzt + slots - 1) / slots;
     nzt = std::min((g.nz + 7) / 8, std::max(nzt, waves * slots / cols));  // at least 8 planes a tile
     const int bz = (g.nz + nzt - 1) / nzt;
     const int ntiles = cols * ((g.nz + bz - 1) / bz);
     const int grid = std::min(ntiles, slots);
-    k_jacobian_tma<T, TXW, TYT, ADJ><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_u, g, jout, jys, jzs, tiles_x,
-                                                                           tiles_y, ntiles, bz, gJ, W, wn);
+    k_jacobian_tma<T, TXW, TYT, ADJ, COF><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_u, g, jout, jys, jzs, tiles_x,
+                                                                                tiles_y, ntiles, bz, gJ, W, wn);
     count_launch();
     return cudaGetLastError();
 }
@@ -2160,8 +2212,9 @@ cudaError_t launch_jacobian_tma_v(const CUtensorMap &tm_u, const Geom &g, T *jou
 template <typename T>
 cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout, long long jys, long long jzs,
                                 int num_sms, cudaStream_t s, const T *gJ, T *W, long long wn) {
-    if (W) return launch_jacobian_tma_v<T, true>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
-    return launch_jacobian_tma_v<T, false>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
+    if (W && gJ) return launch_jacobian_tma_v<T, true, false>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
+    if (W) return launch_jacobian_tma_v<T, false, true>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
+    return launch_jacobian_tma_v<T, false, false>(tm_u, g, jout, jys, jzs, num_sms, s, gJ, W, wn);
 }
 
 // ------------------------------------------------------------------------
@@ -2181,18 +2234,26 @@ cudaError_t launch_jacobian_tma(const CUtensorMap &tm_u, const Geom &g, T *jout,
 // per-lane coefficients for the x taps (both as FP32 pairs); the others
 // choose each tap's coefficient by the tap voxel's scheme.
 // ------------------------------------------------------------------------
-template <typename T, int TXW>
+// GJ: the stages hold C (the weights without their factor gJ) and two boxes
+// of gJ (TXW + 8 columns, TT_Y + 4 rows) at planes ze and q, and each weight
+// is formed as gJ * C where it is read.
+template <typename T, int TXW, bool GJ = false>
 struct GatherTmaLayout {
     static constexpr int XPX = TXW + 2 * TMA_HX;  // W[.][x] box: TXW + 8 columns, TT_Y rows
     static constexpr int X_ELEMS = 3 * TT_Y * XPX;
     static constexpr int YPY = TT_Y + 2 * TMA_HY;  // W[.][y] box: TXW columns, TT_Y + 4 rows
     static constexpr int Y_ELEMS = 3 * YPY * TXW;
     static constexpr int Z_ELEMS = 3 * TT_Y * TXW;  // W[.][z] box: the tile
+    static constexpr int G_ELEMS = YPY * XPX;       // a gJ box
     static constexpr int X_OFF = 0;
     static constexpr int Y_OFF = X_ELEMS * (int) sizeof(T);
     static constexpr int Z_OFF = Y_OFF + Y_ELEMS * (int) sizeof(T);
-    static constexpr int STAGE_BYTES = (Z_OFF + Z_ELEMS * (int) sizeof(T) + 127) / 128 * 128;
-    static constexpr int S = sizeof(T) == 4 ? 3 : 4;  // 63 KB (FP32, three blocks per SM), 168 KB (FP64)
+    static constexpr int G_BYTES = (G_ELEMS * (int) sizeof(T) + 127) / 128 * 128;
+    static constexpr int GE_OFF = (Z_OFF + Z_ELEMS * (int) sizeof(T) + 127) / 128 * 128;  // gJ at ze
+    static constexpr int GQ_OFF = GE_OFF + G_BYTES;                                        // gJ at q
+    static constexpr int STAGE_BYTES = GJ ? GQ_OFF + G_BYTES : GE_OFF;
+    // 63 KB (FP32, three blocks per SM; GJ: two stages, 56 KB), 168 KB (FP64)
+    static constexpr int S = sizeof(T) == 4 ? (GJ ? 2 : 3) : 4;
     static constexpr int B = sizeof(T) == 4 ? 1 : 2;  // planes between block barriers
     static constexpr int LA = S - B;                  // load distance
     static constexpr int BAR_OFF = S * STAGE_BYTES;
@@ -2200,12 +2261,12 @@ struct GatherTmaLayout {
     static_assert(Y_OFF % 128 == 0 && Z_OFF % 128 == 0, "boxes start 128-byte aligned");
 };
 
-template <typename T, int TXW, int TYT>
+template <typename T, int TXW, int TYT, bool GJ = false>
 __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
     k_gather_tma(const __grid_constant__ CUtensorMap tm_wx, const __grid_constant__ CUtensorMap tm_wy,
-                 const __grid_constant__ CUtensorMap tm_wz, const Geom g, T *__restrict__ gout, int tiles_x,
-                 int tiles_y, int ntiles, int bz) {
-    using L = GatherTmaLayout<T, TXW>;
+                 const __grid_constant__ CUtensorMap tm_wz, const __grid_constant__ CUtensorMap tm_gj, const Geom g,
+                 T *__restrict__ gout, int tiles_x, int tiles_y, int ntiles, int bz) {
+    using L = GatherTmaLayout<T, TXW, GJ>;
     using P2 = typename PairOf<T>::type;
     constexpr int TPX = TXW / 2, RYT = TT_Y / TYT, S = L::S, LA = L::LA, XPX = L::XPX, YPY = L::YPY;
     static_assert(TPX <= 32 && 32 % TPX == 0, "a warp spans whole tile rows");
@@ -2221,6 +2282,7 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
         tmap_prefetch(&tm_wx);
         tmap_prefetch(&tm_wy);
         tmap_prefetch(&tm_wz);
+        if (GJ) tmap_prefetch(&tm_gj);
         s_fault = 0;
     }
     __syncthreads();
@@ -2243,11 +2305,15 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
             unsigned char *sb = smem + (k % S) * L::STAGE_BYTES;
             const int q = z0 - 2 + j, ze = q - 2;
             const bool with_xy = ze >= z0 && ze < z1;
-            mbar_arrive_expect_tx(bar, (uint32_t) ((L::Z_ELEMS + (with_xy ? L::X_ELEMS + L::Y_ELEMS : 0)) * sizeof(T)));
+            const int elems = L::Z_ELEMS + (with_xy ? L::X_ELEMS + L::Y_ELEMS : 0) +
+                              (GJ ? L::G_ELEMS * (with_xy ? 2 : 1) : 0);
+            mbar_arrive_expect_tx(bar, (uint32_t) (elems * sizeof(T)));
             tma_load_5d(sb + L::Z_OFF, &tm_wz, bar, x0, y0, q, 2, 0);
+            if (GJ) tma_load_3d(sb + L::GQ_OFF, &tm_gj, bar, x0 - TMA_HX, y0 - TMA_HY, q);
             if (with_xy) {
                 tma_load_5d(sb + L::X_OFF, &tm_wx, bar, x0 - TMA_HX, y0, ze, 0, 0);
                 tma_load_5d(sb + L::Y_OFF, &tm_wy, bar, x0, y0 - TMA_HY, ze, 1, 0);
+                if (GJ) tma_load_3d(sb + L::GE_OFF, &tm_gj, bar, x0 - TMA_HX, y0 - TMA_HY, ze);
             }
         };
         if (tid == 0)
@@ -2283,6 +2349,28 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
             const T *wx = reinterpret_cast<const T *>(sb + L::X_OFF);
             const T *wy = reinterpret_cast<const T *>(sb + L::Y_OFF);
             const T *wz = reinterpret_cast<const T *>(sb + L::Z_OFF);
+            // GJ: gJ at planes ze (x and y taps) and q (z queue), boxes
+            // starting at column x0-4 and row y0-2.
+            const T *gje = reinterpret_cast<const T *>(sb + L::GE_OFF);
+            const T *gjq = reinterpret_cast<const T *>(sb + L::GQ_OFF);
+            // A weight pair gJ * C (GJ) or W as stored.
+            auto wmul = [&](P2 w, const T *gp) -> P2 {
+                if constexpr (GJ) {
+                    const P2 gv = ld_pair(gp);
+                    if constexpr (sizeof(T) == 4) return p_mul(w, gv);
+                    else return P2{w.x * gv.x, w.y * gv.y};
+                } else {
+                    return w;
+                }
+            };
+            auto wmul1 = [&](T w, const T *gp) -> T {
+                if constexpr (GJ) {
+                    if constexpr (sizeof(T) == 4) return __fmul_rn(w, *gp);
+                    else return w * *gp;
+                } else {
+                    return w;
+                }
+            };
             const int q = z0 - 2 + it, ze = q - 2;
 #pragma unroll
             for (int r = 0; r < RYT; ++r) {
@@ -2291,7 +2379,8 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
                 for (int c = 0; c < 3; ++c) {
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk) wq[r][c][kk] = wq[r][c][kk + 1];
-                    wq[r][c][4] = ld_pair(wz + (c * TT_Y + ly) * TXW + 2 * tx);
+                    wq[r][c][4] = wmul(ld_pair(wz + (c * TT_Y + ly) * TXW + 2 * tx),
+                                       gjq + (ly + TMA_HY) * XPX + 2 * tx + TMA_HX);
                 }
             }
 #pragma unroll
@@ -2323,12 +2412,16 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
                         // independent, for instruction-level parallelism.
                         const float2 k12 = p_splat(FD<float>::one_twelfth), k23 = p_splat(FD<float>::two_thirds);
 #pragma unroll
+                        const T *gp = gje + (ly + TMA_HY) * XPX + 2 * tx + TMA_HX;  // gJ at (x, y, ze)
                         for (int c = 0; c < 3; ++c) {
                             const T *px = wx + (c * TT_Y + ly) * XPX + 2 * tx + TMA_HX;
-                            const float2 xm = ld_pair(px - 2), xc = ld_pair(px), xp = ld_pair(px + 2);
+                            const float2 xm = wmul(ld_pair(px - 2), gp - 2), xc = wmul(ld_pair(px), gp),
+                                         xp = wmul(ld_pair(px + 2), gp + 2);
                             const T *py = wy + (c * YPY + ly + TMA_HY) * TXW + 2 * tx;
-                            const float2 ym2 = ld_pair(py - 2 * TXW), ym1 = ld_pair(py - TXW);
-                            const float2 yp1 = ld_pair(py + TXW), yp2 = ld_pair(py + 2 * TXW);
+                            const float2 ym2 = wmul(ld_pair(py - 2 * TXW), gp - 2 * XPX),
+                                         ym1 = wmul(ld_pair(py - TXW), gp - XPX);
+                            const float2 yp1 = wmul(ld_pair(py + TXW), gp + XPX),
+                                         yp2 = wmul(ld_pair(py + 2 * TXW), gp + 2 * XPX);
                             const float2 d1x = make_float2(__fsub_rn(xm.y, xc.y), __fsub_rn(xc.x, xp.x));
                             const float2 sx = p_fma(d1x, k23, p_mul(p_sub(xp, xm), k12));
                             const float2 sy = p_fma(p_sub(ym1, yp1), k23, p_mul(p_sub(yp2, ym2), k12));
@@ -2370,20 +2463,22 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
                             }
                             kyz[i] = make_float2(kv[0], kv[1]);
                         }
+                        const T *gp = gje + (ly + TMA_HY) * XPX + 2 * tx + TMA_HX;  // gJ at (x, y, ze)
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
                             const T *px = wx + (c * TT_Y + ly) * XPX + 2 * tx + TMA_HX;
-                            const float2 xm = ld_pair(px - 2), xc = ld_pair(px), xp = ld_pair(px + 2);
+                            const float2 xm = wmul(ld_pair(px - 2), gp - 2), xc = wmul(ld_pair(px), gp),
+                                         xp = wmul(ld_pair(px + 2), gp + 2);
                             const T *py = wy + (c * YPY + ly + TMA_HY) * TXW + 2 * tx;
                             float2 a2 = p_mul(xp, kx[0]);
                             a2 = p_fma(make_float2(xc.y, xp.x), kx[1], a2);
                             a2 = p_fma(xc, kx[2], a2);
                             a2 = p_fma(make_float2(xm.y, xc.x), kx[3], a2);
                             a2 = p_fma(xm, kx[4], a2);
-                            a2 = p_fma(ld_pair(py + 2 * TXW), kyz[0], a2);
-                            a2 = p_fma(ld_pair(py + TXW), kyz[1], a2);
-                            a2 = p_fma(ld_pair(py - TXW), kyz[2], a2);
-                            a2 = p_fma(ld_pair(py - 2 * TXW), kyz[3], a2);
+                            a2 = p_fma(wmul(ld_pair(py + 2 * TXW), gp + 2 * XPX), kyz[0], a2);
+                            a2 = p_fma(wmul(ld_pair(py + TXW), gp + XPX), kyz[1], a2);
+                            a2 = p_fma(wmul(ld_pair(py - TXW), gp - XPX), kyz[2], a2);
+                            a2 = p_fma(wmul(ld_pair(py - 2 * TXW), gp - 2 * XPX), kyz[3], a2);
                             a2 = p_fma(wq[r][c][4], kyz[0], a2);
                             a2 = p_fma(wq[r][c][3], kyz[1], a2);
                             a2 = p_fma(wq[r][c][1], kyz[2], a2);
@@ -2417,7 +2512,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
                                 if (kp == T(0)) continue;
 #pragma unroll
                                 for (int c = 0; c < 3; ++c)
-                                    a3[c] = acc_op(a3[c], wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX], kp);
+                                    a3[c] = acc_op(a3[c],
+                                                   wmul1(wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX],
+                                                         gje + (ly + TMA_HY) * XPX + 2 * tx + v - t + TMA_HX),
+                                                   kp);
                             }
 #pragma unroll
                             for (int i = 0; i < 4; ++i) {
@@ -2426,7 +2524,10 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
                                 const T kp = x_c2 ? kappa<T>(S_C2, t) : kc[i];
 #pragma unroll
                                 for (int c = 0; c < 3; ++c)
-                                    a3[c] = acc_op(a3[c], wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v], kp);
+                                    a3[c] = acc_op(a3[c],
+                                                   wmul1(wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v],
+                                                         gje + (ly + TMA_HY - t) * XPX + 2 * tx + v + TMA_HX),
+                                                   kp);
                             }
 #pragma unroll
                             for (int i = 0; i < 4; ++i) {
@@ -2467,9 +2568,11 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
                                     for (int c = 0; c < 3; ++c) {
                                         T w;
                                         if (a == 0)
-                                            w = wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX];
+                                            w = wmul1(wx[(c * TT_Y + ly) * XPX + 2 * tx + v - t + TMA_HX],
+                                                      gje + (ly + TMA_HY) * XPX + 2 * tx + v - t + TMA_HX);
                                         else if (a == 1)
-                                            w = wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v];
+                                            w = wmul1(wy[(c * YPY + ly + TMA_HY - t) * TXW + 2 * tx + v],
+                                                      gje + (ly + TMA_HY - t) * XPX + 2 * tx + v + TMA_HX);
                                         else
                                             w = v ? wq[r][c][2 - t].y : wq[r][c][2 - t].x;
                                         a3[c] = acc_op(a3[c], w, kp);
@@ -2519,42 +2622,51 @@ __global__ void __launch_bounds__(TXW / 2 * TYT, sizeof(T) == 4 ? 3 : 1)
     }
 }
 
-template <typename T, int TXW, int TYT>
+template <typename T, int TXW, int TYT, bool GJ>
 int gather_blocks_v() {
     static const int n = [] {
         int v = 0;
-        cudaFuncSetAttribute(k_gather_tma<T, TXW, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             GatherTmaLayout<T, TXW>::BYTES + 128);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gather_tma<T, TXW, TYT>, TXW / 2 * TYT,
-                                                      GatherTmaLayout<T, TXW>::BYTES + 128);
+        cudaFuncSetAttribute(k_gather_tma<T, TXW, TYT, GJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             GatherTmaLayout<T, TXW, GJ>::BYTES + 128);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_gather_tma<T, TXW, TYT, GJ>, TXW / 2 * TYT,
+                                                      GatherTmaLayout<T, TXW, GJ>::BYTES + 128);
         return v;
     }();
     return n;
 }
 
 // Gather pass on TMA-staged weights: tiles of 32 x TT_Y voxels, 16 x 16
-// threads, the z split as in launch_jacobian_tma_v.
-template <typename T>
-cudaError_t launch_gather_tma(const CUtensorMap &tm_wx, const CUtensorMap &tm_wy, const CUtensorMap &tm_wz,
-                              const Geom &g, T *gout, int num_sms, cudaStream_t s) {
+// threads, the z split as in launch_jacobian_tma_v.  With `tm_gj` (a map over
+// gJ with box 40 x (TT_Y + 4)), the three weight maps cover C and each weight
+// is gJ * C.
+template <typename T, bool GJ>
+cudaError_t launch_gather_tma_v(const CUtensorMap &tm_wx, const CUtensorMap &tm_wy, const CUtensorMap &tm_wz,
+                                const CUtensorMap &tm_gj, const Geom &g, T *gout, int num_sms, cudaStream_t s) {
     constexpr int TXW = 32, TYT = 16, BZ = 32;
-    constexpr int smem = GatherTmaLayout<T, TXW>::BYTES + 128;
+    constexpr int smem = GatherTmaLayout<T, TXW, GJ>::BYTES + 128;
     static std::atomic<unsigned long long> devs{0};
-    const cudaError_t attr = opt_in_smem(k_gather_tma<T, TXW, TYT>, smem, devs);
+    const cudaError_t attr = opt_in_smem(k_gather_tma<T, TXW, TYT, GJ>, smem, devs);
     if (attr != cudaSuccess) return attr;
     const int tiles_x = (g.nx + TXW - 1) / TXW, tiles_y = (g.ny + TT_Y - 1) / TT_Y;
     const int cols = tiles_x * tiles_y;
-    const int slots = std::max(1, gather_blocks_v<T, TXW, TYT>()) * num_sms;  // resident blocks
-    int nzt = (g.nz + BZ - 1) / BZ;                                      // z tiles per column
+    const int slots = std::max(1, gather_blocks_v<T, TXW, TYT, GJ>()) * num_sms;  // resident blocks
+    int nzt = (g.nz + BZ - 1) / BZ;                                          // z tiles per column
     const int waves = (cols * nzt + slots - 1) / slots;
     nzt = std::min((g.nz + 7) / 8, std::max(nzt, waves * slots / cols));  // at least 8 planes a tile
     const int bz = (g.nz + nzt - 1) / nzt;
     const int ntiles = cols * ((g.nz + bz - 1) / bz);
     const int grid = std::min(ntiles, slots);
-    k_gather_tma<T, TXW, TYT><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_wx, tm_wy, tm_wz, g, gout, tiles_x, tiles_y,
-                                                                      ntiles, bz);
+    k_gather_tma<T, TXW, TYT, GJ><<<grid, dim3(TXW / 2, TYT), smem, s>>>(tm_wx, tm_wy, tm_wz, tm_gj, g, gout, tiles_x,
+                                                                          tiles_y, ntiles, bz);
     count_launch();
     return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_gather_tma(const CUtensorMap &tm_wx, const CUtensorMap &tm_wy, const CUtensorMap &tm_wz,
+                              const Geom &g, T *gout, int num_sms, cudaStream_t s, const CUtensorMap *tm_gj) {
+    if (tm_gj) return launch_gather_tma_v<T, true>(tm_wx, tm_wy, tm_wz, *tm_gj, g, gout, num_sms, s);
+    return launch_gather_tma_v<T, false>(tm_wx, tm_wy, tm_wz, tm_wz, g, gout, num_sms, s);
 }
 
 // ------------------------------------------------------------------------
@@ -3131,7 +3243,7 @@ cudaError_t launch_adjoint_tma(const CUtensorMap &tm_u, const Geom &g, const T *
     template cudaError_t launch_jacobian_tma<T>(const CUtensorMap &, const Geom &, T *, long long, long long, int, \
                                                 cudaStream_t, const T *, T *, long long);                   \
     template cudaError_t launch_gather_tma<T>(const CUtensorMap &, const CUtensorMap &, const CUtensorMap &,   \
-                                              const Geom &, T *, int, cudaStream_t);                        \
+                                              const Geom &, T *, int, cudaStream_t, const CUtensorMap *);   \
     template int gradient_tma_blocks_per_sm<T>(int, int);                                                   \
     template cudaError_t launch_trial_rel<T>(const VolumeDesc<T> *, const int *, int, int, cudaStream_t,    \
                                              unsigned char *, int, int, TileQueue *);                       \

@@ -83,26 +83,116 @@ def jacobian_adjoint_raw(field: torch.Tensor, grad_J: torch.Tensor,
     return out
 
 
+def cof_supported(field: torch.Tensor, order: int = 4) -> bool:
+    """Whether the cofactor path takes this field: fourth order, float32,
+    rows a multiple of 16 bytes long and a 16-byte-aligned base."""
+    return (order == 4 and field.dtype == torch.float32 and field.is_cuda and field.is_contiguous()
+            and field.shape[-1] % 4 == 0 and field.data_ptr() % 16 == 0)
+
+
+def jacobian_cof_raw(field: torch.Tensor, spacing: Sequence[float] = (1.0, 1.0, 1.0),
+                     out: torch.Tensor | None = None, cof: torch.Tensor | None = None):
+    """Jacobian map of one ``[3, nz, ny, nx]`` device field and the factors
+    C[c][a] = cof_ca(I + grad u) * ih_a (``[9, nz, ny, nx]``) its adjoint
+    needs: returns ``(J, C)``.  Fourth order; see :func:`cof_supported`."""
+    _check(field, "field")
+    if field.dim() != 4 or field.shape[0] != 3:
+        raise ValueError("field must have shape (3, nz, ny, nx)")
+    _, nz, ny, nx = field.shape
+    J = torch.empty((nz, ny, nx), dtype=field.dtype, device=field.device) if out is None else out
+    Cf = torch.empty((9, nz, ny, nx), dtype=field.dtype, device=field.device) if cof is None else cof
+    for t, name in ((J, "out"), (Cf, "cof")):
+        _check(t, name)
+        if t.dtype != field.dtype or t.device != field.device:
+            raise ValueError(f"{name} must match the field's dtype and device")
+    if J.shape != (nz, ny, nx) or Cf.shape != (9, nz, ny, nx):
+        raise ValueError("out must be (nz, ny, nx) and cof (9, nz, ny, nx)")
+    with torch.cuda.device(field.device):
+        N.check(N.lib.dtb_jacobian_cof_device(_precision(field), nx, ny, nz, *map(float, spacing),
+                                              field.data_ptr(), J.data_ptr(), Cf.data_ptr(), _stream(field)))
+    return J, Cf
+
+
+def jacobian_adjoint_cof_raw(cof: torch.Tensor, grad_J: torch.Tensor,
+                             spacing: Sequence[float] = (1.0, 1.0, 1.0),
+                             out: torch.Tensor | None = None) -> torch.Tensor:
+    """(dJ/dfield)^T grad_J from the factors ``cof`` of
+    :func:`jacobian_cof_raw` (no field read), into ``out`` (``[3, nz, ny,
+    nx]``) when given."""
+    _check(cof, "cof")
+    if cof.dim() != 4 or cof.shape[0] != 9:
+        raise ValueError("cof must have shape (9, nz, ny, nx)")
+    grad_J = grad_J.contiguous()
+    if grad_J.data_ptr() % 16:
+        grad_J = grad_J.clone()
+    _check(grad_J, "grad_J")
+    if grad_J.dtype != cof.dtype or grad_J.shape != cof.shape[1:]:
+        raise ValueError("grad_J must match cof's dtype and spatial shape")
+    _, nz, ny, nx = cof.shape
+    if out is None:
+        out = torch.empty((3, nz, ny, nx), dtype=cof.dtype, device=cof.device)
+    else:
+        _check(out, "out")
+        if out.shape != (3, nz, ny, nx) or out.dtype != cof.dtype or out.device != cof.device:
+            raise ValueError("out must be (3, nz, ny, nx) with cof's dtype and device")
+    with torch.cuda.device(cof.device):
+        N.check(N.lib.dtb_jacobian_adjoint_cof_device(_precision(cof), nx, ny, nz, *map(float, spacing),
+                                                      cof.data_ptr(), grad_J.data_ptr(), out.data_ptr(),
+                                                      _stream(cof)))
+    return out
+
+
+def uses_cofactor_path(field: torch.Tensor, order: int = 4) -> bool:
+    """Whether :func:`jacobian`'s forward keeps C for its backward: the
+    layout allows it (:func:`cof_supported`) and DISPTOOLS_B200_AUTOGRAD is
+    not ``weights`` (which asks for the weight pass + gather)."""
+    import os
+    return os.environ.get("DISPTOOLS_B200_AUTOGRAD", "cofactors") != "weights" and cof_supported(field, order)
+
+
 class JacobianFunction(torch.autograd.Function):
     """J = det(I + grad u) with the reference stencil (src/jacobian.c:70-242);
-    the backward pass is the hand-written adjoint stencil kernel."""
+    the backward pass is the hand-written adjoint stencil kernel.  For
+    float32 fields of a TMA-friendly layout the forward also keeps C =
+    cof(I + grad u) * ih (36 bytes a voxel), and the backward is then one
+    gather of grad_J * C; otherwise the backward re-reads the field (weight
+    pass + gather)."""
 
     @staticmethod
     def forward(ctx, field, spacing, order):
-        ctx.save_for_backward(field)
         ctx.spacing = tuple(float(s) for s in spacing)
         ctx.order = order
-        if field.dim() == 5:
-            J = torch.empty((field.shape[0],) + tuple(field.shape[2:]), dtype=field.dtype,
-                            device=field.device)
-            for f, j in zip(field, J):
+        use_cof = ctx.needs_input_grad[0] and uses_cofactor_path(field, order)
+        ctx.use_cof = use_cof
+        batched = field.dim() == 5
+        fields = list(field) if batched else [field]
+        J = torch.empty(((field.shape[0],) if batched else ()) + tuple(field.shape[-3:]), dtype=field.dtype,
+                        device=field.device)
+        Js = list(J) if batched else [J]
+        if use_cof:
+            Cs = torch.empty(((field.shape[0],) if batched else ()) + (9,) + tuple(field.shape[-3:]),
+                             dtype=field.dtype, device=field.device)
+            for f, j, cf in zip(fields, Js, list(Cs) if batched else [Cs]):
+                jacobian_cof_raw(f, spacing, out=j, cof=cf)
+            ctx.save_for_backward(Cs)
+        else:
+            for f, j in zip(fields, Js):
                 jacobian_raw(f, spacing, order, out=j)
-            return J
-        return jacobian_raw(field, spacing, order)
+            ctx.save_for_backward(field)
+        return J
 
     @staticmethod
     def backward(ctx, grad_J):
-        (field,) = ctx.saved_tensors
+        (saved,) = ctx.saved_tensors
+        batched = grad_J.dim() == 4
+        if ctx.use_cof:
+            g = torch.empty(((saved.shape[0],) if batched else ()) + (3,) + tuple(saved.shape[-3:]),
+                            dtype=saved.dtype, device=saved.device)
+            for cf, gj, gf in zip(list(saved) if batched else [saved], list(grad_J) if batched else [grad_J],
+                                  list(g) if batched else [g]):
+                jacobian_adjoint_cof_raw(cf, gj, ctx.spacing, out=gf)
+            return g, None, None
+        field = saved
         if field.dim() == 5:
             g = torch.empty_like(field)
             for f, gj, gf in zip(field, grad_J, g):

@@ -259,6 +259,25 @@ int dtb_jacobian_adjoint_device(
     int precision, int order, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
     const void *field, const void *grad_J, void *grad_field, void *stream);
 
+/* The differentiable Jacobian split differently from the pair above: the
+ * forward also writes C[c][a] = cof_ca(I + A) * ih_a, the cofactors of the
+ * stencil matrix times the inverse spacing ([9][nz][ny][nx], c major), and
+ * the adjoint then needs only C and grad_J (grad_field = the gather of
+ * grad_J * C over the stencil's taps), so no pass re-reads the field.  No
+ * counterpart in the reference.  Fourth order only; rows a multiple of 16
+ * bytes long, `field`, `C` and `grad_J` 16-byte aligned, `J` and
+ * `grad_field` aligned to two elements; other layouts return
+ * DTB_ERR_ARGUMENT (use dtb_jacobian_device / dtb_jacobian_adjoint_device).
+ * The gradient equals dtb_jacobian_adjoint_device's up to the rounding of
+ * grad_J * (cof * ih) against (grad_J * cof) * ih.  Enqueued on `stream`, no
+ * wait, no device memory of their own. */
+int dtb_jacobian_cof_device(
+    int precision, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+    const void *field, void *J, void *C, void *stream);
+int dtb_jacobian_adjoint_cof_device(
+    int precision, size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+    const void *C, const void *grad_J, void *grad_field, void *stream);
+
 /* Jacobian determinant of a device-resident field, like dtb_jacobian_device,
  * but without allocating any memory.  No counterpart in the reference.  It
  * is for callers that cannot let the library allocate device memory: hosts

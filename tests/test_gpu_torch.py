@@ -174,3 +174,50 @@ def test_fused_adjoint_equals_two_pass(monkeypatch, dtype, shape):
         np.testing.assert_array_equal(a, b)
     else:
         np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(b).max())
+
+
+@pytest.mark.parametrize("shape", [(3, 3, 4), (7, 17, 36), (21, 40, 68), (40, 40, 96), (30, 53, 132)])
+def test_autograd_cofactor_path_matches_weight_path(monkeypatch, shape):
+    """The FP32 autograd forward that keeps C = cof * ih and the one-gather
+    backward (the default for TMA-friendly layouts) against the weight pass +
+    gather (DISPTOOLS_B200_AUTOGRAD=weights): the same map bit for bit, the
+    same gradient to float rounding (grad_J * (cof * ih) against
+    (grad_J * cof) * ih); single and batched fields."""
+    import torch
+    from disptools_b200 import torch_ops
+    from disptools_b200.synthetic import smooth_field
+    fields = np.stack([smooth_field(shape, sigma=2.0, max_disp=0.8, seed=s) for s in (3, 4)])
+    w = torch.from_numpy(np.random.default_rng(5).standard_normal((2,) + shape)).float().cuda()
+    sp = (0.9, 1.1, 1.3)
+
+    def run(batched):
+        f = torch.from_numpy(fields).float().cuda().requires_grad_(True)
+        if batched:
+            J = torch_ops.jacobian(f, sp)
+            (J * w).sum().backward()
+        else:
+            J = torch.stack([torch_ops.jacobian(f[b], sp) for b in range(2)])
+            (J * w).sum().backward()
+        return J.detach(), f.grad
+
+    assert torch_ops.cof_supported(torch.zeros((3,) + shape, device="cuda"))
+    for batched in (False, True):
+        Jc, gc = run(batched)
+        monkeypatch.setenv("DISPTOOLS_B200_AUTOGRAD", "weights")
+        Jw, gw = run(batched)
+        monkeypatch.delenv("DISPTOOLS_B200_AUTOGRAD")
+        torch.testing.assert_close(Jc, Jw, rtol=0, atol=0)
+        scale = gw.abs().max().item()
+        torch.testing.assert_close(gc, gw, rtol=1e-5, atol=1e-6 * scale)
+
+
+def test_autograd_cofactor_path_unsupported_layouts_fall_back():
+    """Widths that are not a multiple of four float32 elements and float64
+    fields take the weight pass + gather."""
+    import torch
+    from disptools_b200 import torch_ops
+    assert not torch_ops.cof_supported(torch.zeros((3, 8, 8, 9), device="cuda"))
+    assert not torch_ops.cof_supported(torch.zeros((3, 8, 8, 8), dtype=torch.float64, device="cuda"))
+    f = torch.rand((3, 8, 8, 9), device="cuda", requires_grad=True)
+    torch_ops.jacobian(f).sum().backward()
+    assert f.grad is not None and torch.isfinite(f.grad).all()
