@@ -221,3 +221,26 @@ def test_autograd_cofactor_path_unsupported_layouts_fall_back():
     f = torch.rand((3, 8, 8, 9), device="cuda", requires_grad=True)
     torch_ops.jacobian(f).sum().backward()
     assert f.grad is not None and torch.isfinite(f.grad).all()
+
+
+def test_cof_entry_points_reject_unsupported_layouts():
+    """The C entry points of the cofactor path refuse layouts their tensor
+    maps cannot cover (rows not a multiple of 16 bytes, misaligned bases)
+    with DTB_ERR_ARGUMENT and the error state set, and do no device work."""
+    import torch
+    from disptools_b200 import _native as N
+    f = torch.zeros((3, 8, 8, 9), device="cuda")
+    J = torch.zeros((8, 8, 9), device="cuda")
+    C = torch.zeros((9, 8, 8, 9), device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    rc = N.lib.dtb_jacobian_cof_device(N.PRECISION_MIXED, 9, 8, 8, 1.0, 1.0, 1.0, f.data_ptr(), J.data_ptr(),
+                                       C.data_ptr(), s)
+    assert rc == -1 and N.lib.disptools_has_error()
+    buf = torch.zeros(9 * 8 * 8 * 8 + 1, device="cuda")
+    C8 = buf[1:]  # 4 bytes off the allocation's alignment
+    gJ = torch.zeros((8, 8, 8), device="cuda")
+    g = torch.zeros((3, 8, 8, 8), device="cuda")
+    rc = N.lib.dtb_jacobian_adjoint_cof_device(N.PRECISION_MIXED, 8, 8, 8, 1.0, 1.0, 1.0, C8.data_ptr(),
+                                               gJ.data_ptr(), g.data_ptr(), s)
+    assert rc == -1 and N.lib.disptools_has_error()
+    N.lib.disptools_clear_error()
