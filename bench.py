@@ -56,7 +56,7 @@ def parse():
     p.add_argument("--no-greedy", action="store_true")
     p.add_argument("--no-other-configs", action="store_true",
                    help="skip the short runs of configs 3, 4 and 5 that the default line carries")
-    p.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "greedy"],
+    p.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "greedy", "matching"],
                    help="c2: one 256^3 volume per rank (default); c4: 64 volumes of "
                         "axes U{48..192} split over the ranks; c5: one 512x512x384 volume per "
                         "rank through a 3-level pyramid, plus greedy on the coarsest level; "
@@ -659,9 +659,88 @@ def greedy_leg(dt, torch_ops, torch, Jt, mask, field, stream, IT, nvox, world):
                          "launches": nl}}
 
 
+def run_matching(args, world, rank, local, quiet=False):
+    """The matching solver (volume_matching_3d, src/VolumeMatching3D.c:408-557,
+    on the device): a 128^3 volume of 16 Gaussian blobs (the config-2
+    generator), zero initial field, FP32, it_max = --it-max per step.  The
+    solver takes host arrays (its step control reads the cost after every
+    evaluation), so the step's time includes the host-device copies and is
+    the end-to-end figure as well.  The CPU baseline is the reference's own
+    volume_matching_3d on the same volume, ten iterations."""
+    import numpy as np
+    import torch
+
+    import disptools_b200 as dt
+    from disptools_b200.synthetic import blob_problem
+
+    torch.cuda.set_device(local)
+    n, IT = 128, args.it_max
+    Jt, mask = blob_problem((n, n, n), blobs=16, seed=rank)
+    nvox = n ** 3
+
+    def step():
+        out, st = dt.solve(Jt, mask, algorithm="matching", it_max=IT)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = dt.kernel_launch_count()
+    barrier(world)
+    iters = 0
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            iters += step()["iterations"]
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+    barrier(world)
+    ms = max_over_ranks(world, t * 1000.0)
+    launches = dt.kernel_launch_count() - launches0
+    value = sum_over_ranks(world, float(nvox) * iters) / (ms / 1000.0)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.oracle import Reference
+        if Reference.available("ref64_match"):
+            import ctypes
+            # The reference's gradient reads malloc'd buffers it never clears
+            # (src/VolumeMatching3D.c:422-427): perturb fills them with zeros.
+            ctypes.CDLL(None).mallopt(-6, 255)
+            ref = Reference("ref64_match")
+            t0 = time.perf_counter()
+            ref.solve("matching", Jt, mask, it_max=10)
+            tc = time.perf_counter() - t0
+            cpu = {"value": nvox * 10 / tc, "unit": UNIT,
+                   "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "reference",
+                   "sample": f"reference volume_matching_3d (OpenMP) on the same volume, 10 iterations: {tc:.2f} s"}
+    line = {
+        "metric": "matching-solver voxel-iters/s, 128^3 (16 blobs)", "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"matching solver on {n}^3 (16 Gaussian blobs), zero initial field, "
+                               f"it_max={IT} per step, host arrays",
+                   "iterations_per_step": iters / args.steps, "parallelism": f"{world} independent volumes"},
+        "roofline": None,
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": nvox * (8 + 1 + 24),
+                "d2h_bytes_per_step": nvox * 24,
+                "path": "api.solve(algorithm='matching'), host float64 arrays: the step time includes the copies"},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    if rank == 0 and not quiet:
+        print(json.dumps(line))
+    return line
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.workload == "matching" and args.impl == "b200":
+        run_matching(args, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.workload == "c5" and args.impl == "b200":
         run_c5(args, world, rank, local)
         if world > 1:
