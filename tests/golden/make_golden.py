@@ -11,6 +11,7 @@ as small .npz files.  Run it where the reference sources are available:
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py --maps   # maps.npz only
     python tests/golden/make_golden.py --config2   # config2_converged.json (minutes)
+    python tests/golden/make_golden.py --matching  # matching.npz only
 
 maps.npz comes from the reference's own Python map functions
 (disptools/displacements.py), executed from its source with the SimpleITK
@@ -208,6 +209,41 @@ def config2_converged(ref_verbose) -> dict:
     }
 
 
+def matching_fixtures() -> dict:
+    # Matching solver (src/VolumeMatching3D.c), FP32 arithmetic.  Its first
+    # gradient accumulates into malloc'd buffers it never clears
+    # (src/VolumeMatching3D.c:422-427 and :445): with whatever the allocator
+    # hands back its results are NaN or depend on earlier allocations.  This
+    # script therefore runs with MALLOC_PERTURB_=255 (see main), under which
+    # glibc fills every malloc'd block with zero bytes, i.e. the buffers
+    # start cleared, as every later gradient of the reference does.
+    refm = Reference("ref64_match")
+    mat = {}
+    for k, (shape, init, spacing, it_max) in enumerate([
+        ((20, 20, 20), False, (1.0, 1.0, 1.0), 60),
+        ((14, 12, 10), True, (1.0, 1.0, 1.0), 40),
+        ((12, 13, 11), False, (0.8, 1.1, 1.25), 40),
+        # several tiles along every axis of the device kernels, the last
+        # tile of each axis one point wider than the others
+        ((9, 17, 65), True, (1.0, 0.9, 1.2), 12),
+    ]):
+        if k == 0:
+            mask = ball(20, 10, 5)
+            Jt = np.where(mask, 1.1, 1.0)
+        else:
+            Jt, mask = small_problem(300 + k, shape)
+        field0 = (np.random.default_rng(400 + k).normal(scale=0.05, size=(3,) + shape)
+                  if init else np.zeros((3,) + shape))
+        out = refm.solve("matching", Jt, mask, field=field0, spacing=spacing, it_max=it_max)
+        mat[f"m{k}_Jt"] = Jt
+        mat[f"m{k}_mask"] = mask
+        mat[f"m{k}_field0"] = field0
+        mat[f"m{k}_spacing"] = np.array(spacing)
+        mat[f"m{k}_it_max"] = np.array(it_max)
+        mat[f"m{k}_out"] = out
+    return mat
+
+
 def main() -> None:
     if "--config2" in sys.argv:
         build(ref=True)
@@ -223,9 +259,13 @@ def main() -> None:
         return
     if os.environ.get("MALLOC_PERTURB_") != "255":
         # zero-filled mallocs for the reference matching solver (see below)
-        os.execve(sys.executable, [sys.executable, os.path.abspath(__file__)],
+        os.execve(sys.executable, [sys.executable, os.path.abspath(__file__)] + sys.argv[1:],
                   {**os.environ, "MALLOC_PERTURB_": "255"})
     build(ref=True)
+    if "--matching" in sys.argv:
+        np.savez_compressed(os.path.join(HERE, "matching.npz"), **matching_fixtures())
+        print("matching fixtures written to", HERE)
+        return
     ref = Reference("ref64")
     ref2 = Reference("ref64_pd2")
 
@@ -286,34 +326,7 @@ def main() -> None:
     with open(os.path.join(HERE, "solver_cases.json"), "w") as fh:
         json.dump({"cases": cases, "config1": c1}, fh, indent=1)
 
-    # Matching solver (src/VolumeMatching3D.c), FP32 arithmetic.  Its first
-    # gradient accumulates into malloc'd buffers it never clears
-    # (src/VolumeMatching3D.c:422-427 and :445): with whatever the allocator
-    # hands back its results are NaN or depend on earlier allocations.  This
-    # script therefore runs with MALLOC_PERTURB_=255 (see main), under which
-    # glibc fills every malloc'd block with zero bytes, i.e. the buffers
-    # start cleared, as every later gradient of the reference does.
-    refm = Reference("ref64_match")
-    mat = {}
-    for k, (shape, init, spacing, it_max) in enumerate([
-        ((20, 20, 20), False, (1.0, 1.0, 1.0), 60),
-        ((14, 12, 10), True, (1.0, 1.0, 1.0), 40),
-        ((12, 13, 11), False, (0.8, 1.1, 1.25), 40),
-    ]):
-        if k == 0:
-            mask = ball(20, 10, 5)
-            Jt = np.where(mask, 1.1, 1.0)
-        else:
-            Jt, mask = small_problem(300 + k, shape)
-        field0 = (np.random.default_rng(400 + k).normal(scale=0.05, size=(3,) + shape)
-                  if init else np.zeros((3,) + shape))
-        out = refm.solve("matching", Jt, mask, field=field0, spacing=spacing, it_max=it_max)
-        mat[f"m{k}_Jt"] = Jt
-        mat[f"m{k}_mask"] = mask
-        mat[f"m{k}_field0"] = field0
-        mat[f"m{k}_spacing"] = np.array(spacing)
-        mat[f"m{k}_it_max"] = np.array(it_max)
-        mat[f"m{k}_out"] = out
+    mat = matching_fixtures()
     np.savez_compressed(os.path.join(HERE, "matching.npz"), **mat)
     np.savez_compressed(os.path.join(HERE, "maps.npz"), **map_fixtures(ref))
     print("golden fixtures written to", HERE)
