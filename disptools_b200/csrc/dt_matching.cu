@@ -381,8 +381,13 @@ __global__ void __launch_bounds__(MT_THREADS) k_match_grad(MatchArgs a, int zc, 
     const int cx = a.nx - 1, cy = a.ny - 1, cz = a.nz - 1;
     const int x0 = blockIdx.x * MT_X, y0 = blockIdx.y * MG_Y, zb = blockIdx.z * zc;
     const int ze = min(zb + zc, a.nz);  // points' planes [zb, ze); cell layers zb - 1 .. ze - 1
-    // This thread's cell column: lowest corner (i, j), box point (ccx, ccy).
-    const int ccy = tid / MG_CX, ccx = tid - ccy * MG_CX;
+    // This thread's cell column: lowest corner (i, j), box point (ccx, ccy),
+    // slot cid = 33 ccy + ccx.  Warps 0-6 take the rows' first 32 cells
+    // (a warp reads one box row: no bank conflicts), the first 7 lanes of
+    // warp 7 the last column.
+    const int ccy = tid < MG_CY * MT_X ? tid / MT_X : tid - MG_CY * MT_X;
+    const int ccx = tid < MG_CY * MT_X ? tid % MT_X : MT_X;
+    const int cid = ccy * MG_CX + ccx;
     const int i = x0 - 1 + ccx, j = y0 - 1 + ccy;
     const bool ccol = tid < MG_CELLS && i >= 0 && i < cx && j >= 0 && j < cy;
     const float *tvp = a.TV + (ccol ? j * cx + i : 0);
@@ -467,7 +472,7 @@ __global__ void __launch_bounds__(MT_THREADS) k_match_grad(MatchArgs a, int zc, 
 #pragma unroll
             for (int n = 0; n < 8; ++n)
 #pragma unroll
-                for (int q = 0; q < 3; ++q) cs[n * 3 + q][tid] = acc[n][q];
+                for (int q = 0; q < 3; ++q) cs[n * 3 + q][cid] = acc[n][q];
         }
         __syncthreads();
         // The point (x, y) is corner 3 of cell (px, py), corner 1 of
