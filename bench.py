@@ -662,25 +662,41 @@ def greedy_leg(dt, torch_ops, torch, Jt, mask, field, stream, IT, nvox, world):
 def run_matching(args, world, rank, local, quiet=False):
     """The matching solver (volume_matching_3d, src/VolumeMatching3D.c:408-557,
     on the device): a 128^3 volume of 16 Gaussian blobs (the config-2
-    generator), zero initial field, FP32, it_max = --it-max per step.  The
-    solver takes host arrays (its step control reads the cost after every
-    evaluation), so the step's time includes the host-device copies and is
-    the end-to-end figure as well.  The CPU baseline is the reference's own
+    generator), zero initial field, it_max = --it-max per step.  `value`
+    solves device-resident float64 tensors (dtb_volume_matching_device, the
+    initial field zeroed on the device inside the step); `e2e` calls the C
+    ABI (dtb_volume_matching) on pinned host float64 arrays, the zero initial
+    guess written before each timed call, the copies inside.  The roofline is
+    the gradient kernel's (28 algorithmic bytes per grid point: positions 12
+    in, cell targets 4 in, step 12 out), timed by the library's profiling
+    events over one further solve.  The CPU baseline is the reference's own
     volume_matching_3d on the same volume, ten iterations."""
+    import ctypes as C
+
     import numpy as np
     import torch
 
     import disptools_b200 as dt
+    from disptools_b200 import _native as N
+    from disptools_b200 import torch_ops
+    from disptools_b200.api import make_params
     from disptools_b200.synthetic import blob_problem
 
     torch.cuda.set_device(local)
     n, IT = 128, args.it_max
     Jt, mask = blob_problem((n, n, n), blobs=16, seed=rank)
     nvox = n ** 3
+    dev = torch.device("cuda", local)
+    Jd = torch.from_numpy(np.ascontiguousarray(Jt)).to(dev)
+    md = torch.from_numpy(np.ascontiguousarray(mask)).to(dev)
+    fd = torch.zeros((3, n, n, n), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    scrub = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # twice the L2
 
     def step():
-        out, st = dt.solve(Jt, mask, algorithm="matching", it_max=IT)
-        return st
+        scrub.fill_(1)  # flush L2 between steps
+        fd.zero_()
+        return torch_ops.solve(Jd, md, fd, algorithm="matching", it_max=IT)
 
     for _ in range(args.warmup):
         step()
@@ -688,43 +704,103 @@ def run_matching(args, world, rank, local, quiet=False):
     launches0 = dt.kernel_launch_count()
     barrier(world)
     iters = 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
-        t0 = time.perf_counter()
+        torch.cuda.synchronize()
+        e0.record(stream)
         for _ in range(args.steps):
             iters += step()["iterations"]
+        e1.record(stream)
         torch.cuda.synchronize()
-        t = time.perf_counter() - t0
     barrier(world)
-    ms = max_over_ranks(world, t * 1000.0)
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
     launches = dt.kernel_launch_count() - launches0
     value = sum_over_ranks(world, float(nvox) * iters) / (ms / 1000.0)
+
+    # the gradient kernel's roofline: one more solve with profiling on
+    dt.set_profiling(True)
+    step()
+    torch.cuda.synchronize()
+    prof = dt.kernel_profile()
+    dt.set_profiling(False)
+    hbm, peak_kind = peaks()
+    ng, tg = prof.get("match_gradient", (0, 0.0))
+    nc, tc = prof.get("match_cost", (0, 0.0))
+    avg = tg / max(ng, 1)
+    bpl = 28 * nvox
+    achieved = bpl / (avg / 1000.0) / 1e9 if avg > 0 else 0.0
+    traffic = None
+    try:
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["match_gradient"][
+            "bytes_per_launch_128"]
+    except Exception:
+        traffic = None
+    roofline = {"bound": "hbm", "kernel": "matching gradient", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "peak_source": peak_kind, "bytes_per_launch": bpl,
+                "avg_launch_ms": avg, "launches": ng,
+                "cost_kernel": {"launches": nc, "avg_ms": tc / max(nc, 1)},
+                "note": "issue-bound FP32 arithmetic (72 cofactors per cell under the reference's rounding); "
+                        "the working set stays in L2"}
+
+    # end to end through the C ABI on pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+        Jh = pin(np.ascontiguousarray(Jt))
+        mh = pin(np.ascontiguousarray(mask))
+        fh = pin(np.zeros((3, n, n, n)))
+        prm = make_params(it_max=IT)
+        stt = N.SolveStats()
+
+        def e2e_step():
+            fh[...] = 0.0
+            t0 = time.perf_counter()
+            rc = N.lib.dtb_volume_matching(n, n, n, 1.0, 1.0, 1.0, Jh.ctypes.data, mh.ctypes.data,
+                                           C.byref(prm), fh.ctypes.data, C.byref(stt))
+            dt_s = time.perf_counter() - t0
+            N.check(rc)
+            return stt.as_dict(), dt_s
+
+        e2e_step()
+        barrier(world)
+        te, ie = 0.0, 0
+        for _ in range(args.steps):
+            st_e, dt_s = e2e_step()
+            ie += st_e["iterations"]
+            te += dt_s
+        te = max_over_ranks(world, te)
+        e2e = {"value": sum_over_ranks(world, float(nvox) * ie) / te, "unit": UNIT,
+               "h2d_bytes_per_step": int(Jh.nbytes + fh.nbytes), "d2h_bytes_per_step": int(fh.nbytes),
+               "steps": args.steps, "ms_per_step": te * 1000.0 / args.steps,
+               "path": "dtb_volume_matching (C ABI, host float64 arrays in pinned memory; the mask is not "
+                       "read, as by the reference)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle.oracle import Reference
         if Reference.available("ref64_match"):
-            import ctypes
             # The reference's gradient reads malloc'd buffers it never clears
             # (src/VolumeMatching3D.c:422-427): perturb fills them with zeros.
-            ctypes.CDLL(None).mallopt(-6, 255)
+            C.CDLL(None).mallopt(-6, 255)
             ref = Reference("ref64_match")
             t0 = time.perf_counter()
             ref.solve("matching", Jt, mask, it_max=10)
-            tc = time.perf_counter() - t0
-            cpu = {"value": nvox * 10 / tc, "unit": UNIT,
+            tcpu = time.perf_counter() - t0
+            cpu = {"value": nvox * 10 / tcpu, "unit": UNIT,
                    "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "reference",
-                   "sample": f"reference volume_matching_3d (OpenMP) on the same volume, 10 iterations: {tc:.2f} s"}
+                   "sample": f"reference volume_matching_3d (OpenMP) on the same volume, 10 iterations: {tcpu:.2f} s"}
     line = {
         "metric": "matching-solver voxel-iters/s, 128^3 (16 blobs)", "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"matching solver on {n}^3 (16 Gaussian blobs), zero initial field, "
-                               f"it_max={IT} per step, host arrays",
-                   "iterations_per_step": iters / args.steps, "parallelism": f"{world} independent volumes"},
-        "roofline": None,
+                               f"it_max={IT} per step, device-resident float64 arrays",
+                   "iterations_per_step": iters / args.steps, "parallelism": f"{world} independent volumes",
+                   "l2": "flushed between steps (256 MB write); within a solve the working set (positions, "
+                         "step and next positions, 25 MB each) stays in L2"},
+        "roofline": roofline,
         "cpu_baseline": cpu,
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": nvox * (8 + 1 + 24),
-                "d2h_bytes_per_step": nvox * 24,
-                "path": "api.solve(algorithm='matching'), host float64 arrays: the step time includes the copies"},
+        "e2e": e2e,
         "gpu_launches": launches, "clocks": clk.summary(),
     }
     if rank == 0 and not quiet:

@@ -160,6 +160,9 @@ lib.volume_matching_3d.restype = None
 lib.dtb_volume_matching.argtypes = [_SZ, _SZ, _SZ, _D, _D, _D, _P, _P, C.POINTER(Params), _P,
                                     C.POINTER(SolveStats)]
 lib.dtb_volume_matching.restype = _I
+lib.dtb_volume_matching_device.argtypes = [_SZ, _SZ, _SZ, _D, _D, _D, _P, C.POINTER(Params), _P,
+                                           C.POINTER(SolveStats), _P]
+lib.dtb_volume_matching_device.restype = _I
 lib.dtb_set_device_memory_limit.argtypes = [_SZ]
 lib.dtb_set_device_memory_limit.restype = _I
 lib.dtb_test_drop_tma_load.argtypes = [C.c_longlong, _I, C.c_uint]
@@ -197,7 +200,8 @@ EXPORTED = [
     "dtb_smooth_recursive_device", "dtb_resample_device",
     "dtb_write_rvf", "dtb_read_rvf_header", "dtb_read_rvf", "dtb_write_vtk", "dtb_read_vtk_header",
     "dtb_read_vtk", "dtb_volume_change_device", "dtb_log_jacobian_accumulate_device",
-    "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching", "dtb_set_verbose",
+    "dtb_exp_mean_device", "volume_matching_3d", "dtb_volume_matching", "dtb_volume_matching_device",
+    "dtb_set_verbose",
     "dtb_set_device_memory_limit", "dtb_test_drop_tma_load",
 ]
 

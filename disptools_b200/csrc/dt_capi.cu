@@ -82,16 +82,28 @@ extern "C" unsigned long long dtb_kernel_launch_count(void) { return g_launches.
 // the captured step graph.
 // ---------------------------------------------------------------------------
 namespace {
-enum { PROF_TRIAL = 0, PROF_GRADIENT = 1, PROF_KINDS = 2 };
-const char *const kProfNames[PROF_KINDS] = {"trial", "gradient"};
+enum { PROF_TRIAL = 0, PROF_GRADIENT = 1, PROF_KINDS = 2 + dtb::PROF_MATCH_KINDS };
+const char *const kProfNames[PROF_KINDS] = {"trial", "gradient", "match_gradient", "match_cost"};
 struct Profile {
     bool on = false;
-    long long launches[PROF_KINDS] = {0, 0};
-    double ms[PROF_KINDS] = {0.0, 0.0};
+    long long launches[PROF_KINDS] = {};
+    double ms[PROF_KINDS] = {};
 };
 std::mutex g_prof_mutex;
 Profile g_prof;
 }  // namespace
+
+bool dtb::profiling_on() {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    return g_prof.on;
+}
+
+void dtb::profile_match(int kind, double ms) {
+    std::lock_guard<std::mutex> lock(g_prof_mutex);
+    if (!g_prof.on || kind < 0 || kind >= PROF_MATCH_KINDS) return;
+    g_prof.launches[2 + kind]++;
+    g_prof.ms[2 + kind] += ms;
+}
 
 extern "C" int dtb_set_profiling(int on) {
     std::lock_guard<std::mutex> lock(g_prof_mutex);
@@ -1268,6 +1280,23 @@ extern "C" int dtb_generate_displacement_batched_device(int algorithm, int preci
                                                         const dtb_params *params, dtb_solve_stats *stats,
                                                         void *stream) {
     disptools_clear_error();
+    if (algorithm == DTB_ALGORITHM_MATCHING) {
+        // The matching solver, one volume after the other, on float64 arrays.
+        if (precision != DTB_PRECISION_FP64)
+            DTB_FAIL(DTB_ERR_ARGUMENT, "the matching solver takes float64 device arrays");
+        if (!params || count < 1 || !volumes) DTB_FAIL(DTB_ERR_ARGUMENT, "null argument");
+        const char *why = nullptr;
+        if (!check_params(*params, &why)) DTB_FAIL(DTB_ERR_ARGUMENT, why);
+        for (int i = 0; i < count; ++i) {
+            const dtb_device_volume &v = volumes[i];
+            const int rc = dtb_volume_matching_device(v.nx, v.ny, v.nz, v.dx, v.dy, v.dz,
+                                                      static_cast<const double *>(v.J), params,
+                                                      static_cast<double *>(v.field), stats ? &stats[i] : nullptr,
+                                                      stream);
+            if (rc != DTB_OK) return rc;
+        }
+        return DTB_OK;
+    }
     if (algorithm != DTB_ALGORITHM_GRADIENT && algorithm != DTB_ALGORITHM_GREEDY)
         DTB_FAIL(DTB_ERR_ARGUMENT, "invalid algorithm");
     if (precision != DTB_PRECISION_MIXED && precision != DTB_PRECISION_FP64)

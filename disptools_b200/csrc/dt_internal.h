@@ -204,6 +204,12 @@ cudaError_t launch_regularise(T *J, long long n, double eps, cudaStream_t s);
 template <typename T>
 cudaError_t launch_boundary_nonzero(const T *field, const Geom &g, int *flag, cudaStream_t s);
 
+// Kernel profiling (dtb_set_profiling): whether it is on, and one timed
+// launch of a matching-solver kernel (PROF_MATCH_GRAD or PROF_MATCH_COST).
+enum { PROF_MATCH_GRAD = 0, PROF_MATCH_COST = 1, PROF_MATCH_KINDS = 2 };
+bool profiling_on();
+void profile_match(int kind, double ms);
+
 // Kernel-launch counter (host side).  Launches issued while a stream is being
 // captured are not counted; each replay of a graph counts its kernels.
 void count_launch(unsigned n = 1);

@@ -571,29 +571,50 @@ struct DeviceBuffers {
     }
 };
 
+// Four timing events, destroyed with the object.
+struct Events {
+    cudaEvent_t e[4] = {};
+    bool create() {
+        for (cudaEvent_t &x : e)
+            if (cudaEventCreate(&x) != cudaSuccess) {
+                cudaGetLastError();
+                x = nullptr;
+                return false;
+            }
+        return true;
+    }
+    ~Events() {
+        for (cudaEvent_t x : e)
+            if (x) cudaEventDestroy(x);
+    }
+};
+
 }  // namespace
 
-// volume_matching_3d with statistics; `mask` is not used, as by the
-// reference (:727).  Returns DTB_OK or a DTB_ERR_* code.
-extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz, const double *J,
-                                   const bool *mask, const dtb_params *params, double *field,
-                                   dtb_solve_stats *stats) {
-    (void) mask;
+namespace {
+
+// The solve.  J [nz][ny][nx] and field [3][nz][ny][nx] (in: the initial
+// guess, out: the result) are host arrays, copied in and out, or with
+// `device` device arrays used in place; the work runs on `s`.  `entry`
+// names the caller in argument errors.  Returns DTB_OK or a DTB_ERR_* code.
+int matching_solve(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz, const double *J,
+                   const dtb_params *params, double *field, dtb_solve_stats *stats, bool device, cudaStream_t s,
+                   const char *entry) {
     disptools_clear_error();
     if (!J || !field || !params) {
-        report(__LINE__, __func__, "null argument");
+        report(__LINE__, entry, "null argument");
         return DTB_ERR_ARGUMENT;
     }
     if (nx < 2 || ny < 2 || nz < 2) {
-        report(__LINE__, __func__, "every axis needs at least 2 voxels");
+        report(__LINE__, entry, "every axis needs at least 2 voxels");
         return DTB_ERR_ARGUMENT;
     }
     if (3 * nx * ny * nz >= (1ull << 32)) {
-        report(__LINE__, __func__, "volume too large (3 n must stay below 2^32)");
+        report(__LINE__, entry, "volume too large (3 n must stay below 2^32)");
         return DTB_ERR_ARGUMENT;
     }
     if (!(dx > 0.0 && dy > 0.0 && dz > 0.0)) {
-        report(__LINE__, __func__, "spacing must be positive");
+        report(__LINE__, entry, "spacing must be positive");
         return DTB_ERR_ARGUMENT;
     }
     const dtb_params &p = *params;
@@ -603,7 +624,8 @@ extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, d
     // Positions (current and moved) and the gradient step, [3][n] each.
     float *cur = b.take<float>(3 * n), *next = b.take<float>(3 * n), *step = b.take<float>(3 * n);
     float *tv = b.take<float>(cells);
-    double *dfield = b.take<double>(3 * n), *dJ = b.take<double>(n);
+    double *dfield = device ? field : b.take<double>(3 * n);
+    const double *dJ = device ? J : b.take<double>(n);
     // Launch shapes: 32 x 8 cell columns (cost) or 32 x 6 point columns
     // (gradient) per block, runs of zc planes, about eight blocks per SM in all.
     const int ncx = (int) nx - 1, ncy = (int) ny - 1, ncz = (int) nz - 1;
@@ -622,10 +644,11 @@ extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, d
         report(__LINE__, __func__, "cannot allocate device buffers");
         return DTB_ERR_ALLOC;
     }
-    cudaStream_t s = nullptr;
     M_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), s));
-    M_CUDA(cudaMemcpy(dfield, field, 3 * n * sizeof(double), cudaMemcpyHostToDevice));
-    M_CUDA(cudaMemcpy(dJ, J, n * sizeof(double), cudaMemcpyHostToDevice));
+    if (!device) {
+        M_CUDA(cudaMemcpyAsync(dfield, field, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+        M_CUDA(cudaMemcpyAsync(const_cast<double *>(dJ), J, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
     k_match_prepare<<<grid_for(n), 256, 0, s>>>(dfield, dJ, (int) nx, (int) ny, (int) nz, dx, dy, dz, cur, cur + n,
                                                 cur + 2 * n, tv);
     count_launch();
@@ -634,12 +657,18 @@ extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, d
     const float eps = (float) p.delta, zeta = (float) p.zeta;
     double2 h_res;
     double max_voxel_error = DBL_MAX;
+    // Profiling (dtb_set_profiling): events around the gradient and cost
+    // launches, read after the host wait that follows every cost.
+    Events ev;
+    const bool prof = profiling_on() && ev.create();
+    bool grad_timed = false;
     // Cost of the current positions (alpha < 0) or of the positions moved by
     // alpha, which are then in `next`; updates max_voxel_error like the
     // reference's global (:103, :176-179).
     auto cost = [&](float alpha, float *H) -> int {
         const MatchArgs a{cur, tv, (int) nx, (int) ny, (int) nz, (unsigned) n, eps, zeta};
         double2 *res = partial + cost_blocks;
+        if (prof) M_CUDA(cudaEventRecord(ev.e[2], s));
         if (alpha < 0.0f) {
             k_match_cost<false><<<cost_grid, MT_THREADS, 0, s>>>(a, MoveArgs{}, zc_cost, partial, counter, res);
         } else {
@@ -648,16 +677,30 @@ extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, d
         }
         count_launch();
         M_CUDA(cudaGetLastError());
-        M_CUDA(cudaMemcpy(&h_res, res, sizeof h_res, cudaMemcpyDeviceToHost));
+        if (prof) M_CUDA(cudaEventRecord(ev.e[3], s));
+        M_CUDA(cudaMemcpyAsync(&h_res, res, sizeof h_res, cudaMemcpyDeviceToHost, s));
+        M_CUDA(cudaStreamSynchronize(s));
         *H = (float) h_res.x;
         max_voxel_error = h_res.y;
+        if (prof) {
+            float ms = 0.0f;
+            if (grad_timed && cudaEventElapsedTime(&ms, ev.e[0], ev.e[1]) == cudaSuccess)
+                profile_match(PROF_MATCH_GRAD, ms);
+            if (cudaEventElapsedTime(&ms, ev.e[2], ev.e[3]) == cudaSuccess) profile_match(PROF_MATCH_COST, ms);
+            grad_timed = false;
+        }
         return DTB_OK;
     };
     auto grads = [&]() -> int {
         const MatchArgs a{cur, tv, (int) nx, (int) ny, (int) nz, (unsigned) n, eps, zeta};
+        if (prof) M_CUDA(cudaEventRecord(ev.e[0], s));
         k_match_grad<<<grad_grid, MT_THREADS, 0, s>>>(a, zc_grad, step);
         count_launch();
         M_CUDA(cudaGetLastError());
+        if (prof) {
+            M_CUDA(cudaEventRecord(ev.e[1], s));
+            grad_timed = true;
+        }
         return DTB_OK;
     };
     auto move = [&](float alpha) -> int {
@@ -716,7 +759,8 @@ extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, d
                                                dfield);
     count_launch();
     M_CUDA(cudaGetLastError());
-    M_CUDA(cudaMemcpy(field, dfield, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (!device) M_CUDA(cudaMemcpyAsync(field, dfield, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    M_CUDA(cudaStreamSynchronize(s));
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
         stats->iterations = itnum;
@@ -728,6 +772,26 @@ extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, d
                                        : (alpha > 0.000000001 ? DTB_STOP_EPSILON : DTB_STOP_ETA);
     }
     return DTB_OK;
+}
+
+}  // namespace
+
+// volume_matching_3d with statistics, host arrays; `mask` is not used, as by
+// the reference (:727).  Returns DTB_OK or a DTB_ERR_* code.
+extern "C" int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz, const double *J,
+                                   const bool *mask, const dtb_params *params, double *field,
+                                   dtb_solve_stats *stats) {
+    (void) mask;
+    return matching_solve(nx, ny, nz, dx, dy, dz, J, params, field, stats, false, nullptr, __func__);
+}
+
+// The same on device arrays (J and field device pointers of doubles), on
+// `stream`; returns once the solve is complete.
+extern "C" int dtb_volume_matching_device(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+                                          const double *J, const dtb_params *params, double *field,
+                                          dtb_solve_stats *stats, void *stream) {
+    return matching_solve(nx, ny, nz, dx, dy, dz, J, params, field, stats, true,
+                          static_cast<cudaStream_t>(stream), __func__);
 }
 
 // Replaces volume_matching_3d (src/VolumeMatching3D.c:689-796), computed

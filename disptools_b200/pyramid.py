@@ -128,15 +128,16 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
     element type.
     ``spacing`` is (dx, dy, dz).  ``precision`` selects the device solver
     (``"mixed"``: FP32 fields, ``"fp64"``); the target and mask pyramids are
-    built in FP64.  With ``return_stats`` also returns the per-level solver
+    built in FP64.  ``algorithm`` is "gradient", "greedy" or "matching"; the
+    matching solver always keeps float64 fields (it computes in FP32).  With ``return_stats`` also returns the per-level solver
     statistics, coarsest first.  ``smoothing`` is the anti-aliasing filter
     of every scaling: "recursive" (the default) or "sampled"."""
     if smoothing not in SMOOTHING:
         raise ValueError(f"smoothing must be one of {SMOOTHING}")
     if levels < 1:
         raise ValueError("levels must be at least 1")
-    if algorithm not in ("gradient", "greedy"):
-        raise ValueError("algorithm must be 'gradient' or 'greedy' ('matching' has no device path)")
+    if algorithm not in ("gradient", "greedy", "matching"):
+        raise ValueError("algorithm must be 'gradient', 'greedy' or 'matching'")
     if precision not in ("mixed", "fp64"):
         raise ValueError("precision must be 'mixed' or 'fp64'")
     if isinstance(it_max, (list, tuple)):
@@ -188,7 +189,8 @@ def displacement(jacobian, *, levels: int = 1, pad: int = 0, redistribute: bool 
         m0 = torch.from_numpy(m).to(dev)
         shape0 = J.shape
 
-    ftype = torch.float64 if precision == "fp64" else torch.float32
+    # The matching solver takes float64 arrays (it computes in FP32 inside).
+    ftype = torch.float64 if precision == "fp64" or algorithm == "matching" else torch.float32
     sizes, spacings = level_geometry(shape0, spacing, levels)
     # Every coarser level is scaled from the same full-resolution images with
     # the same smoothing (2.0 physical units at the finest spacing), so each

@@ -219,7 +219,9 @@ def solve(J: torch.Tensor, mask: torch.Tensor, field: torch.Tensor,
 
 def solve_batched(volumes, algorithm: str = "gradient", **params):
     """Batched in-place solve of ``(J, mask, field[, spacing])`` device
-    tensors; all volumes share one dtype (float32 = mixed, float64 = FP64)."""
+    tensors; all volumes share one dtype (float32 = mixed, float64 = FP64).
+    The matching solver takes float64 tensors and solves the volumes one
+    after the other (its mask is not used, as by the reference)."""
     vols = list(volumes)
     arr = (N.Volume * len(vols))()
     prec = None

@@ -236,6 +236,16 @@ int dtb_volume_matching(size_t nx, size_t ny, size_t nz, double dx, double dy, d
                         const double *J, const bool *mask, const dtb_params *params,
                         double *field, dtb_solve_stats *stats);
 
+/* The matching solver on device arrays: `J` [nz][ny][nx] and `field`
+ * [3][nz][ny][nx] (in: initial guess, out: result) are device pointers of
+ * doubles; the work runs on `stream` (a cudaStream_t or NULL).  Its step
+ * control reads every cost evaluation on the host, so the call returns once
+ * the solve is complete.  dtb_generate_displacement_batched_device with
+ * DTB_ALGORITHM_MATCHING and DTB_PRECISION_FP64 runs this per volume. */
+int dtb_volume_matching_device(size_t nx, size_t ny, size_t nz, double dx, double dy, double dz,
+                               const double *J, const dtb_params *params, double *field,
+                               dtb_solve_stats *stats, void *stream);
+
 /* Jacobian determinant of a device-resident field (reference stencil and
  * boundary rules, src/jacobian.c:70-242).  `field` is [3][nz][ny][nx] and
  * `J` [nz][ny][nx], both device pointers of the element type of
@@ -482,11 +492,15 @@ int dtb_release_device_memory(void);
  * replay of a captured step graph counts the kernels it contains). */
 unsigned long long dtb_kernel_launch_count(void);
 
-/* Per-kernel profile of the solver: launches that did work and their summed
+/* Per-kernel profile of the solvers: launches that did work and their summed
  * device time, measured with CUDA events recorded between the kernels of the
- * step graph while profiling is on. */
+ * step graph (gradient and greedy solvers) or around each launch (matching
+ * solver) while profiling is on. */
 typedef struct dtb_kernel_profile {
-    char name[32];        /* "trial" or "gradient" */
+    char name[32];        /* "trial", "gradient" (gradient and greedy
+                             solvers), "match_gradient", "match_cost"
+                             (matching solver; the cost kernel includes the
+                             trial move) */
     long long launches;
     double total_ms;
 } dtb_kernel_profile;

@@ -219,11 +219,12 @@ def scale_image(vol: np.ndarray, spacing_xyz, size_zyx, nearest: bool = False,
 
 def displacement(jacobian, *, levels=1, pad=0, redistribute=False, mask=None, initial_guess=None,
                  spacing=(1.0, 1.0, 1.0), it_max=50000, algorithm="gradient", field_dtype=np.float64,
-                 smoothing="recursive", **params):
+                 smoothing="recursive", solver=None, **params):
     """disptools/displacements.py:238-480 on NumPy arrays, each level solved
-    by the C oracle.  ``field_dtype`` float32 rounds the fields passed
-    between levels like the mixed-precision device path."""
-    o = Oracle(4)
+    by the C oracle (or by ``solver``, an object with the oracle's ``solve``,
+    such as the reference library).  ``field_dtype`` float32 rounds the
+    fields passed between levels like the mixed-precision device path."""
+    o = solver if solver is not None else Oracle(4)
     J = np.array(jacobian, dtype=np.float64)
     m = np.ones(J.shape) if mask is None else np.asarray(mask, dtype=np.float64)
     its = list(it_max) if isinstance(it_max, (list, tuple)) else [it_max] * levels
@@ -247,8 +248,9 @@ def displacement(jacobian, *, levels=1, pad=0, redistribute=False, mask=None, in
         if field is not None:
             field = scale_image(field.astype(field_dtype), field_spacing, sizes[lv], method=smoothing)
         f0 = None if field is None else field.astype(np.float64)
-        out, _ = o.solve(algorithm, np.ascontiguousarray(Js[lv]), np.ascontiguousarray(ms[lv] != 0),
-                         field=f0, spacing=spacings[lv], it_max=it, **params)
+        out = o.solve(algorithm, np.ascontiguousarray(Js[lv]), np.ascontiguousarray(ms[lv] != 0),
+                      field=f0, spacing=spacings[lv], it_max=it, **params)
+        out = out[0] if isinstance(out, tuple) else out  # the oracle also returns its statistics
         field = out.astype(field_dtype)
         field_spacing = spacings[lv]
     return field[:, p:-p, p:-p, p:-p].astype(np.float64)             # :483

@@ -244,6 +244,18 @@ def matching_fixtures() -> dict:
     return mat
 
 
+def matching_pyramid_fixture() -> dict:
+    # The multi-resolution wrapper (disptools/displacements.py:238-480, as
+    # restated in oracle/pyramid.py) with the reference's matching solver at
+    # every level: two levels, one voxel of padding, anisotropic spacing.
+    from oracle import pyramid as P
+    Jt, mask = small_problem(330, (18, 20, 22))
+    kw = dict(levels=2, it_max=[15, 15], spacing=(1.0, 1.1, 0.9))
+    out = P.displacement(Jt, mask=mask, algorithm="matching", solver=Reference("ref64_match"), **kw)
+    return {"Jt": Jt, "mask": mask, "spacing": np.array(kw["spacing"]), "it_max": np.array(kw["it_max"]),
+            "levels": np.array(kw["levels"]), "out": out}
+
+
 def main() -> None:
     if "--config2" in sys.argv:
         build(ref=True)
@@ -264,6 +276,7 @@ def main() -> None:
     build(ref=True)
     if "--matching" in sys.argv:
         np.savez_compressed(os.path.join(HERE, "matching.npz"), **matching_fixtures())
+        np.savez_compressed(os.path.join(HERE, "matching_pyramid.npz"), **matching_pyramid_fixture())
         print("matching fixtures written to", HERE)
         return
     ref = Reference("ref64")
@@ -328,6 +341,7 @@ def main() -> None:
 
     mat = matching_fixtures()
     np.savez_compressed(os.path.join(HERE, "matching.npz"), **mat)
+    np.savez_compressed(os.path.join(HERE, "matching_pyramid.npz"), **matching_pyramid_fixture())
     np.savez_compressed(os.path.join(HERE, "maps.npz"), **map_fixtures(ref))
     print("golden fixtures written to", HERE)
 

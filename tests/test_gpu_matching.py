@@ -68,3 +68,41 @@ def test_matching_cost_decreases_and_stops():
     # a loose epsilon stops the solver before it_max
     _, s2 = dt.solve(Jt, m, algorithm="matching", it_max=500, epsilon=0.05)
     assert s2["iterations"] < 500 and s2["max_error"] <= 0.05
+
+
+def test_matching_device_entry_equals_host(cases):
+    """dtb_volume_matching_device (through torch_ops.solve on float64
+    tensors, on a side stream) gives the host entry's field bit for bit;
+    float32 tensors are refused."""
+    import torch
+
+    from disptools_b200 import torch_ops
+    Jt, m, f0, sp, it, _ = cases[3]
+    a, sa = dt.solve(Jt, m, f0, spacing=tuple(sp), algorithm="matching", it_max=int(it))
+    Jd, md = torch.from_numpy(Jt).cuda(), torch.from_numpy(m).cuda()
+    fd = torch.from_numpy(f0.copy()).cuda()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        st = torch_ops.solve(Jd, md, fd, spacing=tuple(sp), algorithm="matching", it_max=int(it))
+    torch.cuda.current_stream().wait_stream(side)
+    np.testing.assert_array_equal(fd.cpu().numpy(), a)
+    assert (st["iterations"], st["reason"]) == (sa["iterations"], sa["reason"])
+    with pytest.raises(ValueError):
+        torch_ops.solve(Jd.float(), md, fd.float(), spacing=tuple(sp), algorithm="matching", it_max=1)
+
+
+def test_matching_profile_counts_kernels():
+    """With profiling on, every gradient and cost launch of the matching
+    solver is timed."""
+    Jt, m = ball_problem(20, 10, 5, 1.1)
+    dt.set_profiling(True)
+    try:
+        _, st = dt.solve(Jt, m, algorithm="matching", it_max=5)
+        prof = dt.kernel_profile()
+    finally:
+        dt.set_profiling(False)
+    assert st["iterations"] == 5
+    g, c = prof["match_gradient"], prof["match_cost"]
+    assert g[0] >= 5 and c[0] >= g[0] + 1
+    assert g[1] > 0.0 and c[1] > 0.0

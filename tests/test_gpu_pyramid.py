@@ -1,8 +1,10 @@
 """Multi-resolution pyramid on the device against its CPU restatement
 (oracle/pyramid.py): the smoothing and resampling kernels bit for bit, the
 driver through the FP64 solver to 1e-10, the mixed path by the residual
-rule."""
+rule, the matching solver against the reference's own at every level."""
 from __future__ import annotations
+
+import os
 
 import numpy as np
 import pytest
@@ -97,4 +99,20 @@ def test_driver_argument_errors():
     with pytest.raises(ValueError):
         D.displacement(Jt, mask=mask[:-1])
     with pytest.raises(ValueError):
-        D.displacement(Jt, mask=mask, algorithm="matching")
+        D.displacement(Jt, mask=mask, algorithm="newton")
+
+
+def test_driver_matching_matches_reference():
+    """The wrapper with the matching solver at every level against the
+    reference's volume_matching_3d run through the restated pyramid
+    (tests/golden/matching_pyramid.npz; both solvers compute in FP32, fields
+    agree to 2e-3 as for one level).  A device tensor gives the same field."""
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "matching_pyramid.npz"))
+    kw = dict(levels=int(d["levels"]), it_max=[int(v) for v in d["it_max"]], spacing=tuple(d["spacing"]),
+              algorithm="matching")
+    got = D.displacement(d["Jt"], mask=d["mask"], **kw)
+    assert got.shape == d["out"].shape
+    assert np.max(np.abs(got - d["out"])) <= 2e-3
+    dev = D.displacement(torch.from_numpy(d["Jt"]).cuda(), mask=torch.from_numpy(d["mask"]).cuda(), **kw)
+    assert dev.dtype == torch.float64
+    np.testing.assert_array_equal(dev.cpu().numpy(), got)
