@@ -179,6 +179,16 @@ def workload_c2(algorithm: str, n: int, it_max: int) -> str:
             f"the reference's default parameters, it_max={it_max} per step")
 
 
+def workload_matching(n: int, it_max: int) -> str:
+    """The workload string of the matching lines (both arms)."""
+    return (f"matching solver on {n}^3 (16 Gaussian blobs), zero initial field, the reference's default "
+            f"parameters, it_max={it_max} per step")
+
+
+MATCHING_SIZE = 128
+MATCHING_SAMPLE_ITERATIONS = 10
+
+
 def reference_impl():
     """The reference C library's FP64 build with its stock verbose output
     (what its Python package builds, setup.py: DISPTOOLS_VERBOSE=ON), which
@@ -234,6 +244,9 @@ def run_reference_arm(args, world, rank):
     if args.workload == "c3":
         run_reference_c3(args)
         return
+    if args.workload == "matching":
+        run_reference_matching(args)
+        return
     # the seeded generator only: this arm loads no library of this package
     from disptools_b200.synthetic import blob_problem
     n = args.size
@@ -269,6 +282,49 @@ def run_reference_arm(args, world, rank):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
+
+
+def run_reference_matching(args):
+    """The reference's volume_matching_3d (oracle/_ref, FP64 build, OpenMP)
+    on the matching line's volume; each step a bounded sample of ten
+    iterations of the same solve (the rate is per voxel-iteration)."""
+    import ctypes as C
+
+    from disptools_b200.synthetic import blob_problem
+    from oracle.oracle import Reference
+    n, IT = MATCHING_SIZE, args.it_max
+    metric = "matching-solver voxel-iters/s, 128^3 (16 blobs)"
+    if not Reference.available("ref64_match"):
+        print(json.dumps({"impl": "reference", "metric": metric,
+                          "unavailable": "the reference matching build (oracle/_ref) is missing"}))
+        return
+    # The reference's gradient reads malloc'd buffers it never clears
+    # (src/VolumeMatching3D.c:422-427): perturb fills them with zeros.
+    C.CDLL(None).mallopt(-6, 255)
+    Jt, mask = blob_problem((n, n, n), blobs=16, seed=0)
+    ref = Reference("ref64_match")
+    k = min(IT, MATCHING_SAMPLE_ITERATIONS)
+    for _ in range(args.warmup):
+        ref.solve("matching", Jt, mask, it_max=1)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.solve("matching", Jt, mask, it_max=k)
+        times.append(time.perf_counter() - t0)
+    value = Jt.size * k * len(times) / sum(times)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"per step: {k} iterations of the matching solve of the {n}^3 volume from the zero field "
+              f"(a bounded sample of the it_max={IT} step), reference volume_matching_3d (OpenMP) through its "
+              f"C ABI")
+    print(json.dumps({
+        "impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_matching(n, IT), "iterations_per_step": k,
+                   "warmup_steps": "it_max=1 solves"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
 
 
 def run_reference_c3(args):
@@ -683,7 +739,7 @@ def run_matching(args, world, rank, local, quiet=False):
     from disptools_b200.synthetic import blob_problem
 
     torch.cuda.set_device(local)
-    n, IT = 128, args.it_max
+    n, IT = MATCHING_SIZE, args.it_max
     Jt, mask = blob_problem((n, n, n), blobs=16, seed=rank)
     nvox = n ** 3
     dev = torch.device("cuda", local)
@@ -784,17 +840,17 @@ def run_matching(args, world, rank, local, quiet=False):
             C.CDLL(None).mallopt(-6, 255)
             ref = Reference("ref64_match")
             t0 = time.perf_counter()
-            ref.solve("matching", Jt, mask, it_max=10)
+            ref.solve("matching", Jt, mask, it_max=MATCHING_SAMPLE_ITERATIONS)
             tcpu = time.perf_counter() - t0
-            cpu = {"value": nvox * 10 / tcpu, "unit": UNIT,
+            cpu = {"value": nvox * MATCHING_SAMPLE_ITERATIONS / tcpu, "unit": UNIT,
                    "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "reference",
-                   "sample": f"reference volume_matching_3d (OpenMP) on the same volume, 10 iterations: {tcpu:.2f} s"}
+                   "sample": f"reference volume_matching_3d (OpenMP) on the same volume, "
+                             f"{MATCHING_SAMPLE_ITERATIONS} iterations: {tcpu:.2f} s"}
     line = {
         "metric": "matching-solver voxel-iters/s, 128^3 (16 blobs)", "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"matching solver on {n}^3 (16 Gaussian blobs), zero initial field, "
-                               f"it_max={IT} per step, device-resident float64 arrays",
+        "config": {"workload": workload_matching(n, IT), "arrays": "device-resident float64",
                    "iterations_per_step": iters / args.steps, "parallelism": f"{world} independent volumes",
                    "l2": "flushed between steps (256 MB write); within a solve the working set (positions, "
                          "step and next positions, 25 MB each) stays in L2"},

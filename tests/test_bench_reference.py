@@ -57,3 +57,20 @@ def test_reference_arm_prints_one_contract_line(workload):
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert d["config"]["size"] == [40, 40, 40]
+
+
+@pytest.mark.skipif(not Reference.available("ref64_match"), reason="reference matching build not present")
+def test_reference_arm_matching_line():
+    """The matching workload's reference arm: the reference's own
+    volume_matching_3d, the b200 arm's workload string and metric."""
+    d = _run("--workload", "matching", "--steps", "1", "--warmup", "1")
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["impl"] == "reference"
+    assert d["metric"] == "matching-solver voxel-iters/s, 128^3 (16 blobs)"
+    assert d["config"]["workload"] == bench.workload_matching(bench.MATCHING_SIZE, 100)
+    assert d["config"]["iterations_per_step"] == bench.MATCHING_SAMPLE_ITERATIONS
+    assert d["value"] > 0 and d["unit"] == "voxel-iters/s"
+    assert abs(d["ms_per_step"] / 1000.0 - 128 ** 3 * 10 / d["value"]) <= 0.05 * d["ms_per_step"] / 1000.0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0
